@@ -1,0 +1,376 @@
+// Test-oracle glue: a C entry layer over the reference's own TFHEpp and HEDB
+// CPU code, compiled from the reference sources by oracle/Makefile (target
+// `ref`).  Used only by tests/ and by bench.py's CPU-baseline leg, as the
+// checker and as the timed CPU reference; never by the product library.
+//
+// Key material comes from the caller (the deterministic generator in
+// tfhe_oracle.c), so the reference runs on exactly the keys the GPU path uses.
+// TFHEpp's own generator (thirdparty/TFHEpp/src/cloudkey.cpp:22-74) draws from
+// std::random_device and cannot be seeded.
+
+#include <cstdlib>
+#include <cstring>
+#include <thread>
+#include <vector>
+#include <atomic>
+
+#include <tfhe++.hpp>
+#include "HEDB/comparison/comparison.h"
+
+using namespace TFHEpp;
+using HEDB::TLWELvl1;
+
+namespace {
+struct RefCtx {
+    SecretKey sk;
+    EvalKey ek;
+    // key-switching keys are allocated with calloc so that rows never written
+    // stay untouched zero pages; they are released with free().
+    KeySwitchingKey<lvl10param> *ksk10 = nullptr;
+    KeySwitchingKey<lvl20param> *ksk20 = nullptr;
+    KeySwitchingKey<lvl21param> *ksk21 = nullptr;
+};
+
+template <class T>
+T *calloc_obj()
+{
+    return reinterpret_cast<T *>(std::calloc(1, sizeof(T)));
+}
+}  // namespace
+
+extern "C" {
+
+void *tref_new() { return new RefCtx(); }
+
+void tref_free(void *p)
+{
+    RefCtx *c = static_cast<RefCtx *>(p);
+    c->ek.iksklvl10.release();
+    c->ek.iksklvl20.release();
+    c->ek.iksklvl21.release();
+    std::free(c->ksk10);
+    std::free(c->ksk20);
+    std::free(c->ksk21);
+    delete c;
+}
+
+void tref_set_secret(void *p, const uint32_t *s0, const uint32_t *s1,
+                     const uint64_t *s2)
+{
+    RefCtx *c = static_cast<RefCtx *>(p);
+    for (uint32_t i = 0; i < lvl0param::n; i++) c->sk.key.lvl0[i] = s0[i];
+    for (uint32_t i = 0; i < lvl1param::n; i++) c->sk.key.lvl1[i] = s1[i];
+    for (uint32_t i = 0; i < lvl2param::n; i++) c->sk.key.lvl2[i] = s2[i];
+}
+
+// Integer bootstrapping key [672][(k+1)l][2][N] -> BootstrappingKeyFFT via
+// TFHEpp's own ApplyFFT2trgsw (thirdparty/TFHEpp/src/trgsw.cpp:183-193), which
+// is what bkfftgen does after trgswSymEncrypt (cloudkey.cpp:22-33).
+void tref_set_bk01_int(void *p, const uint32_t *bk)
+{
+    RefCtx *c = static_cast<RefCtx *>(p);
+    if (!c->ek.bkfftlvl01)
+        c->ek.bkfftlvl01 = std::make_unique<BootstrappingKeyFFT<lvl01param>>();
+    const size_t per = sizeof(TRGSW<lvl1param>) / sizeof(uint32_t);
+    for (uint32_t i = 0; i < lvl0param::n; i++) {
+        TRGSW<lvl1param> t;
+        std::memcpy(t.data(), bk + i * per, sizeof(t));
+        (*c->ek.bkfftlvl01)[i] = ApplyFFT2trgsw<lvl1param>(t);
+    }
+}
+
+void tref_set_bk02_int(void *p, const uint64_t *bk)
+{
+    RefCtx *c = static_cast<RefCtx *>(p);
+    if (!c->ek.bkfftlvl02)
+        c->ek.bkfftlvl02 = std::make_unique<BootstrappingKeyFFT<lvl02param>>();
+    const size_t per = sizeof(TRGSW<lvl2param>) / sizeof(uint64_t);
+    for (uint32_t i = 0; i < lvl0param::n; i++) {
+        TRGSW<lvl2param> t;
+        std::memcpy(t.data(), bk + i * per, sizeof(t));
+        (*c->ek.bkfftlvl02)[i] = ApplyFFT2trgsw<lvl2param>(t);
+    }
+}
+
+void tref_get_bkfft01(void *p, double *out)
+{
+    RefCtx *c = static_cast<RefCtx *>(p);
+    std::memcpy(out, c->ek.bkfftlvl01->data(), sizeof(BootstrappingKeyFFT<lvl01param>));
+}
+
+void tref_get_bkfft02(void *p, double *out)
+{
+    RefCtx *c = static_cast<RefCtx *>(p);
+    std::memcpy(out, c->ek.bkfftlvl02->data(), sizeof(BootstrappingKeyFFT<lvl02param>));
+}
+
+// kind: 10, 20, 21.  Returns the base of a zero-initialised full-size key the
+// caller fills (all rows, or only the rows a given input will touch).
+void *tref_ksk_alloc(void *p, int kind)
+{
+    RefCtx *c = static_cast<RefCtx *>(p);
+    if (kind == 10) {
+        if (!c->ksk10) {
+            c->ksk10 = calloc_obj<KeySwitchingKey<lvl10param>>();
+            c->ek.iksklvl10.reset(c->ksk10);
+        }
+        return c->ksk10;
+    }
+    if (kind == 20) {
+        if (!c->ksk20) {
+            c->ksk20 = calloc_obj<KeySwitchingKey<lvl20param>>();
+            c->ek.iksklvl20.reset(c->ksk20);
+        }
+        return c->ksk20;
+    }
+    if (kind == 21) {
+        if (!c->ksk21) {
+            c->ksk21 = calloc_obj<KeySwitchingKey<lvl21param>>();
+            c->ek.iksklvl21.reset(c->ksk21);
+        }
+        return c->ksk21;
+    }
+    return nullptr;
+}
+
+size_t tref_ksk_bytes(int kind)
+{
+    if (kind == 10) return sizeof(KeySwitchingKey<lvl10param>);
+    if (kind == 20) return sizeof(KeySwitchingKey<lvl20param>);
+    if (kind == 21) return sizeof(KeySwitchingKey<lvl21param>);
+    return 0;
+}
+
+// ---- primitives (mulfft.hpp:57-121, trgsw.cpp:20-39,77-103) -----------------
+void tref_twist_ifft_lvl1(double *out, const uint32_t *a)
+{
+    PolynomialInFD<lvl1param> r;
+    Polynomial<lvl1param> x;
+    std::memcpy(x.data(), a, sizeof(x));
+    TwistIFFT<lvl1param>(r, x);
+    std::memcpy(out, r.data(), sizeof(r));
+}
+
+void tref_twist_fft_lvl1(uint32_t *out, const double *a)
+{
+    PolynomialInFD<lvl1param> x;
+    Polynomial<lvl1param> r;
+    std::memcpy(x.data(), a, sizeof(x));
+    TwistFFT<lvl1param>(r, x);
+    std::memcpy(out, r.data(), sizeof(r));
+}
+
+void tref_twist_ifft_lvl2(double *out, const uint64_t *a)
+{
+    PolynomialInFD<lvl2param> r;
+    Polynomial<lvl2param> x;
+    std::memcpy(x.data(), a, sizeof(x));
+    TwistIFFT<lvl2param>(r, x);
+    std::memcpy(out, r.data(), sizeof(r));
+}
+
+void tref_twist_fft_lvl2(uint64_t *out, const double *a)
+{
+    PolynomialInFD<lvl2param> x;
+    Polynomial<lvl2param> r;
+    std::memcpy(x.data(), a, sizeof(x));
+    TwistFFT<lvl2param>(r, x);
+    std::memcpy(out, r.data(), sizeof(r));
+}
+
+void tref_decomp_lvl1(uint32_t *out, const uint32_t *poly, int digit)
+{
+    Polynomial<lvl1param> x;
+    DecomposedPolynomial<lvl1param> d;
+    std::memcpy(x.data(), poly, sizeof(x));
+    DecompositionPolynomial<lvl1param>(d, x, digit);
+    std::memcpy(out, d.data(), sizeof(d));
+}
+
+void tref_decomp_lvl2(uint64_t *out, const uint64_t *poly, int digit)
+{
+    Polynomial<lvl2param> x;
+    DecomposedPolynomial<lvl2param> d;
+    std::memcpy(x.data(), poly, sizeof(x));
+    DecompositionPolynomial<lvl2param>(d, x, digit);
+    std::memcpy(out, d.data(), sizeof(d));
+}
+
+void tref_extprod_lvl1(uint32_t *res, const uint32_t *trlwe, const double *trgswfft)
+{
+    TRLWE<lvl1param> in, out;
+    auto *g = new TRGSWFFT<lvl1param>;
+    std::memcpy(in.data(), trlwe, sizeof(in));
+    std::memcpy(g->data(), trgswfft, sizeof(*g));
+    trgswfftExternalProduct<lvl1param>(out, in, *g);
+    std::memcpy(res, out.data(), sizeof(out));
+    delete g;
+}
+
+void tref_extprod_lvl2(uint64_t *res, const uint64_t *trlwe, const double *trgswfft)
+{
+    TRLWE<lvl2param> in, out;
+    auto *g = new TRGSWFFT<lvl2param>;
+    std::memcpy(in.data(), trlwe, sizeof(in));
+    std::memcpy(g->data(), trgswfft, sizeof(*g));
+    trgswfftExternalProduct<lvl2param>(out, in, *g);
+    std::memcpy(res, out.data(), sizeof(out));
+    delete g;
+}
+
+// ---- PBS / IKS / gates ------------------------------------------------------
+void tref_pbs01(void *p, uint32_t *out, const uint32_t *in0, const uint32_t *tv)
+{
+    RefCtx *c = static_cast<RefCtx *>(p);
+    TLWE<lvl0param> x;
+    TLWE<lvl1param> r;
+    Polynomial<lvl1param> t;
+    std::memcpy(x.data(), in0, sizeof(x));
+    std::memcpy(t.data(), tv, sizeof(t));
+    GateBootstrappingTLWE2TLWEFFT<lvl01param>(r, x, *c->ek.bkfftlvl01, t);
+    std::memcpy(out, r.data(), sizeof(r));
+}
+
+void tref_pbs02(void *p, uint64_t *out, const uint32_t *in0, const uint64_t *tv)
+{
+    RefCtx *c = static_cast<RefCtx *>(p);
+    TLWE<lvl0param> x;
+    TLWE<lvl2param> r;
+    Polynomial<lvl2param> t;
+    std::memcpy(x.data(), in0, sizeof(x));
+    std::memcpy(t.data(), tv, sizeof(t));
+    GateBootstrappingTLWE2TLWEFFT<lvl02param>(r, x, *c->ek.bkfftlvl02, t);
+    std::memcpy(out, r.data(), sizeof(r));
+}
+
+void tref_iks10(void *p, uint32_t *out, const uint32_t *in)
+{
+    RefCtx *c = static_cast<RefCtx *>(p);
+    TLWE<lvl1param> x;
+    TLWE<lvl0param> r;
+    std::memcpy(x.data(), in, sizeof(x));
+    IdentityKeySwitch<lvl10param>(r, x, *c->ksk10);
+    std::memcpy(out, r.data(), sizeof(r));
+}
+
+void tref_iks20(void *p, uint32_t *out, const uint64_t *in)
+{
+    RefCtx *c = static_cast<RefCtx *>(p);
+    TLWE<lvl2param> x;
+    TLWE<lvl0param> r;
+    std::memcpy(x.data(), in, sizeof(x));
+    IdentityKeySwitch<lvl20param>(r, x, *c->ksk20);
+    std::memcpy(out, r.data(), sizeof(r));
+}
+
+void tref_iks21(void *p, uint32_t *out, const uint64_t *in)
+{
+    RefCtx *c = static_cast<RefCtx *>(p);
+    TLWE<lvl2param> x;
+    TLWE<lvl1param> r;
+    std::memcpy(x.data(), in, sizeof(x));
+    IdentityKeySwitch<lvl21param>(r, x, *c->ksk21);
+    std::memcpy(out, r.data(), sizeof(r));
+}
+
+// HomNAND over lvl1 ciphertexts (thirdparty/TFHEpp/src/gate.cpp:50-65 with
+// GateBootstrapping<lvl1> at gatebootstrapping.hpp:150-158: IKS10 then PBS01).
+void tref_homnand(void *p, uint32_t *out, const uint32_t *ca, const uint32_t *cb)
+{
+    RefCtx *c = static_cast<RefCtx *>(p);
+    TLWE<lvl1param> a, b, r;
+    std::memcpy(a.data(), ca, sizeof(a));
+    std::memcpy(b.data(), cb, sizeof(b));
+    HomNAND<lvl1param>(r, a, b, c->ek);
+    std::memcpy(out, r.data(), sizeof(r));
+}
+
+// n independent HomNANDs on `nthreads` host threads (row-parallel, as the
+// reference's query drivers run them under `omp parallel for`).
+void tref_homnand_batch(void *p, uint32_t *out, const uint32_t *ca, const uint32_t *cb,
+                        int n, int nthreads)
+{
+    const size_t w = lvl1param::n + 1;
+    std::atomic<int> next(0);
+    auto work = [&]() {
+        for (;;) {
+            int i = next.fetch_add(1);
+            if (i >= n) break;
+            tref_homnand(p, out + i * w, ca + i * w, cb + i * w);
+        }
+    };
+    if (nthreads <= 1) { work(); return; }
+    std::vector<std::thread> th;
+    for (int t = 0; t < nthreads; t++) th.emplace_back(work);
+    for (auto &t : th) t.join();
+}
+
+void tref_pbs01_batch(void *p, uint32_t *out, const uint32_t *in0, const uint32_t *tv,
+                      int n, int nthreads)
+{
+    std::atomic<int> next(0);
+    auto work = [&]() {
+        for (;;) {
+            int i = next.fetch_add(1);
+            if (i >= n) break;
+            tref_pbs01(p, out + (size_t)i * (lvl1param::n + 1),
+                       in0 + (size_t)i * (lvl0param::n + 1), tv);
+        }
+    };
+    if (nthreads <= 1) { work(); return; }
+    std::vector<std::thread> th;
+    for (int t = 0; t < nthreads; t++) th.emplace_back(work);
+    for (auto &t : th) t.join();
+}
+
+// ---- HEDB CPU operators (src/HEDB/comparison/HomCompare.h:14-75) -------------
+// op: 0 greater_than, 1 greater_than_equal, 2 less_than, 3 less_than_equal, 4 equal
+void tref_compare_lvl1(void *p, uint32_t *res, const uint32_t *c1, const uint32_t *c2,
+                       int op, uint32_t plain_bits, int logic)
+{
+    RefCtx *c = static_cast<RefCtx *>(p);
+    TLWE<lvl1param> a, b;
+    TLWELvl1 r;
+    std::memcpy(a.data(), c1, sizeof(a));
+    std::memcpy(b.data(), c2, sizeof(b));
+    bool rt = logic != 0;
+    switch (op) {
+    case 0: HEDB::greater_than<lvl1param>(a, b, r, plain_bits, c->ek, rt); break;
+    case 1: HEDB::greater_than_equal<lvl1param>(a, b, r, plain_bits, c->ek, rt); break;
+    case 2: HEDB::less_than<lvl1param>(a, b, r, plain_bits, c->ek, rt); break;
+    case 3: HEDB::less_than_equal<lvl1param>(a, b, r, plain_bits, c->ek, rt); break;
+    default: HEDB::equal<lvl1param>(a, b, r, plain_bits, c->ek, rt); break;
+    }
+    std::memcpy(res, r.data(), sizeof(r));
+}
+
+void tref_compare_lvl2(void *p, uint32_t *res, const uint64_t *c1, const uint64_t *c2,
+                       int op, uint32_t plain_bits, int logic)
+{
+    RefCtx *c = static_cast<RefCtx *>(p);
+    TLWE<lvl2param> a, b;
+    TLWELvl1 r;
+    std::memcpy(a.data(), c1, sizeof(a));
+    std::memcpy(b.data(), c2, sizeof(b));
+    bool rt = logic != 0;
+    switch (op) {
+    case 0: HEDB::greater_than<lvl2param>(a, b, r, plain_bits, c->ek, rt); break;
+    case 1: HEDB::greater_than_equal<lvl2param>(a, b, r, plain_bits, c->ek, rt); break;
+    case 2: HEDB::less_than<lvl2param>(a, b, r, plain_bits, c->ek, rt); break;
+    case 3: HEDB::less_than_equal<lvl2param>(a, b, r, plain_bits, c->ek, rt); break;
+    default: HEDB::equal<lvl2param>(a, b, r, plain_bits, c->ek, rt); break;
+    }
+    std::memcpy(res, r.data(), sizeof(r));
+}
+
+void tref_homand(void *p, uint32_t *res, const uint32_t *ca, const uint32_t *cb, int logic)
+{
+    RefCtx *c = static_cast<RefCtx *>(p);
+    TLWELvl1 a, b, r;
+    std::memcpy(a.data(), ca, sizeof(a));
+    std::memcpy(b.data(), cb, sizeof(b));
+    HEDB::HomAND(r, a, b, c->ek, logic != 0);
+    std::memcpy(res, r.data(), sizeof(r));
+}
+
+}  // extern "C"
