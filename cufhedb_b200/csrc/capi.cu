@@ -1,0 +1,519 @@
+// C ABI of the engine (include/cufhedb_b200.h): context, key material,
+// batched operations and host-buffer entry points.
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "cufhedb_b200.h"
+#include "fftops.cuh"
+#include "iks.cuh"
+#include "keys.cuh"
+#include "pbs_common.cuh"
+
+using namespace cfdb;
+
+struct cufhedb_ctx {
+    int device = 0;
+    int num_sms = 0;
+    Fft512Tables *tab512 = nullptr;   // device copy of the lvl1 transform tables
+    double2 *bk01 = nullptr;          // FFT-domain lvl01 key, chunk layout
+    uint32_t *bk01_int = nullptr;     // integer lvl01 key (when loaded or generated)
+    uint32_t *ksk[3] = {nullptr, nullptr, nullptr};   // lvl10, lvl20, lvl21
+    int *err = nullptr;               // device failure word
+    cudaStream_t io = nullptr;        // stream of the host-buffer entry points
+    std::mutex io_mu;
+    bool have_sk = false;
+    uint32_t *s0_d = nullptr, *s1_d = nullptr;
+    uint64_t *s2_d = nullptr;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what)
+{
+    const int code = (e == cudaErrorMemoryAllocation) ? CUFHEDB_ERR_OOM : CUFHEDB_ERR_CUDA;
+    return fail(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                                \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);     \
+    } while (0)
+
+#define NEED(cond, msg)                                                 \
+    do {                                                                \
+        if (!(cond)) return fail(CUFHEDB_ERR_ARG, std::string(msg));    \
+    } while (0)
+
+constexpr size_t BK01_ROWS = (size_t)N0 * 2 * L1;   // TRGSW rows of the lvl01 key
+constexpr size_t BK01_WORDS = BK01_ROWS * 2 * N1;
+
+size_t ksk_words(int kind)
+{
+    if (kind == 10) return (size_t)1024 * 2 * 1023 * (N0 + 1);
+    if (kind == 20) return (size_t)2048 * 2 * 1023 * (N0 + 1);
+    if (kind == 21) return (size_t)2048 * 10 * 7 * (N1 + 1);
+    return 0;
+}
+
+int ksk_slot(int kind) { return kind == 10 ? 0 : kind == 20 ? 1 : kind == 21 ? 2 : -1; }
+
+void build_tables(Fft512Tables &T)
+{
+    const long double PI = 3.141592653589793238462643383279502884L;
+    for (int q2 = 0; q2 < 16; ++q2)
+        for (int m1 = 0; m1 < 32; ++m1) {
+            const long double a = 2.0L * PI * (long double)((m1 * q2) % 512) / 512.0L;
+            T.tw512[q2 * 32 + m1] = make_double2((double)cosl(a), (double)sinl(a));
+        }
+    for (int m2 = 0; m2 < 16; ++m2)
+        for (int m1 = 0; m1 < 32; ++m1) {
+            const long double a = 2.0L * PI * (long double)(m1 + 32 * m2) / 2048.0L;
+            T.twist[m2 * 32 + m1] = make_double2((double)cosl(a), (double)sinl(a));
+        }
+    for (int j = 0; j < 16; ++j) {
+        const long double a = 2.0L * PI * (long double)j / 32.0L;
+        T.w32[j] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+}
+
+struct GateSpec {
+    int sa, sb;
+    uint32_t offset;
+};
+
+// thirdparty/TFHEpp/src/gate.cpp:60-181 (mu = lvl1param::mu = 2^29)
+const GateSpec kGates[10] = {
+    {-1, -1, 1u << 29},          {-1, -1, 0u - (1u << 29)}, {-2, -2, 0u - (2u << 29)}, {1, 1, 0u - (1u << 29)},
+    {1, 1, 1u << 29},            {2, 2, 2u << 29},          {-1, 1, 0u - (1u << 29)},  {1, -1, 0u - (1u << 29)},
+    {-1, 1, 1u << 29},           {1, -1, 1u << 29},
+};
+
+TestVec to_tv(const cufhedb_testvec *tv)
+{
+    TestVec t{};
+    t.kind = tv->kind;
+    t.pad = tv->pad_bits;
+    t.value = tv->value;
+    t.poly = tv->poly;
+    return t;
+}
+
+int check_tv(const cufhedb_testvec *tv, int N)
+{
+    NEED(tv != nullptr, "test vector is null");
+    NEED(tv->kind >= 0 && tv->kind <= 2, "unknown test-vector kind");
+    if (tv->kind == CUFHEDB_TV_STAIRCASE) {
+        NEED(tv->pad_bits >= 0 && tv->pad_bits < 31, "staircase pad_bits out of range");
+        NEED(tv->value < 64, "staircase scale_bits out of range");
+    }
+    if (tv->kind == CUFHEDB_TV_POLY) NEED(tv->poly != nullptr, "test-vector polynomial is null");
+    (void)N;
+    return CUFHEDB_OK;
+}
+
+int pbs01_enqueue(cufhedb_ctx *ctx, const uint32_t *in, uint32_t *out, int B, const cufhedb_testvec *tv,
+                  int precision, cudaStream_t st)
+{
+    if (!ctx->bk01) return fail(CUFHEDB_ERR_NOKEY, "lvl01 bootstrapping key not loaded");
+    if (precision != CUFHEDB_FP64) return fail(CUFHEDB_ERR_ARG, "unsupported precision");
+    Pbs01Args a{};
+    a.in = in;
+    a.out = out;
+    a.B = B;
+    a.bk = ctx->bk01;
+    a.tables = ctx->tab512;
+    a.tv = to_tv(tv);
+    a.err = ctx->err;
+    CK(launch_pbs01_f64(a, ctx->num_sms, st));
+    return CUFHEDB_OK;
+}
+
+int gate_enqueue(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint32_t *cb, uint32_t *out, int B,
+                 int precision, cudaStream_t st)
+{
+    NEED(gate >= 0 && gate < 10, "unknown gate");
+    if (!ctx->ksk[0]) return fail(CUFHEDB_ERR_NOKEY, "lvl10 key-switching key not loaded");
+    if (!ctx->bk01) return fail(CUFHEDB_ERR_NOKEY, "lvl01 bootstrapping key not loaded");
+    uint32_t *mid = nullptr;
+    CK(cudaMallocAsync((void **)&mid, (size_t)B * (N0 + 1) * sizeof(uint32_t), st));
+    IksArgs k{};
+    k.in32 = ca;
+    k.in32b = cb;
+    k.sa = kGates[gate].sa;
+    k.sb = kGates[gate].sb;
+    k.offset = kGates[gate].offset;
+    k.out = mid;
+    k.ksk = ctx->ksk[0];
+    k.B = B;
+    cudaError_t e = launch_iks(k, 10, st);
+    cufhedb_testvec tv{CUFHEDB_TV_CONST, 0, 1u << 29, nullptr};
+    int rc = (e == cudaSuccess) ? pbs01_enqueue(ctx, mid, out, B, &tv, precision, st) : cuda_fail(e, "iks10");
+    cudaError_t ef = cudaFreeAsync(mid, st);
+    if (rc != CUFHEDB_OK) return rc;
+    CK(ef);
+    return CUFHEDB_OK;
+}
+
+struct DeviceGuard {
+    explicit DeviceGuard(int dev) { cudaSetDevice(dev); }
+};
+
+}  // namespace
+
+extern "C" {
+
+int cufhedb_abi_version(void) { return CUFHEDB_ABI_VERSION; }
+
+const char *cufhedb_last_error(void) { return g_err.c_str(); }
+
+int cufhedb_ctx_create(cufhedb_ctx **out, int device)
+{
+    NEED(out != nullptr, "out is null");
+    *out = nullptr;
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev));
+    NEED(device >= 0 && device < ndev, "device index out of range");
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10)
+        return fail(CUFHEDB_ERR_UNSUPPORTED, "cufhedb_b200 needs an sm_100 (Blackwell) device");
+    CK(cudaSetDevice(device));
+    cufhedb_ctx *ctx = new cufhedb_ctx();
+    ctx->device = device;
+    ctx->num_sms = prop.multiProcessorCount;
+    Fft512Tables host_tab;
+    build_tables(host_tab);
+    cudaError_t e = cudaMalloc((void **)&ctx->tab512, sizeof(Fft512Tables));
+    if (e == cudaSuccess) e = cudaMemcpy(ctx->tab512, &host_tab, sizeof(Fft512Tables), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&ctx->err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(ctx->err, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->io, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        cufhedb_ctx_destroy(ctx);
+        return cuda_fail(e, "context set-up");
+    }
+    *out = ctx;
+    return CUFHEDB_OK;
+}
+
+int cufhedb_ctx_destroy(cufhedb_ctx *ctx)
+{
+    if (!ctx) return CUFHEDB_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->io) cudaStreamSynchronize(ctx->io);
+    cudaFree(ctx->tab512);
+    cudaFree(ctx->bk01);
+    cudaFree(ctx->bk01_int);
+    for (auto p : ctx->ksk) cudaFree(p);
+    cudaFree(ctx->err);
+    cudaFree(ctx->s0_d);
+    cudaFree(ctx->s1_d);
+    cudaFree(ctx->s2_d);
+    if (ctx->io) cudaStreamDestroy(ctx->io);
+    delete ctx;
+    return CUFHEDB_OK;
+}
+
+int cufhedb_ctx_num_sms(const cufhedb_ctx *ctx) { return ctx ? ctx->num_sms : 0; }
+
+int cufhedb_sync(cufhedb_ctx *ctx, cufhedb_stream_t stream)
+{
+    NEED(ctx != nullptr, "ctx is null");
+    DeviceGuard g(ctx->device);
+    CK(cudaStreamSynchronize((cudaStream_t)stream));
+    int flag = 0;
+    CK(cudaMemcpy(&flag, ctx->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+        CK(cudaMemset(ctx->err, 0, sizeof(int)));
+        return fail(CUFHEDB_ERR_DEVICE, "a kernel gave up a bounded wait (code " + std::to_string(flag) + ")");
+    }
+    return CUFHEDB_OK;
+}
+
+// ---- keys ----------------------------------------------------------------
+
+int cufhedb_secret_keys(uint64_t seed, uint32_t *s0, uint32_t *s1, uint64_t *s2)
+{
+    NEED(s0 && s1 && s2, "null output");
+    host_secret_keys(seed, s0, s1, s2);
+    return CUFHEDB_OK;
+}
+
+static int ensure_alloc(void **p, size_t bytes)
+{
+    if (*p) return CUFHEDB_OK;
+    CK(cudaMalloc(p, bytes));
+    return CUFHEDB_OK;
+}
+
+int cufhedb_load_bkfft_lvl01(cufhedb_ctx *ctx, const double *bkfft)
+{
+    NEED(ctx && bkfft, "null argument");
+    DeviceGuard g(ctx->device);
+    int rc = ensure_alloc((void **)&ctx->bk01, BK01_ROWS * 1024 * sizeof(double2));
+    if (rc) return rc;
+    double *tmp = nullptr;
+    CK(cudaMalloc((void **)&tmp, BK01_WORDS * sizeof(double)));
+    cudaError_t e = cudaMemcpy(tmp, bkfft, BK01_WORDS * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = bkfft01_permute(ctx->bk01, tmp, (int)BK01_ROWS, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    cudaFree(tmp);
+    if (e != cudaSuccess) return cuda_fail(e, "load_bkfft_lvl01");
+    return CUFHEDB_OK;
+}
+
+int cufhedb_load_bk_lvl01(cufhedb_ctx *ctx, const uint32_t *bk)
+{
+    NEED(ctx && bk, "null argument");
+    DeviceGuard g(ctx->device);
+    int rc = ensure_alloc((void **)&ctx->bk01, BK01_ROWS * 1024 * sizeof(double2));
+    if (rc) return rc;
+    rc = ensure_alloc((void **)&ctx->bk01_int, BK01_WORDS * sizeof(uint32_t));
+    if (rc) return rc;
+    CK(cudaMemcpy(ctx->bk01_int, bk, BK01_WORDS * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    CK(bk01_to_fft(ctx->bk01, ctx->bk01_int, (int)BK01_ROWS, ctx->tab512, 0));
+    CK(cudaDeviceSynchronize());
+    return CUFHEDB_OK;
+}
+
+int cufhedb_load_ksk(cufhedb_ctx *ctx, int kind, const uint32_t *ksk)
+{
+    NEED(ctx && ksk, "null argument");
+    const int slot = ksk_slot(kind);
+    NEED(slot >= 0, "unknown key-switching key kind");
+    DeviceGuard g(ctx->device);
+    const size_t bytes = ksk_words(kind) * sizeof(uint32_t);
+    int rc = ensure_alloc((void **)&ctx->ksk[slot], bytes);
+    if (rc) return rc;
+    CK(cudaMemcpy(ctx->ksk[slot], ksk, bytes, cudaMemcpyHostToDevice));
+    return CUFHEDB_OK;
+}
+
+int cufhedb_keygen(cufhedb_ctx *ctx, uint64_t seed, unsigned flags)
+{
+    NEED(ctx != nullptr, "ctx is null");
+    NEED((flags & ~31u) == 0, "unknown keygen flag");
+    DeviceGuard g(ctx->device);
+    std::vector<uint32_t> s0(N0), s1(N1);
+    std::vector<uint64_t> s2(N2);
+    host_secret_keys(seed, s0.data(), s1.data(), s2.data());
+    int rc = ensure_alloc((void **)&ctx->s0_d, N0 * 4);
+    if (!rc) rc = ensure_alloc((void **)&ctx->s1_d, N1 * 4);
+    if (!rc) rc = ensure_alloc((void **)&ctx->s2_d, N2 * 8);
+    if (rc) return rc;
+    CK(cudaMemcpy(ctx->s0_d, s0.data(), N0 * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->s1_d, s1.data(), N1 * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->s2_d, s2.data(), N2 * 8, cudaMemcpyHostToDevice));
+    ctx->have_sk = true;
+
+    if (flags & CUFHEDB_GEN_BK01) {
+        std::vector<int> pos;
+        for (int i = 0; i < N1; ++i)
+            if (s1[i]) pos.push_back(i);
+        int *pos_d = nullptr;
+        CK(cudaMalloc((void **)&pos_d, pos.size() * sizeof(int)));
+        cudaError_t e = cudaMemcpy(pos_d, pos.data(), pos.size() * sizeof(int), cudaMemcpyHostToDevice);
+        rc = ensure_alloc((void **)&ctx->bk01_int, BK01_WORDS * sizeof(uint32_t));
+        if (!rc) rc = ensure_alloc((void **)&ctx->bk01, BK01_ROWS * 1024 * sizeof(double2));
+        if (rc) {
+            cudaFree(pos_d);
+            return rc;
+        }
+        if (e == cudaSuccess) e = gen_bk01(ctx->bk01_int, seed, ctx->s0_d, pos_d, (int)pos.size(), 0);
+        if (e == cudaSuccess) e = bk01_to_fft(ctx->bk01, ctx->bk01_int, (int)BK01_ROWS, ctx->tab512, 0);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        cudaFree(pos_d);
+        if (e != cudaSuccess) return cuda_fail(e, "keygen bk01");
+    }
+    const int kinds[3] = {10, 20, 21};
+    const unsigned kflags[3] = {CUFHEDB_GEN_KSK10, CUFHEDB_GEN_KSK20, CUFHEDB_GEN_KSK21};
+    for (int t = 0; t < 3; ++t) {
+        if (!(flags & kflags[t])) continue;
+        rc = ensure_alloc((void **)&ctx->ksk[t], ksk_words(kinds[t]) * sizeof(uint32_t));
+        if (rc) return rc;
+        const void *dom = kinds[t] == 10 ? (const void *)ctx->s1_d : (const void *)ctx->s2_d;
+        const uint32_t *tgt = kinds[t] == 21 ? ctx->s1_d : ctx->s0_d;
+        CK(gen_ksk(ctx->ksk[t], kinds[t], seed, dom, tgt, 0));
+        CK(cudaDeviceSynchronize());
+    }
+    return CUFHEDB_OK;
+}
+
+int cufhedb_export_bk_lvl01(cufhedb_ctx *ctx, uint32_t *bk)
+{
+    NEED(ctx && bk, "null argument");
+    if (!ctx->bk01_int) return fail(CUFHEDB_ERR_NOKEY, "no integer lvl01 key on the device");
+    DeviceGuard g(ctx->device);
+    CK(cudaMemcpy(bk, ctx->bk01_int, BK01_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    return CUFHEDB_OK;
+}
+
+int cufhedb_export_ksk_rows(cufhedb_ctx *ctx, int kind, const uint64_t *rows, int n, uint32_t *out)
+{
+    NEED(ctx && rows && out && n >= 0, "bad argument");
+    const int slot = ksk_slot(kind);
+    NEED(slot >= 0, "unknown key-switching key kind");
+    if (!ctx->ksk[slot]) return fail(CUFHEDB_ERR_NOKEY, "key-switching key not loaded");
+    DeviceGuard g(ctx->device);
+    const size_t width = kind == 21 ? N1 + 1 : N0 + 1;
+    const size_t nrows = ksk_words(kind) / width;
+    for (int r = 0; r < n; ++r) {
+        NEED(rows[r] < nrows, "row index out of range");
+        CK(cudaMemcpy(out + r * width, ctx->ksk[slot] + rows[r] * width, width * 4, cudaMemcpyDeviceToHost));
+    }
+    return CUFHEDB_OK;
+}
+
+int cufhedb_encrypt_lvl1(cufhedb_ctx *ctx, uint64_t seed, uint64_t stream_id, uint64_t idx0, const uint32_t *msg,
+                         uint32_t *out, int B, cufhedb_stream_t stream)
+{
+    NEED(ctx && msg && out && B >= 0, "bad argument");
+    if (!ctx->have_sk) return fail(CUFHEDB_ERR_NOKEY, "no deterministic key set (call cufhedb_keygen)");
+    DeviceGuard g(ctx->device);
+    CK(encrypt_tlwe32(out, msg, B, N1, ctx->s1_d, NS_LVL1, seed, stream_id, idx0, (cudaStream_t)stream));
+    return CUFHEDB_OK;
+}
+
+// ---- batched operations --------------------------------------------------
+
+int cufhedb_pbs_lvl01(cufhedb_ctx *ctx, const uint32_t *in_lvl0, uint32_t *out_lvl1, int B,
+                      const cufhedb_testvec *tv, int precision, cufhedb_stream_t stream)
+{
+    NEED(ctx != nullptr, "ctx is null");
+    NEED(B >= 0, "negative batch");
+    if (B == 0) return CUFHEDB_OK;
+    NEED(in_lvl0 && out_lvl1, "null buffer");
+    int rc = check_tv(tv, N1);
+    if (rc) return rc;
+    DeviceGuard g(ctx->device);
+    return pbs01_enqueue(ctx, in_lvl0, out_lvl1, B, tv, precision, (cudaStream_t)stream);
+}
+
+int cufhedb_iks(cufhedb_ctx *ctx, int kind, const void *in, uint32_t *out, int B, cufhedb_stream_t stream)
+{
+    NEED(ctx != nullptr, "ctx is null");
+    const int slot = ksk_slot(kind);
+    NEED(slot >= 0, "unknown key-switching kind");
+    NEED(B >= 0, "negative batch");
+    if (B == 0) return CUFHEDB_OK;
+    NEED(in && out, "null buffer");
+    if (!ctx->ksk[slot]) return fail(CUFHEDB_ERR_NOKEY, "key-switching key not loaded");
+    DeviceGuard g(ctx->device);
+    IksArgs a{};
+    if (kind == 10) a.in32 = (const uint32_t *)in;
+    else a.in64 = (const uint64_t *)in;
+    a.sa = 1;
+    a.out = out;
+    a.ksk = ctx->ksk[slot];
+    a.B = B;
+    CK(launch_iks(a, kind, (cudaStream_t)stream));
+    return CUFHEDB_OK;
+}
+
+int cufhedb_gate_lvl1(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint32_t *cb, uint32_t *out, int B,
+                      int precision, cufhedb_stream_t stream)
+{
+    NEED(ctx != nullptr, "ctx is null");
+    NEED(B >= 0, "negative batch");
+    if (B == 0) return CUFHEDB_OK;
+    NEED(ca && cb && out, "null buffer");
+    DeviceGuard g(ctx->device);
+    return gate_enqueue(ctx, gate, ca, cb, out, B, precision, (cudaStream_t)stream);
+}
+
+int cufhedb_twist_ifft_lvl1(cufhedb_ctx *ctx, const uint32_t *in, double *out, int B, cufhedb_stream_t stream)
+{
+    NEED(ctx && B >= 0, "bad argument");
+    if (B == 0) return CUFHEDB_OK;
+    NEED(in && out, "null buffer");
+    DeviceGuard g(ctx->device);
+    CK(launch_twist_ifft1(out, in, B, ctx->tab512, (cudaStream_t)stream));
+    return CUFHEDB_OK;
+}
+
+int cufhedb_twist_fft_lvl1(cufhedb_ctx *ctx, const double *in, uint32_t *out, int B, cufhedb_stream_t stream)
+{
+    NEED(ctx && B >= 0, "bad argument");
+    if (B == 0) return CUFHEDB_OK;
+    NEED(in && out, "null buffer");
+    DeviceGuard g(ctx->device);
+    CK(launch_twist_fft1(out, in, B, ctx->tab512, (cudaStream_t)stream));
+    return CUFHEDB_OK;
+}
+
+// ---- host-buffer entry points ----------------------------------------------
+
+int cufhedb_pbs_lvl01_host(cufhedb_ctx *ctx, const uint32_t *in_lvl0, uint32_t *out_lvl1, int B,
+                           const cufhedb_testvec *tv, int precision)
+{
+    NEED(ctx != nullptr, "ctx is null");
+    NEED(B >= 0, "negative batch");
+    if (B == 0) return CUFHEDB_OK;
+    NEED(in_lvl0 && out_lvl1, "null buffer");
+    int rc = check_tv(tv, N1);
+    if (rc) return rc;
+    DeviceGuard g(ctx->device);
+    std::lock_guard<std::mutex> lk(ctx->io_mu);
+    cudaStream_t st = ctx->io;
+    const size_t ib = (size_t)B * (N0 + 1) * 4, ob = (size_t)B * (N1 + 1) * 4;
+    uint32_t *din = nullptr, *dout = nullptr;
+    CK(cudaMallocAsync((void **)&din, ib, st));
+    CK(cudaMallocAsync((void **)&dout, ob, st));
+    cudaError_t e = cudaMemcpyAsync(din, in_lvl0, ib, cudaMemcpyHostToDevice, st);
+    rc = (e == cudaSuccess) ? pbs01_enqueue(ctx, din, dout, B, tv, precision, st) : cuda_fail(e, "h2d");
+    if (rc == CUFHEDB_OK) {
+        e = cudaMemcpyAsync(out_lvl1, dout, ob, cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) rc = cuda_fail(e, "d2h");
+    }
+    cudaFreeAsync(din, st);
+    cudaFreeAsync(dout, st);
+    if (rc != CUFHEDB_OK) {
+        cudaStreamSynchronize(st);
+        return rc;
+    }
+    return cufhedb_sync(ctx, st);
+}
+
+int cufhedb_gate_lvl1_host(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint32_t *cb, uint32_t *out, int B,
+                           int precision)
+{
+    NEED(ctx != nullptr, "ctx is null");
+    NEED(B >= 0, "negative batch");
+    if (B == 0) return CUFHEDB_OK;
+    NEED(ca && cb && out, "null buffer");
+    DeviceGuard g(ctx->device);
+    std::lock_guard<std::mutex> lk(ctx->io_mu);
+    cudaStream_t st = ctx->io;
+    const size_t nb = (size_t)B * (N1 + 1) * 4;
+    uint32_t *dbuf = nullptr;
+    CK(cudaMallocAsync((void **)&dbuf, 3 * nb, st));
+    uint32_t *da = dbuf, *db = dbuf + (size_t)B * (N1 + 1), *dout = dbuf + 2 * (size_t)B * (N1 + 1);
+    int rc = CUFHEDB_OK;
+    cudaError_t e = cudaMemcpyAsync(da, ca, nb, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(db, cb, nb, cudaMemcpyHostToDevice, st);
+    rc = (e == cudaSuccess) ? gate_enqueue(ctx, gate, da, db, dout, B, precision, st) : cuda_fail(e, "h2d");
+    if (rc == CUFHEDB_OK) {
+        e = cudaMemcpyAsync(out, dout, nb, cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) rc = cuda_fail(e, "d2h");
+    }
+    cudaFreeAsync(dbuf, st);
+    if (rc != CUFHEDB_OK) {
+        cudaStreamSynchronize(st);
+        return rc;
+    }
+    return cufhedb_sync(ctx, st);
+}
+
+}  // extern "C"

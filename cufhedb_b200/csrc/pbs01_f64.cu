@@ -1,0 +1,214 @@
+// Batched lvl0 -> lvl1 programmable bootstrapping, FP64 path.
+//
+// Restates GateBootstrappingTLWE2TLWEFFT<lvl01param>
+// (thirdparty/TFHEpp/src/gatebootstrapping.cpp:14-23): BlindRotate
+// (include/gatebootstrapping.hpp:15-43) = 672 x CMUXFFTwithPolynomialMulByXaiMinusOne
+// (src/detwfa.cpp:20-35) followed by SampleExtractIndex(0) (src/trlwe.cpp:108-118).
+//
+// B200 layout: one CTA per group of W ciphertexts (one warp each) plus one
+// producer warp.  Every accumulator TRLWE lives in shared memory for the whole
+// blind rotation; the FFT-domain bootstrapping key streams through a ring of
+// S 16 KB slots filled by bulk (TMA-engine) copies and shared by the W warps,
+// so each key byte crosses L2->SM once per CTA instead of once per ciphertext.
+// Per CMux each warp runs 6 forward transforms (decomposition fused into the
+// load), a register-resident frequency-domain multiply-accumulate against the
+// key chunk, and 2 inverse transforms whose output is added into the
+// accumulator.  No grid-wide barrier: CTAs are independent.
+#include "pbs_common.cuh"
+
+namespace cfdb {
+
+template <int W, int S>
+struct Pbs01Smem {
+    static constexpr int RING_OFF = 128;
+    static constexpr int CHUNK_BYTES = 16384;  // one TRGSW row: 2 outputs x 512 complex x 16 B
+    static constexpr int TAB_OFF = RING_OFF + S * CHUNK_BYTES;
+    static constexpr int WARP_OFF = TAB_OFF + ((int)sizeof(Fft512Tables) + 127) / 128 * 128;
+    static constexpr int XP_BYTES = 512 * 16;
+    static constexpr int ACC_BYTES = 2 * N1 * 4;
+    static constexpr int ABAR_BYTES = ((N0 * 2) + 127) / 128 * 128;
+    static constexpr int PER_WARP = XP_BYTES + ACC_BYTES + ABAR_BYTES;
+    static constexpr int TOTAL = WARP_OFF + W * PER_WARP;
+};
+
+// (X^a - 1) * poly at coefficients m and m+512, decomposed to digit d and
+// twisted: v[m2] = (dig(m) + i dig(m+512)) * w^m,  m = lane + 32 m2
+__device__ __forceinline__ void load_digit_poly1(double2 v[16], const uint32_t *poly, uint32_t abar, int d,
+                                                 int lane, const Fft512Tables &T)
+{
+    const int sh = 32 - BGBIT1 * (d + 1);
+#pragma unroll
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int m = lane + 32 * m2;
+        uint32_t t0 = rot_coef<N1>(poly, m, abar) - poly[m];
+        uint32_t t1 = rot_coef<N1>(poly, m + 512, abar) - poly[m + 512];
+        int d0 = (int)(((t0 + DEC1_OFFSET + DEC1_ROUND) >> sh) & 63u) - 32;
+        int d1 = (int)(((t1 + DEC1_OFFSET + DEC1_ROUND) >> sh) & 63u) - 32;
+        v[m2] = cmul(make_double2((double)d0, (double)d1), T.twist[m2 * 32 + lane]);
+    }
+}
+
+// poly[m] += a_m, poly[m+512] += a_{m+512} from v[m2] = 512 z_m
+__device__ __forceinline__ void add_inverse_poly1(uint32_t *poly, const double2 v[16], int lane,
+                                                  const Fft512Tables &T)
+{
+#pragma unroll
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int m = lane + 32 * m2;
+        double2 y = cmulc(v[m2], T.twist[m2 * 32 + lane]);
+        poly[m] += f64_to_torus32(y.x * (1.0 / 512.0));
+        poly[m + 512] += f64_to_torus32(y.y * (1.0 / 512.0));
+    }
+}
+
+template <int W, int S>
+__global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_f64_kernel(Pbs01Args a)
+{
+    using L = Pbs01Smem<W, S>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+    uint64_t *empty = full + S;
+    double2 *ring = reinterpret_cast<double2 *>(smem + L::RING_OFF);
+    Fft512Tables *T = reinterpret_cast<Fft512Tables *>(smem + L::TAB_OFF);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], W);
+        }
+        fence_barrier_init();
+    }
+    {
+        const double2 *src = reinterpret_cast<const double2 *>(a.tables);
+        double2 *dst = reinterpret_cast<double2 *>(T);
+        for (int i = threadIdx.x; i < (int)(sizeof(Fft512Tables) / 16); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+
+    const int ngroups = (a.B + W - 1) / W;
+    constexpr int CHUNKS = N0 * 2 * L1;
+
+    if (warp == W) {
+        // producer: one elected lane streams the key, chunk by chunk
+        if (lane == 0) {
+            uint32_t c = 0;
+            bool ok = true;
+            for (int g = blockIdx.x; g < ngroups && ok; g += gridDim.x) {
+                for (int ch = 0; ch < CHUNKS; ++ch, ++c) {
+                    const int slot = c % S;
+                    if (c >= (uint32_t)S && !mbar_wait(&empty[slot], ((c / S) - 1) & 1)) {
+                        report_error(a.err, DEV_TIMEOUT_EMPTY);
+                        ok = false;
+                        break;
+                    }
+                    mbar_arrive_expect_tx(&full[slot], L::CHUNK_BYTES);
+                    bulk_g2s(ring + slot * 1024, a.bk + (size_t)ch * 1024, L::CHUNK_BYTES, &full[slot]);
+                }
+            }
+            // no copy may still be in flight when the CTA exits
+            for (uint32_t k = (c > (uint32_t)S ? c - S : 0); k < c; ++k)
+                if (!mbar_wait(&full[k % S], (k / S) & 1)) report_error(a.err, DEV_TIMEOUT_DRAIN);
+        }
+        return;
+    }
+
+    unsigned char *wb = smem + L::WARP_OFF + warp * L::PER_WARP;
+    double2 *xp = reinterpret_cast<double2 *>(wb);
+    uint32_t *acc = reinterpret_cast<uint32_t *>(wb + L::XP_BYTES);
+    uint16_t *abar_s = reinterpret_cast<uint16_t *>(wb + L::XP_BYTES + L::ACC_BYTES);
+
+    uint32_t c = 0;
+    for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
+        const int ct = g * W + warp;
+        const bool valid = ct < a.B;
+        uint32_t bbar = 2 * N1;
+        if (valid) {
+            const uint32_t *in = a.in + (size_t)ct * (N0 + 1);
+            for (int i = lane; i < N0; i += 32) abar_s[i] = (uint16_t)((in[i] + (1u << 20)) >> 21);
+            bbar = 2 * N1 - (in[N0] >> 21);
+        }
+        for (int j = lane; j < N1; j += 32) {
+            acc[j] = 0;
+            acc[N1 + j] = testvec_rot1(a.tv, j, bbar);
+        }
+        __syncwarp();
+
+        for (int i = 0; i < N0; ++i) {
+            const uint32_t ab = valid ? abar_s[i] : 0u;
+            const bool active = ab != 0;
+            double2 f0[16], f1[16];
+#pragma unroll 1
+            for (int r = 0; r < 2 * L1; ++r, ++c) {
+                const int slot = c % S;
+                if (!mbar_wait(&full[slot], (c / S) & 1)) {
+                    report_error(a.err, DEV_TIMEOUT_FULL);
+                    return;
+                }
+                if (active) {
+                    double2 v[16];
+                    load_digit_poly1(v, acc + (r / L1) * N1, ab, r % L1, lane, *T);
+                    fft512_fwd(v, xp, *T, lane);
+                    const double2 *bkc = ring + slot * 1024;
+                    if (r == 0) {
+#pragma unroll
+                        for (int s = 0; s < 16; ++s) {
+                            f0[s] = cmul(v[s], bkc[(2 * s) * 32 + lane]);
+                            f1[s] = cmul(v[s], bkc[(2 * s + 1) * 32 + lane]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int s = 0; s < 16; ++s) {
+                            cfma(f0[s], v[s], bkc[(2 * s) * 32 + lane]);
+                            cfma(f1[s], v[s], bkc[(2 * s + 1) * 32 + lane]);
+                        }
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&empty[slot]);
+            }
+            if (active) {
+                fft512_inv(f0, xp, *T, lane);
+                add_inverse_poly1(acc, f0, lane, *T);
+                fft512_inv(f1, xp, *T, lane);
+                add_inverse_poly1(acc + N1, f1, lane, *T);
+                __syncwarp();
+            }
+        }
+        if (valid) {
+            uint32_t *o = a.out + (size_t)ct * (N1 + 1);
+            for (int j = lane; j < N1; j += 32) o[j] = j == 0 ? acc[0] : (uint32_t)(0u - acc[N1 - j]);
+            if (lane == 0) o[N1] = acc[N1];
+        }
+        __syncwarp();
+    }
+}
+
+template <int W, int S>
+static cudaError_t launch_pbs01_f64_t(const Pbs01Args &a, int grid, cudaStream_t st)
+{
+    using L = Pbs01Smem<W, S>;
+    cudaError_t e = cudaFuncSetAttribute(pbs01_f64_kernel<W, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         L::TOTAL);
+    if (e != cudaSuccess) return e;
+    pbs01_f64_kernel<W, S><<<grid, (W + 1) * 32, L::TOTAL, st>>>(a);
+    return cudaGetLastError();
+}
+
+// Persistent grid: min(groups, SMs) CTAs of W = 7 consumer warps + 1 producer
+// warp, each looping over groups of 7 ciphertexts.  8 warps put 2 warps on
+// each SM sub-partition, so every thread may hold 255 registers (the 16
+// complex FFT values plus two 16-complex frequency accumulators per lane);
+// 1,024 ciphertexts map to 147 CTAs, one wave on 148 SMs.
+constexpr int PBS01_W = 7, PBS01_S = 4;
+
+cudaError_t launch_pbs01_f64(const Pbs01Args &a, int num_sms, cudaStream_t st)
+{
+    if (a.B <= 0) return cudaSuccess;
+    const int groups = (a.B + PBS01_W - 1) / PBS01_W;
+    return launch_pbs01_f64_t<PBS01_W, PBS01_S>(a, groups < num_sms ? groups : num_sms, st);
+}
+
+size_t pbs01_f64_smem_bytes() { return Pbs01Smem<PBS01_W, PBS01_S>::TOTAL; }
+
+}  // namespace cfdb

@@ -1,0 +1,72 @@
+// Kernel-argument structs and helpers shared by the PBS / external-product
+// kernels.
+#pragma once
+#include "common.cuh"
+#include "fft_f64.cuh"
+
+namespace cfdb {
+
+// Test-vector descriptor.  The accumulator starts as (0, X^bbar * tv).
+//   kind 0: constant tv[i] = value (TFHEpp mu-polygen, gatebootstrapping.hpp:132-138;
+//           the GPU reference's upolygen, cuHEDB fft_gpu/BlindRotate_gpu.cuh:92-124)
+//   kind 1: staircase tv[i] = 2^value * (i >> pad) (HEDB gpolygen,
+//           src/HEDB/comparison/tfhepp_utils.h:113-120)
+//   kind 2: an arbitrary polynomial `poly` (device memory, N words)
+struct TestVec {
+    int kind;
+    int pad;
+    uint64_t value;
+    const void *poly;
+};
+
+// coefficient j of X^a * poly, a in [0, 2N]  (utils.hpp:110-125)
+template <int N, typename T>
+__device__ __forceinline__ T rot_coef(const T *poly, int j, uint32_t a)
+{
+    const uint32_t idx = (uint32_t)(j - (int)a) & (2 * N - 1);
+    T v = poly[idx & (N - 1)];
+    return (idx & N) ? (T)(T(0) - v) : v;
+}
+
+__device__ __forceinline__ uint32_t testvec_coef1(const TestVec &tv, uint32_t i)
+{
+    if (tv.kind == 0) return (uint32_t)tv.value;
+    if (tv.kind == 1) return (uint32_t)((1ull << tv.value) * (uint64_t)(i >> tv.pad));
+    return reinterpret_cast<const uint32_t *>(tv.poly)[i];
+}
+
+__device__ __forceinline__ uint64_t testvec_coef2(const TestVec &tv, uint32_t i)
+{
+    if (tv.kind == 0) return tv.value;
+    if (tv.kind == 1) return (1ull << tv.value) * (uint64_t)(i >> tv.pad);
+    return reinterpret_cast<const uint64_t *>(tv.poly)[i];
+}
+
+// coefficient j of X^bbar * tv for the lvl1 ring
+__device__ __forceinline__ uint32_t testvec_rot1(const TestVec &tv, int j, uint32_t bbar)
+{
+    const uint32_t idx = (uint32_t)(j - (int)bbar) & (2 * N1 - 1);
+    const uint32_t v = testvec_coef1(tv, idx & (N1 - 1));
+    return (idx & N1) ? 0u - v : v;
+}
+
+__device__ __forceinline__ uint64_t testvec_rot2(const TestVec &tv, int j, uint32_t bbar)
+{
+    const uint32_t idx = (uint32_t)(j - (int)bbar) & (2 * N2 - 1);
+    const uint64_t v = testvec_coef2(tv, idx & (N2 - 1));
+    return (idx & N2) ? 0ull - v : v;
+}
+
+struct Pbs01Args {
+    const uint32_t *in;      // B x (N0+1) lvl0 TLWE
+    uint32_t *out;           // B x (N1+1) lvl1 TLWE
+    int B;
+    const double2 *bk;       // N0 x 6 chunks x 1024 complex, chunk layout [s][o][lane]
+    const void *tables;      // Fft512Tables in global memory
+    TestVec tv;
+    int *err;
+};
+
+cudaError_t launch_pbs01_f64(const Pbs01Args &a, int num_sms, cudaStream_t st);
+
+}  // namespace cfdb

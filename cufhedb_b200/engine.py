@@ -1,0 +1,172 @@
+"""Host-side mirror of the engine for Python callers (tests, benchmarks).
+
+``Engine`` owns one context (``cufhedb_ctx``) on one device.  Device buffers
+are torch CUDA tensors used as raw storage: 32-bit torus words live in
+``torch.int32`` tensors and 64-bit ones in ``torch.int64`` tensors, bit for
+bit (torch is only the allocator and stream provider here).  Host buffers are
+numpy arrays of ``uint32`` / ``uint64`` / ``float64``.
+
+Sizes follow TFHEpp (thirdparty/TFHEpp/include/params/128bit.hpp:7-83).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+N0, N1, L1, N2, L2 = 672, 1024, 3, 2048, 4
+MU1 = 1 << 29
+BK01_SHAPE = (N0, 2 * L1, 2, N1)
+
+
+def _ptr(t) -> int:
+    """Device or host address of a torch tensor or numpy array."""
+    if isinstance(t, np.ndarray):
+        if not t.flags["C_CONTIGUOUS"]:
+            raise ValueError("numpy buffers must be C-contiguous")
+        return t.ctypes.data
+    if not t.is_contiguous():
+        raise ValueError("tensors must be contiguous")
+    return t.data_ptr()
+
+
+def _stream(stream) -> int | None:
+    if stream is None:
+        try:
+            import torch
+            return torch.cuda.current_stream().cuda_stream
+        except Exception:
+            return None
+    return getattr(stream, "cuda_stream", stream)
+
+
+def testvec_const(mu: int) -> _lib.TestVec:
+    return _lib.TestVec(_lib.TV_CONST, 0, mu & 0xFFFFFFFFFFFFFFFF, None)
+
+
+def testvec_staircase(scale_bits: int, pad_bits: int = 6) -> _lib.TestVec:
+    return _lib.TestVec(_lib.TV_STAIRCASE, pad_bits, scale_bits, None)
+
+
+def testvec_poly(dev_tensor) -> _lib.TestVec:
+    return _lib.TestVec(_lib.TV_POLY, 0, 0, C.c_void_p(_ptr(dev_tensor)))
+
+
+class Engine:
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        check(self.lib.cufhedb_ctx_create(C.byref(h), device))
+        self.ctx = h
+        self.device = device
+
+    def close(self):
+        if self.ctx:
+            self.lib.cufhedb_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def num_sms(self) -> int:
+        return self.lib.cufhedb_ctx_num_sms(self.ctx)
+
+    def sync(self, stream=None):
+        check(self.lib.cufhedb_sync(self.ctx, _stream(stream)))
+
+    # ---- keys ----------------------------------------------------------------
+    def keygen(self, seed: int, flags: int = _lib.GEN_ALL):
+        check(self.lib.cufhedb_keygen(self.ctx, seed, flags))
+
+    def load_bkfft_lvl01(self, bkfft: np.ndarray):
+        bkfft = np.ascontiguousarray(bkfft, np.float64)
+        assert bkfft.size == N0 * 2 * L1 * 2 * N1
+        check(self.lib.cufhedb_load_bkfft_lvl01(self.ctx, _ptr(bkfft)))
+
+    def load_bk_lvl01(self, bk: np.ndarray):
+        bk = np.ascontiguousarray(bk, np.uint32)
+        assert bk.size == N0 * 2 * L1 * 2 * N1
+        check(self.lib.cufhedb_load_bk_lvl01(self.ctx, _ptr(bk)))
+
+    def load_ksk(self, kind: int, ksk: np.ndarray):
+        ksk = np.ascontiguousarray(ksk, np.uint32)
+        check(self.lib.cufhedb_load_ksk(self.ctx, kind, _ptr(ksk)))
+
+    def export_bk_lvl01(self) -> np.ndarray:
+        out = np.zeros(BK01_SHAPE, np.uint32)
+        check(self.lib.cufhedb_export_bk_lvl01(self.ctx, _ptr(out)))
+        return out
+
+    def export_ksk_rows(self, kind: int, rows) -> np.ndarray:
+        rows = np.ascontiguousarray(rows, np.uint64)
+        width = N1 + 1 if kind == 21 else N0 + 1
+        out = np.zeros((rows.size, width), np.uint32)
+        check(self.lib.cufhedb_export_ksk_rows(self.ctx, kind, _ptr(rows), rows.size, _ptr(out)))
+        return out
+
+    @staticmethod
+    def secret_keys(seed: int):
+        lib = _lib.load()
+        s0 = np.zeros(N0, np.uint32); s1 = np.zeros(N1, np.uint32); s2 = np.zeros(N2, np.uint64)
+        check(lib.cufhedb_secret_keys(seed, _ptr(s0), _ptr(s1), _ptr(s2)))
+        return s0, s1, s2
+
+    def encrypt_lvl1(self, seed: int, stream_id: int, idx0: int, msg_dev, out_dev, stream=None):
+        B = msg_dev.numel()
+        check(self.lib.cufhedb_encrypt_lvl1(self.ctx, seed, stream_id, idx0, _ptr(msg_dev), _ptr(out_dev), B,
+                                            _stream(stream)))
+
+    # ---- batched device operations ---------------------------------------------
+    def pbs_lvl01(self, in_dev, out_dev, tv: _lib.TestVec, precision: int = _lib.FP64, stream=None):
+        B = in_dev.numel() // (N0 + 1)
+        check(self.lib.cufhedb_pbs_lvl01(self.ctx, _ptr(in_dev), _ptr(out_dev), B, C.byref(tv), precision,
+                                         _stream(stream)))
+
+    def iks(self, kind: int, in_dev, out_dev, stream=None):
+        width = N1 + 1 if kind == 10 else N2 + 1
+        B = in_dev.numel() // width
+        check(self.lib.cufhedb_iks(self.ctx, kind, _ptr(in_dev), _ptr(out_dev), B, _stream(stream)))
+
+    def gate_lvl1(self, gate: str, ca_dev, cb_dev, out_dev, precision: int = _lib.FP64, stream=None):
+        B = ca_dev.numel() // (N1 + 1)
+        check(self.lib.cufhedb_gate_lvl1(self.ctx, _lib.GATES[gate], _ptr(ca_dev), _ptr(cb_dev), _ptr(out_dev), B,
+                                         precision, _stream(stream)))
+
+    def twist_ifft_lvl1(self, in_dev, out_dev, stream=None):
+        B = in_dev.numel() // N1
+        check(self.lib.cufhedb_twist_ifft_lvl1(self.ctx, _ptr(in_dev), _ptr(out_dev), B, _stream(stream)))
+
+    def twist_fft_lvl1(self, in_dev, out_dev, stream=None):
+        B = in_dev.numel() // N1
+        check(self.lib.cufhedb_twist_fft_lvl1(self.ctx, _ptr(in_dev), _ptr(out_dev), B, _stream(stream)))
+
+    # ---- host-buffer entry points --------------------------------------------------
+    def pbs_lvl01_host(self, in_lvl0: np.ndarray, tv: _lib.TestVec, precision: int = _lib.FP64) -> np.ndarray:
+        in_lvl0 = np.ascontiguousarray(in_lvl0, np.uint32).reshape(-1, N0 + 1)
+        out = np.zeros((in_lvl0.shape[0], N1 + 1), np.uint32)
+        check(self.lib.cufhedb_pbs_lvl01_host(self.ctx, _ptr(in_lvl0), _ptr(out), in_lvl0.shape[0], C.byref(tv),
+                                              precision))
+        return out
+
+    def gate_lvl1_host(self, gate: str, ca: np.ndarray, cb: np.ndarray, precision: int = _lib.FP64,
+                       out: np.ndarray | None = None) -> np.ndarray:
+        ca = np.ascontiguousarray(ca, np.uint32).reshape(-1, N1 + 1)
+        cb = np.ascontiguousarray(cb, np.uint32).reshape(-1, N1 + 1)
+        if out is None:
+            out = np.zeros_like(ca)
+        check(self.lib.cufhedb_gate_lvl1_host(self.ctx, _lib.GATES[gate], _ptr(ca), _ptr(cb), _ptr(out),
+                                              ca.shape[0], precision))
+        return out

@@ -1,0 +1,176 @@
+/*
+ * cufhedb_b200 -- B200-native (sm_100a) TFHE programmable-bootstrapping engine.
+ *
+ * C ABI of the engine that replaces cuFHEDB's GPU layer (src/cuHEDB/, header-
+ * only CUDA: fft_gpu/cufft_gpu.cuh, BlindRotate_gpu.cuh, ExternalProduct_gpu.cuh,
+ * fft_gpu.cuh) and the host-side TFHEpp::IdentityKeySwitch calls its operator
+ * wrappers make (src/cuHEDB/gatebootstrap_gpu.cuh:42,59,76,90,101,113,133,149,
+ * 159,167; msb_gpu.cuh:67,75,95).  Plain pointers and sizes only; every call
+ * returns an int status (CUFHEDB_OK = 0) and cufhedb_last_error() gives the
+ * message of the calling thread's last failure.
+ *
+ * Data layouts are TFHEpp's (thirdparty/TFHEpp/include/params.hpp:31-91),
+ * parameter set params/128bit.hpp:7-83:
+ *   TLWE<lvl0param>  673 x uint32   (a[672], b)
+ *   TLWE<lvl1param>  1025 x uint32  (a[1024], b)
+ *   TLWE<lvl2param>  2049 x uint64  (a[2048], b)
+ *   BootstrappingKey<lvl01param>     [672][6][2][1024] uint32
+ *   BootstrappingKeyFFT<lvl01param>  [672][6][2][1024] double (spqlios layout)
+ *   BootstrappingKey<lvl02param>     [672][8][2][2048] uint64
+ *   BootstrappingKeyFFT<lvl02param>  [672][8][2][2048] double
+ *   KeySwitchingKey<lvl10param>      [1024][2][1023][673] uint32
+ *   KeySwitchingKey<lvl20param>      [2048][2][1023][673] uint32
+ *   KeySwitchingKey<lvl21param>      [2048][10][7][1025] uint32
+ * Batches are arrays of B such objects, back to back.
+ *
+ * Entry points taking a stream enqueue work and return; device-side failures
+ * (a bounded wait inside a kernel that expired) are reported by the next
+ * cufhedb_sync() on that context.  *_host entry points take host buffers,
+ * copy in and out on an internal stream and return when the results are in
+ * the caller's memory.
+ */
+#ifndef CUFHEDB_B200_H
+#define CUFHEDB_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CUFHEDB_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define CUFHEDB_API __attribute__((visibility("default")))
+#else
+#define CUFHEDB_API
+#endif
+
+typedef struct cufhedb_ctx cufhedb_ctx;
+typedef void *cufhedb_stream_t; /* a cudaStream_t; NULL is the legacy default stream */
+
+enum cufhedb_status {
+    CUFHEDB_OK = 0,
+    CUFHEDB_ERR_ARG = 1,         /* null pointer, negative size, unknown kind */
+    CUFHEDB_ERR_NOKEY = 2,       /* the key this call needs was never loaded or generated */
+    CUFHEDB_ERR_CUDA = 3,        /* CUDA runtime error */
+    CUFHEDB_ERR_OOM = 4,         /* device or pinned allocation failed */
+    CUFHEDB_ERR_DEVICE = 5,      /* a kernel gave up a bounded wait and flagged the context */
+    CUFHEDB_ERR_UNSUPPORTED = 6  /* no usable sm_100 device */
+};
+
+enum cufhedb_precision {
+    CUFHEDB_FP64 = 0,   /* FP64 FFT and FP64 frequency-domain products */
+    CUFHEDB_SPLIT32 = 1 /* FP32 transforms, two-limb key, exact top-limb rounding */
+};
+
+enum cufhedb_ksk_kind { CUFHEDB_KSK10 = 10, CUFHEDB_KSK20 = 20, CUFHEDB_KSK21 = 21 };
+
+enum cufhedb_keygen_flags {
+    CUFHEDB_GEN_BK01 = 1,
+    CUFHEDB_GEN_BK02 = 2,
+    CUFHEDB_GEN_KSK10 = 4,
+    CUFHEDB_GEN_KSK20 = 8,
+    CUFHEDB_GEN_KSK21 = 16,
+    CUFHEDB_GEN_ALL = 31
+};
+
+/* test vector of a bootstrap: the accumulator starts as (0, X^bbar * tv) */
+enum cufhedb_tv_kind {
+    CUFHEDB_TV_CONST = 0,     /* tv[i] = value (TFHEpp mu-polygen) */
+    CUFHEDB_TV_STAIRCASE = 1, /* tv[i] = 2^value * (i >> pad_bits) (HEDB gpolygen) */
+    CUFHEDB_TV_POLY = 2       /* tv = poly, N words of device memory */
+};
+
+typedef struct {
+    int kind;
+    int pad_bits;
+    uint64_t value;
+    const void *poly;
+} cufhedb_testvec;
+
+/* two-input lvl1 gates of TFHEpp (thirdparty/TFHEpp/src/gate.cpp:60-181):
+ * out = PBS(IKS10(sa*ca + sb*cb + offset)) with a constant mu test vector */
+enum cufhedb_gate {
+    CUFHEDB_NAND = 0,
+    CUFHEDB_NOR = 1,
+    CUFHEDB_XNOR = 2,
+    CUFHEDB_AND = 3,
+    CUFHEDB_OR = 4,
+    CUFHEDB_XOR = 5,
+    CUFHEDB_ANDNY = 6,
+    CUFHEDB_ANDYN = 7,
+    CUFHEDB_ORNY = 8,
+    CUFHEDB_ORYN = 9
+};
+
+/* ---- context ------------------------------------------------------------ */
+CUFHEDB_API int cufhedb_abi_version(void);
+CUFHEDB_API const char *cufhedb_last_error(void);
+/* replaces the CuFFT_Torus constructor (src/cuHEDB/fft_gpu/cufft_gpu.cuh:135-163):
+ * binds a device, builds the twiddle tables; keys are loaded separately */
+CUFHEDB_API int cufhedb_ctx_create(cufhedb_ctx **out, int device);
+CUFHEDB_API int cufhedb_ctx_destroy(cufhedb_ctx *ctx);
+CUFHEDB_API int cufhedb_ctx_num_sms(const cufhedb_ctx *ctx);
+/* waits for `stream`, then reports (and clears) any device-side failure flag */
+CUFHEDB_API int cufhedb_sync(cufhedb_ctx *ctx, cufhedb_stream_t stream);
+
+/* ---- key material ----------------------------------------------------------- */
+/* LoadBK (cufft_gpu.cuh:175-184): TFHEpp BootstrappingKeyFFT<lvl01param>, host memory */
+CUFHEDB_API int cufhedb_load_bkfft_lvl01(cufhedb_ctx *ctx, const double *bkfft);
+/* integer BootstrappingKey<lvl01param> (TFHEpp bkgen output), host memory */
+CUFHEDB_API int cufhedb_load_bk_lvl01(cufhedb_ctx *ctx, const uint32_t *bk);
+/* KeySwitchingKey<lvl10/20/21param>, host memory; kind is cufhedb_ksk_kind.
+ * Replaces the host-resident key TFHEpp::IdentityKeySwitch reads (EvalKey::iksklvl*). */
+CUFHEDB_API int cufhedb_load_ksk(cufhedb_ctx *ctx, int kind, const uint32_t *ksk);
+/* Deterministic key set from `seed`, generated on the device (restates
+ * TFHEpp bkgen / ikskgen, thirdparty/TFHEpp/src/cloudkey.cpp:7-69, with a
+ * counter-based generator).  For tests and benchmarks: not a cryptographic
+ * generator. */
+CUFHEDB_API int cufhedb_keygen(cufhedb_ctx *ctx, uint64_t seed, unsigned flags);
+/* copies of device-resident key material, for checking and serialisation:
+ * the integer lvl01 key (when loaded with cufhedb_load_bk_lvl01 or generated),
+ * and n rows of a key-switching key (row = (i*t + j)*(2^basebit-1) + k) */
+CUFHEDB_API int cufhedb_export_bk_lvl01(cufhedb_ctx *ctx, uint32_t *bk);
+CUFHEDB_API int cufhedb_export_ksk_rows(cufhedb_ctx *ctx, int kind, const uint64_t *rows, int n, uint32_t *out);
+/* the secret keys of the deterministic key set (host-only computation) */
+CUFHEDB_API int cufhedb_secret_keys(uint64_t seed, uint32_t *s0, uint32_t *s1, uint64_t *s2);
+/* deterministic lvl1 TLWE encryptions of B messages (device arrays), counter
+ * blocks idx0.. of generator stream `stream_id` (test/benchmark inputs) */
+CUFHEDB_API int cufhedb_encrypt_lvl1(cufhedb_ctx *ctx, uint64_t seed, uint64_t stream_id, uint64_t idx0, const uint32_t *msg,
+                         uint32_t *out, int B, cufhedb_stream_t stream);
+
+/* ---- batched operations on device memory ------------------------------------- */
+/* B x GateBootstrappingTLWE2TLWEFFT<lvl01param> (cufft_gpu.cuh:250-294;
+ * TFHEpp src/gatebootstrapping.cpp:14-23): lvl0 TLWE in, lvl1 TLWE out */
+CUFHEDB_API int cufhedb_pbs_lvl01(cufhedb_ctx *ctx, const uint32_t *in_lvl0, uint32_t *out_lvl1, int B,
+                      const cufhedb_testvec *tv, int precision, cufhedb_stream_t stream);
+/* B x IdentityKeySwitch<lvl10/20/21param> (TFHEpp src/keyswitch.cpp:11-48).
+ * kind 10: in = B x 1025 uint32; kinds 20, 21: in = B x 2049 uint64.
+ * out = B x 673 (10, 20) or B x 1025 (21) uint32. */
+CUFHEDB_API int cufhedb_iks(cufhedb_ctx *ctx, int kind, const void *in, uint32_t *out, int B, cufhedb_stream_t stream);
+/* B two-input lvl1 gates (TFHEpp HomNAND etc., src/gate.cpp:50-181):
+ * IKS10 of the combined input, then PBS01 with the constant mu = 2^29 test vector */
+CUFHEDB_API int cufhedb_gate_lvl1(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint32_t *cb, uint32_t *out, int B,
+                      int precision, cufhedb_stream_t stream);
+/* B TwistIFFT<lvl1param> / TwistFFT<lvl1param> in TFHEpp's frequency layout
+ * (include/mulfft.hpp:57-121; the reference's ifft_st / fft_st, cufft_gpu.cuh:187-211) */
+CUFHEDB_API int cufhedb_twist_ifft_lvl1(cufhedb_ctx *ctx, const uint32_t *in, double *out, int B, cufhedb_stream_t stream);
+CUFHEDB_API int cufhedb_twist_fft_lvl1(cufhedb_ctx *ctx, const double *in, uint32_t *out, int B, cufhedb_stream_t stream);
+
+/* ---- host-buffer entry points (synchronous; the _st calls of cufft_gpu.cuh) ---- */
+CUFHEDB_API int cufhedb_pbs_lvl01_host(cufhedb_ctx *ctx, const uint32_t *in_lvl0, uint32_t *out_lvl1, int B,
+                           const cufhedb_testvec *tv, int precision);
+CUFHEDB_API int cufhedb_gate_lvl1_host(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint32_t *cb, uint32_t *out, int B,
+                           int precision);
+
+/* ---- diagnostics ------------------------------------------------------------ */
+/* measured CUDA-core FMA throughput (TFLOP/s) of `device`, FP64 (fp64 != 0) or
+ * FP32: the roofline denominator of the bootstrapping kernels */
+CUFHEDB_API int cufhedb_measure_fma_peak(int device, int fp64, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUFHEDB_B200_H */

@@ -1,0 +1,210 @@
+"""GPU parity: the lvl1 path (keys, transforms, IKS10, PBS01, gates) through
+the C ABI against the oracle and the reference's own TFHEpp."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import SEED, fill_ref_ksk, signed_diff
+
+from oracle.oracle import N0, N1, NS_LVL0, NS_LVL1
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+MU = 1 << 29
+
+
+def dev(a):
+    import torch
+    a = np.ascontiguousarray(a)
+    view = a.view(np.int32) if a.dtype == np.uint32 else a.view(np.int64) if a.dtype == np.uint64 else a
+    return torch.from_numpy(view.copy()).cuda()
+
+
+def host(t, dtype=np.uint32):
+    return t.cpu().numpy().view(dtype)
+
+
+def empty_dev(n, dtype="i32"):
+    import torch
+    return torch.zeros(n, dtype={"i32": torch.int32, "i64": torch.int64, "f64": torch.float64}[dtype], device="cuda")
+
+
+def phase(oracle, c, key):
+    return int(signed_diff(oracle.phase32(c, key), 0))
+
+
+def test_keygen_matches_oracle(engine, oracle, keys, bk01):
+    assert np.array_equal(engine.export_bk_lvl01(), bk01)
+    rows = np.array([0, 1, 777_777, 1024 * 2 * 1023 - 1], np.uint64)
+    got = engine.export_ksk_rows(10, rows)
+    for q, row in zip(rows, got):
+        q = int(q)
+        assert np.array_equal(oracle.ksk_row(10, SEED, keys, q // 2046, (q % 2046) // 1023, q % 1023), row)
+
+
+def test_twist_transforms_match_reference(engine, ref):
+    rng = np.random.default_rng(21)
+    B = 37
+    a = rng.integers(0, 2 ** 32, (B, N1), dtype=np.uint64).astype(np.uint32)
+    out = empty_dev(B * N1, "f64")
+    engine.twist_ifft_lvl1(dev(a), out)
+    engine.sync()
+    got = out.cpu().numpy().reshape(B, N1)
+    want = np.stack([ref.twist_ifft32(x) for x in a])
+    assert np.max(np.abs(got - want)) <= 1e-13 * np.max(np.abs(want))
+    back = empty_dev(B * N1)
+    import torch
+    engine.twist_fft_lvl1(torch.from_numpy(want.copy()).cuda(), back)
+    engine.sync()
+    back = host(back).reshape(B, N1)
+    want_back = np.stack([ref.twist_fft32(v) for v in want])
+    d = signed_diff(back, want_back)
+    assert np.max(np.abs(d)) <= 1
+    assert np.max(np.abs(signed_diff(back, a))) <= 1
+    g = np.load(os.path.join(GOLD, "tfhepp_lvl1.npz"))
+    out = empty_dev(4 * N1, "f64")
+    engine.twist_ifft_lvl1(dev(g["fft_in"]), out)
+    engine.sync()
+    assert np.max(np.abs(out.cpu().numpy().reshape(4, N1) - g["fft_out"])) <= 1e-13 * np.max(np.abs(g["fft_out"]))
+
+
+def test_iks10_bit_exact(engine, oracle, keys):
+    s0, s1, _ = keys
+    B = 37
+    xs = np.stack([oracle.tlwe32((i % 8) << 29, s1, NS_LVL1, SEED, 0x41, i) for i in range(B)])
+    xs[0, :] = 0
+    xs[1, :N1] = 0xFFFFFFFF
+    out = empty_dev(B * (N0 + 1))
+    engine.iks(10, dev(xs), out)
+    engine.sync()
+    got = host(out).reshape(B, N0 + 1)
+    for x, o in zip(xs, got):
+        assert np.array_equal(oracle.iks(10, x, SEED, keys), o)
+    g = np.load(os.path.join(GOLD, "tfhepp_lvl1.npz"))
+    out = empty_dev(4 * (N0 + 1))
+    engine.iks(10, dev(g["iks_in"]), out)
+    engine.sync()
+    assert np.array_equal(host(out).reshape(4, N0 + 1), g["iks_out"])
+
+
+@pytest.mark.parametrize("tvkind", ["const", "staircase", "poly"])
+def test_pbs01_trivial_inputs_exact(engine, oracle, tvkind):
+    """a = 0 makes every rotation index 0, so the PBS is exactly X^bbar * tv,
+    sample-extracted: bit-exact, including bbar = 2N (b < 2^21)."""
+    from cufhedb_b200 import testvec_const, testvec_poly, testvec_staircase
+    B = 9
+    x = np.zeros((B, N0 + 1), np.uint32)
+    x[:, N0] = np.array([0, 1, (1 << 21) - 1, 1 << 21, 0x80000000, 0xFFFFFFFF, 12345 << 21, 3 << 30, 7], np.uint32)
+    if tvkind == "const":
+        tv = testvec_const(MU); tvp = np.full(N1, MU, np.uint32)
+    elif tvkind == "staircase":
+        tv = testvec_staircase(24, 6); tvp = oracle.gpoly32(4, 24)
+    else:
+        tvp = np.random.default_rng(5).integers(0, 2 ** 32, N1, dtype=np.uint64).astype(np.uint32)
+        tvd = dev(tvp)
+        tv = testvec_poly(tvd)
+    out = empty_dev(B * (N1 + 1))
+    engine.pbs_lvl01(dev(x), out, tv)
+    engine.sync()
+    got = host(out).reshape(B, N1 + 1)
+    dummy_bkf = np.zeros((N0, 6, 2, N1), np.float64)
+    for xi, o in zip(x, got):
+        assert np.array_equal(oracle.pbs01(xi, dummy_bkf, tvp), o)
+
+
+def test_pbs01_decrypts_batch(engine, oracle, keys):
+    s0, s1, _ = keys
+    B = 7 * 20 + 3
+    bits = np.random.default_rng(22).integers(0, 2, B)
+    x = np.stack([oracle.tlwe32(MU if b else (-MU) & 0xFFFFFFFF, s0, NS_LVL0, SEED, 0x50, i) for i, b in enumerate(bits)])
+    from cufhedb_b200 import testvec_const
+    out = empty_dev(B * (N1 + 1))
+    engine.pbs_lvl01(dev(x), out, testvec_const(MU))
+    engine.sync()
+    got = host(out).reshape(B, N1 + 1)
+    ph = np.array([phase(oracle, o, s1) for o in got])
+    assert np.array_equal((ph > 0).astype(int), bits)
+    err = np.abs(ph) - MU
+    assert np.max(np.abs(err)) < 2 ** 26, np.max(np.abs(err))
+
+
+def test_pbs01_matches_reference(engine, oracle, ref_keyed, keys, bkfft01):
+    """Same keys and inputs through the reference's TFHEpp: same decryptions,
+    output phases within the bootstrapping noise of each other."""
+    s0, s1, _ = keys
+    B = 6
+    from cufhedb_b200 import testvec_const
+    x = np.stack([oracle.tlwe32(MU if i % 2 else (-MU) & 0xFFFFFFFF, s0, NS_LVL0, SEED, 0x51, i) for i in range(B)])
+    out = empty_dev(B * (N1 + 1))
+    engine.pbs_lvl01(dev(x), out, testvec_const(MU))
+    engine.sync()
+    got = host(out).reshape(B, N1 + 1)
+    tv = np.full(N1, MU, np.uint32)
+    for xi, o in zip(x, got):
+        r = ref_keyed.pbs01(xi, tv)
+        pr, pg = phase(oracle, r, s1), phase(oracle, o, s1)
+        assert (pr > 0) == (pg > 0)
+        assert abs(pr - pg) < 2 ** 25
+    g = np.load(os.path.join(GOLD, "tfhepp_lvl1.npz"))
+    out = empty_dev(4 * (N1 + 1))
+    engine.pbs_lvl01(dev(g["pbs_in"]), out, testvec_const(MU))
+    engine.sync()
+    for o, bit in zip(host(out).reshape(4, N1 + 1), g["pbs_bit"]):
+        assert int(phase(oracle, o, s1) > 0) == int(bit)
+
+
+@pytest.mark.parametrize("gate", ["NAND", "AND", "OR", "NOR", "XOR", "XNOR", "ANDNY", "ANDYN", "ORNY", "ORYN"])
+def test_gates_truth_table(engine, oracle, keys, gate):
+    s0, s1, _ = keys
+    B = 64
+    rng = np.random.default_rng(hash(gate) % 1000)
+    a = rng.integers(0, 2, B); b = rng.integers(0, 2, B)
+    enc = lambda bits, base: np.stack([oracle.tlwe32(MU if t else (-MU) & 0xFFFFFFFF, s1, NS_LVL1, SEED, 0x60, base + i)
+                                       for i, t in enumerate(bits)])
+    ca, cb = enc(a, 0), enc(b, 1000)
+    out = empty_dev(B * (N1 + 1))
+    engine.gate_lvl1(gate, dev(ca), dev(cb), out)
+    engine.sync()
+    got = np.array([phase(oracle, o, s1) > 0 for o in host(out).reshape(B, N1 + 1)]).astype(int)
+    truth = {"NAND": 1 - (a & b), "AND": a & b, "OR": a | b, "NOR": 1 - (a | b), "XOR": a ^ b, "XNOR": 1 - (a ^ b),
+             "ANDNY": (1 - a) & b, "ANDYN": a & (1 - b), "ORNY": (1 - a) | b, "ORYN": a | (1 - b)}[gate]
+    assert np.array_equal(got, truth)
+
+
+def test_homnand_matches_reference(engine, oracle, ref_keyed, keys):
+    s0, s1, _ = keys
+    B = 4
+    a, b = np.array([0, 0, 1, 1]), np.array([0, 1, 0, 1])
+    enc = lambda bits, base: np.stack([oracle.tlwe32(MU if t else (-MU) & 0xFFFFFFFF, s1, NS_LVL1, SEED, 0x61, base + i)
+                                       for i, t in enumerate(bits)])
+    ca, cb = enc(a, 0), enc(b, 100)
+    gate_in = [((0 - ca[i].astype(np.uint64) - cb[i].astype(np.uint64)) & 0xFFFFFFFF).astype(np.uint32) for i in range(B)]
+    for g_ in gate_in:
+        g_[N1] = (int(g_[N1]) + MU) & 0xFFFFFFFF
+    fill_ref_ksk(ref_keyed, oracle, keys, 10, gate_in)
+    got = engine.gate_lvl1_host("NAND", ca, cb)
+    for i in range(B):
+        r = ref_keyed.homnand(ca[i], cb[i])
+        pr, pg = phase(oracle, r, s1), phase(oracle, got[i], s1)
+        assert (pr > 0) == (pg > 0) == bool(1 - (a[i] & b[i]))
+        assert abs(pr - pg) < 2 ** 25
+
+
+def test_api_errors(engine):
+    from cufhedb_b200 import CufhedbError, Engine, testvec_const
+    import torch
+    x = empty_dev(N0 + 1)
+    out = empty_dev(N1 + 1)
+    engine.pbs_lvl01(x[:0], out[:0], testvec_const(MU))  # B = 0 is a no-op
+    with pytest.raises(CufhedbError) as e:
+        engine.pbs_lvl01(x, out, testvec_const(MU), precision=7)
+    assert e.value.code == 1
+    fresh = Engine(0)
+    with pytest.raises(CufhedbError) as e:
+        fresh.pbs_lvl01(x, out, testvec_const(MU))
+    assert e.value.code == 2
+    fresh.close()
+    engine.sync()
