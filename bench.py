@@ -48,6 +48,9 @@ def parse():
     p.add_argument("--batch", type=int, default=1024)
     p.add_argument("--precision", choices=["fp64", "split32"], default="fp64")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--profile-pbs", action="store_true",
+                   help="run only the lvl01 PBS kernel on `--batch` random lvl0 inputs (lvl01 key only, "
+                        "~0.1 GB on the device): the small case for ncu captures")
     return p.parse_args()
 
 
@@ -100,7 +103,7 @@ class ClockSampler:
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]})
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip() == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows)}
 
@@ -335,9 +338,37 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_profile_pbs(args):
+    """--steps launches of the PBS kernel alone, no key-switching key."""
+    import torch
+    from cufhedb_b200 import FP64, GEN_BK01, SPLIT32, Engine, testvec_const
+    prec = FP64 if args.precision == "fp64" else SPLIT32
+    eng = Engine(0)
+    eng.keygen(SEED, GEN_BK01)
+    g = torch.Generator(device="cuda").manual_seed(99)
+    x = torch.randint(-2 ** 31, 2 ** 31, (args.batch * (N0 + 1),), generator=g, device="cuda", dtype=torch.int64)
+    x = x.to(torch.int32)
+    out = torch.empty(args.batch * (N1 + 1), dtype=torch.int32, device="cuda")
+    tv = testvec_const(MU)
+    for _ in range(args.warmup):
+        eng.pbs_lvl01(x, out, tv, prec)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for e0, e1 in ev:
+        e0.record()
+        eng.pbs_lvl01(x, out, tv, prec)
+        e1.record()
+    eng.sync()
+    ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+    print(json.dumps({"profile": "pbs01", "batch": args.batch, "precision": args.precision,
+                      "ms": ms, "pbs_per_s": args.batch / (statistics.median(ms) / 1000.0) if ms else None}))
+    eng.close()
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.profile_pbs:
+        run_profile_pbs(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
