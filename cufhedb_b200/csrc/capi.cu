@@ -172,6 +172,38 @@ struct DeviceGuard {
 
 }  // namespace
 
+// Internal entry points shared with other translation units of the library
+// (not exported).
+namespace cfdb {
+
+int set_error(int code, const char *msg) { return fail(code, msg); }
+
+int ctx_device(const cufhedb_ctx *ctx) { return ctx->device; }
+
+// IKS10 of the combined gate input into the caller's lvl0 scratch (B x 673
+// words, fully overwritten), then PBS01 into `out`; allocates nothing.
+int gate_enqueue_into(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint32_t *cb, uint32_t *out, int B,
+                      int precision, cudaStream_t st, uint32_t *scratch_lvl0)
+{
+    NEED(gate >= 0 && gate < 10, "unknown gate");
+    if (!ctx->ksk[0]) return fail(CUFHEDB_ERR_NOKEY, "lvl10 key-switching key not loaded");
+    if (!ctx->bk01) return fail(CUFHEDB_ERR_NOKEY, "lvl01 bootstrapping key not loaded");
+    IksArgs k{};
+    k.in32 = ca;
+    k.in32b = cb;
+    k.sa = kGates[gate].sa;
+    k.sb = kGates[gate].sb;
+    k.offset = kGates[gate].offset;
+    k.out = scratch_lvl0;
+    k.ksk = ctx->ksk[0];
+    k.B = B;
+    CK(launch_iks(k, 10, st));
+    cufhedb_testvec tv{CUFHEDB_TV_CONST, 0, 1u << 29, nullptr};
+    return pbs01_enqueue(ctx, scratch_lvl0, out, B, &tv, precision, st);
+}
+
+}  // namespace cfdb
+
 extern "C" {
 
 int cufhedb_abi_version(void) { return CUFHEDB_ABI_VERSION; }

@@ -145,6 +145,14 @@ class Engine:
         check(self.lib.cufhedb_gate_lvl1(self.ctx, _lib.GATES[gate], _ptr(ca_dev), _ptr(cb_dev), _ptr(out_dev), B,
                                          precision, _stream(stream)))
 
+    def gate_lvl1_noalloc(self, gate: str, ca_dev, cb_dev, out_dev, precision: int = _lib.FP64, stream=None):
+        """Same result as gate_lvl1 without any device allocation: at most
+        1,024 gates per call, one shared per-device intermediate (calls that
+        overlap on the GPU race)."""
+        B = ca_dev.numel() // (N1 + 1)
+        check(self.lib.cufhedb_gate_lvl1_noalloc(self.ctx, _lib.GATES[gate], _ptr(ca_dev), _ptr(cb_dev),
+                                                 _ptr(out_dev), B, precision, _stream(stream)))
+
     def twist_ifft_lvl1(self, in_dev, out_dev, stream=None):
         B = in_dev.numel() // N1
         check(self.lib.cufhedb_twist_ifft_lvl1(self.ctx, _ptr(in_dev), _ptr(out_dev), B, _stream(stream)))

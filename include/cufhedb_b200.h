@@ -154,6 +154,17 @@ CUFHEDB_API int cufhedb_iks(cufhedb_ctx *ctx, int kind, const void *in, uint32_t
  * IKS10 of the combined input, then PBS01 with the constant mu = 2^29 test vector */
 CUFHEDB_API int cufhedb_gate_lvl1(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint32_t *cb, uint32_t *out, int B,
                       int precision, cufhedb_stream_t stream);
+/* cufhedb_gate_lvl1 without any allocation, for callers that cannot let a
+ * library allocate device memory while they run (an engine that reserves all
+ * device memory up front, or an allocator that owns the device).  No
+ * counterpart in the reference.  The key-switched intermediate lives in a
+ * fixed per-device array inside the library (2.63 MiB, held by every GPU that
+ * loads the library until exit): B <= 1024 gates per call, larger batches are
+ * rejected with CUFHEDB_ERR_ARG.  All calls on a device share that array, so
+ * calls that overlap on the GPU race; order them on one stream.  The first
+ * call on a device looks the array up (make it before any stream capture). */
+CUFHEDB_API int cufhedb_gate_lvl1_noalloc(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint32_t *cb,
+                                          uint32_t *out, int B, int precision, cufhedb_stream_t stream);
 /* B TwistIFFT<lvl1param> / TwistFFT<lvl1param> in TFHEpp's frequency layout
  * (include/mulfft.hpp:57-121; the reference's ifft_st / fft_st, cufft_gpu.cuh:187-211) */
 CUFHEDB_API int cufhedb_twist_ifft_lvl1(cufhedb_ctx *ctx, const uint32_t *in, double *out, int B, cufhedb_stream_t stream);
