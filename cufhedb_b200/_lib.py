@@ -53,6 +53,10 @@ SIGNATURES = {
     "cufhedb_iks": [_vp, _i32, _vp, _vp, _i32, _vp],
     "cufhedb_gate_lvl1": [_vp, _i32, _vp, _vp, _vp, _i32, _i32, _vp],
     "cufhedb_gate_lvl1_noalloc": [_vp, _i32, _vp, _vp, _vp, _i32, _i32, _vp],
+    "cufhedb_trgsw_prepare_lvl1": [_vp, _vp, _vp, _i32, _i32, _vp],
+    "cufhedb_trgswfft_prepare_lvl1": [_vp, _vp, _vp, _i32, _vp],
+    "cufhedb_extprod_lvl1": [_vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp],
+    "cufhedb_extprod_lvl1_host": [_vp, _vp, _vp, _vp, _i32, _i32],
     "cufhedb_twist_ifft_lvl1": [_vp, _vp, _vp, _i32, _vp],
     "cufhedb_twist_fft_lvl1": [_vp, _vp, _vp, _i32, _vp],
     "cufhedb_pbs_lvl01_host": [_vp, _vp, _vp, _i32, C.POINTER(TestVec), _i32],

@@ -7,6 +7,8 @@
 #include <vector>
 
 #include "cufhedb_b200.h"
+#include "fft_f32.cuh"
+#include "extprod.cuh"
 #include "fftops.cuh"
 #include "iks.cuh"
 #include "keys.cuh"
@@ -18,6 +20,8 @@ struct cufhedb_ctx {
     int device = 0;
     int num_sms = 0;
     Fft512Tables *tab512 = nullptr;   // device copy of the lvl1 transform tables
+    Fft512TablesF *tab512f = nullptr; // the same tables in FP32 (split-precision path)
+    float4 *bk01_split = nullptr;     // split-precision lvl01 key (hi/lo limbs, FP32)
     double2 *bk01 = nullptr;          // FFT-domain lvl01 key, chunk layout
     uint32_t *bk01_int = nullptr;     // integer lvl01 key (when loaded or generated)
     uint32_t *ksk[3] = {nullptr, nullptr, nullptr};   // lvl10, lvl20, lvl21
@@ -88,6 +92,15 @@ void build_tables(Fft512Tables &T)
     }
 }
 
+void build_tables_f(const Fft512Tables &D, Fft512TablesF &F)
+{
+    for (int i = 0; i < 512; ++i) {
+        F.tw512[i] = make_float2((float)D.tw512[i].x, (float)D.tw512[i].y);
+        F.twist[i] = make_float2((float)D.twist[i].x, (float)D.twist[i].y);
+    }
+    for (int j = 0; j < 16; ++j) F.w32[j] = make_float2((float)D.w32[j].x, (float)D.w32[j].y);
+}
+
 struct GateSpec {
     int sa, sb;
     uint32_t offset;
@@ -127,16 +140,23 @@ int pbs01_enqueue(cufhedb_ctx *ctx, const uint32_t *in, uint32_t *out, int B, co
                   int precision, cudaStream_t st)
 {
     if (!ctx->bk01) return fail(CUFHEDB_ERR_NOKEY, "lvl01 bootstrapping key not loaded");
-    if (precision != CUFHEDB_FP64) return fail(CUFHEDB_ERR_ARG, "unsupported precision");
+    if (precision != CUFHEDB_FP64 && precision != CUFHEDB_SPLIT32) return fail(CUFHEDB_ERR_ARG, "unsupported precision");
     Pbs01Args a{};
     a.in = in;
     a.out = out;
     a.B = B;
-    a.bk = ctx->bk01;
-    a.tables = ctx->tab512;
     a.tv = to_tv(tv);
     a.err = ctx->err;
-    CK(launch_pbs01_f64(a, ctx->num_sms, st));
+    if (precision == CUFHEDB_FP64) {
+        a.bk = ctx->bk01;
+        a.tables = ctx->tab512;
+        CK(launch_pbs01_f64(a, ctx->num_sms, st));
+    } else {
+        if (!ctx->bk01_split) return fail(CUFHEDB_ERR_NOKEY, "split-precision lvl01 key not prepared");
+        a.bk = reinterpret_cast<const double2 *>(ctx->bk01_split);
+        a.tables = ctx->tab512f;
+        CK(launch_pbs01_split(a, ctx->num_sms, st));
+    }
     return CUFHEDB_OK;
 }
 
@@ -227,8 +247,12 @@ int cufhedb_ctx_create(cufhedb_ctx **out, int device)
     ctx->num_sms = prop.multiProcessorCount;
     Fft512Tables host_tab;
     build_tables(host_tab);
+    Fft512TablesF host_tabf;
+    build_tables_f(host_tab, host_tabf);
     cudaError_t e = cudaMalloc((void **)&ctx->tab512, sizeof(Fft512Tables));
     if (e == cudaSuccess) e = cudaMemcpy(ctx->tab512, &host_tab, sizeof(Fft512Tables), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&ctx->tab512f, sizeof(Fft512TablesF));
+    if (e == cudaSuccess) e = cudaMemcpy(ctx->tab512f, &host_tabf, sizeof(Fft512TablesF), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc((void **)&ctx->err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(ctx->err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->io, cudaStreamNonBlocking);
@@ -246,7 +270,9 @@ int cufhedb_ctx_destroy(cufhedb_ctx *ctx)
     cudaSetDevice(ctx->device);
     if (ctx->io) cudaStreamSynchronize(ctx->io);
     cudaFree(ctx->tab512);
+    cudaFree(ctx->tab512f);
     cudaFree(ctx->bk01);
+    cudaFree(ctx->bk01_split);
     cudaFree(ctx->bk01_int);
     for (auto p : ctx->ksk) cudaFree(p);
     cudaFree(ctx->err);
@@ -290,6 +316,16 @@ static int ensure_alloc(void **p, size_t bytes)
     return CUFHEDB_OK;
 }
 
+// split-precision copy of the lvl01 key, from the integer key on the device
+static int prepare_split01(cufhedb_ctx *ctx)
+{
+    int rc = ensure_alloc((void **)&ctx->bk01_split, BK01_ROWS * 1024 * sizeof(float4));
+    if (rc) return rc;
+    CK(bk01_to_split(ctx->bk01_split, ctx->bk01_int, (int)BK01_ROWS, ctx->tab512, 0));
+    CK(cudaDeviceSynchronize());
+    return CUFHEDB_OK;
+}
+
 int cufhedb_load_bkfft_lvl01(cufhedb_ctx *ctx, const double *bkfft)
 {
     NEED(ctx && bkfft, "null argument");
@@ -303,7 +339,11 @@ int cufhedb_load_bkfft_lvl01(cufhedb_ctx *ctx, const double *bkfft)
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     cudaFree(tmp);
     if (e != cudaSuccess) return cuda_fail(e, "load_bkfft_lvl01");
-    return CUFHEDB_OK;
+    // the integer key (inverse transform, rounded) feeds the split-precision limbs
+    rc = ensure_alloc((void **)&ctx->bk01_int, BK01_WORDS * sizeof(uint32_t));
+    if (rc) return rc;
+    CK(bk01_fft_to_int(ctx->bk01_int, ctx->bk01, (int)BK01_ROWS, ctx->tab512, 0));
+    return prepare_split01(ctx);
 }
 
 int cufhedb_load_bk_lvl01(cufhedb_ctx *ctx, const uint32_t *bk)
@@ -317,7 +357,7 @@ int cufhedb_load_bk_lvl01(cufhedb_ctx *ctx, const uint32_t *bk)
     CK(cudaMemcpy(ctx->bk01_int, bk, BK01_WORDS * sizeof(uint32_t), cudaMemcpyHostToDevice));
     CK(bk01_to_fft(ctx->bk01, ctx->bk01_int, (int)BK01_ROWS, ctx->tab512, 0));
     CK(cudaDeviceSynchronize());
-    return CUFHEDB_OK;
+    return prepare_split01(ctx);
 }
 
 int cufhedb_load_ksk(cufhedb_ctx *ctx, int kind, const uint32_t *ksk)
@@ -368,6 +408,8 @@ int cufhedb_keygen(cufhedb_ctx *ctx, uint64_t seed, unsigned flags)
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
         cudaFree(pos_d);
         if (e != cudaSuccess) return cuda_fail(e, "keygen bk01");
+        rc = prepare_split01(ctx);
+        if (rc) return rc;
     }
     const int kinds[3] = {10, 20, 21};
     const unsigned kflags[3] = {CUFHEDB_GEN_KSK10, CUFHEDB_GEN_KSK20, CUFHEDB_GEN_KSK21};
@@ -485,6 +527,52 @@ int cufhedb_twist_fft_lvl1(cufhedb_ctx *ctx, const double *in, uint32_t *out, in
     return CUFHEDB_OK;
 }
 
+int cufhedb_trgsw_prepare_lvl1(cufhedb_ctx *ctx, const uint32_t *trgsw, void *out, int B, int precision,
+                               cufhedb_stream_t stream)
+{
+    NEED(ctx && B >= 0, "bad argument");
+    if (B == 0) return CUFHEDB_OK;
+    NEED(trgsw && out, "null buffer");
+    NEED(precision == CUFHEDB_FP64 || precision == CUFHEDB_SPLIT32, "unsupported precision");
+    DeviceGuard g(ctx->device);
+    const int rows = B * 2 * L1;
+    if (precision == CUFHEDB_FP64)
+        CK(bk01_to_fft((double2 *)out, trgsw, rows, ctx->tab512, (cudaStream_t)stream));
+    else
+        CK(bk01_to_split((float4 *)out, trgsw, rows, ctx->tab512, (cudaStream_t)stream));
+    return CUFHEDB_OK;
+}
+
+int cufhedb_trgswfft_prepare_lvl1(cufhedb_ctx *ctx, const double *trgswfft, void *out, int B,
+                                  cufhedb_stream_t stream)
+{
+    NEED(ctx && B >= 0, "bad argument");
+    if (B == 0) return CUFHEDB_OK;
+    NEED(trgswfft && out, "null buffer");
+    DeviceGuard g(ctx->device);
+    CK(bkfft01_permute((double2 *)out, trgswfft, B * 2 * L1, (cudaStream_t)stream));
+    return CUFHEDB_OK;
+}
+
+int cufhedb_extprod_lvl1(cufhedb_ctx *ctx, const uint32_t *trlwe, const void *trgsw, uint32_t *out, int B,
+                         int shared, int precision, cufhedb_stream_t stream)
+{
+    NEED(ctx && B >= 0, "bad argument");
+    if (B == 0) return CUFHEDB_OK;
+    NEED(trlwe && trgsw && out, "null buffer");
+    NEED(precision == CUFHEDB_FP64 || precision == CUFHEDB_SPLIT32, "unsupported precision");
+    DeviceGuard g(ctx->device);
+    ExtProdArgs a{};
+    a.trlwe = trlwe;
+    a.trgsw = trgsw;
+    a.out = out;
+    a.B = B;
+    a.shared = shared ? 1 : 0;
+    a.tables = precision == CUFHEDB_FP64 ? (const void *)ctx->tab512 : (const void *)ctx->tab512f;
+    CK(launch_extprod1(a, precision == CUFHEDB_FP64 ? 0 : 1, (cudaStream_t)stream));
+    return CUFHEDB_OK;
+}
+
 // ---- host-buffer entry points ----------------------------------------------
 
 int cufhedb_pbs_lvl01_host(cufhedb_ctx *ctx, const uint32_t *in_lvl0, uint32_t *out_lvl1, int B,
@@ -511,6 +599,47 @@ int cufhedb_pbs_lvl01_host(cufhedb_ctx *ctx, const uint32_t *in_lvl0, uint32_t *
     }
     cudaFreeAsync(din, st);
     cudaFreeAsync(dout, st);
+    if (rc != CUFHEDB_OK) {
+        cudaStreamSynchronize(st);
+        return rc;
+    }
+    return cufhedb_sync(ctx, st);
+}
+
+int cufhedb_extprod_lvl1_host(cufhedb_ctx *ctx, const uint32_t *trlwe, const double *trgswfft, uint32_t *out, int B,
+                              int shared)
+{
+    NEED(ctx != nullptr, "ctx is null");
+    NEED(B >= 0, "negative batch");
+    if (B == 0) return CUFHEDB_OK;
+    NEED(trlwe && trgswfft && out, "null buffer");
+    DeviceGuard g(ctx->device);
+    std::lock_guard<std::mutex> lk(ctx->io_mu);
+    cudaStream_t st = ctx->io;
+    const int ng = shared ? 1 : B;
+    const size_t tb = (size_t)B * 2 * N1 * 4, gb = (size_t)ng * 2 * L1 * 2 * N1 * 8;
+    char *buf = nullptr;
+    CK(cudaMallocAsync((void **)&buf, 2 * tb + 2 * gb, st));
+    uint32_t *din = (uint32_t *)buf, *dout = (uint32_t *)(buf + tb);
+    double *graw = (double *)(buf + 2 * tb);
+    void *gprep = buf + 2 * tb + gb;
+    int rc = CUFHEDB_OK;
+    cudaError_t e = cudaMemcpyAsync(din, trlwe, tb, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(graw, trgswfft, gb, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = bkfft01_permute((double2 *)gprep, graw, ng * 2 * L1, st);
+    if (e == cudaSuccess) {
+        ExtProdArgs a{};
+        a.trlwe = din;
+        a.trgsw = gprep;
+        a.out = dout;
+        a.B = B;
+        a.shared = shared ? 1 : 0;
+        a.tables = ctx->tab512;
+        e = launch_extprod1(a, 0, st);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, tb, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) rc = cuda_fail(e, "extprod_lvl1_host");
+    cudaFreeAsync(buf, st);
     if (rc != CUFHEDB_OK) {
         cudaStreamSynchronize(st);
         return rc;

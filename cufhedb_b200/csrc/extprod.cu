@@ -1,0 +1,159 @@
+// Batched lvl1 external products TRGSW (x) TRLWE, FP64 and split-precision
+// FP32 paths, plus the conversion of integer TRGSWs into the engine's
+// frequency-domain layout.
+//
+// Restates trgswfftExternalProduct<lvl1param> (thirdparty/TFHEpp/src/
+// trgsw.cpp:77-103): res_o = sum_{k,d} IFFT(dec_d(trlwe_k)) * trgsw[k l + d][o],
+// transformed back per output polynomial.  One warp per product; the TRGSW
+// rows (one per TRGSW or one shared by the batch) are read straight from HBM
+// in the per-lane chunk layout the PBS kernels use, so every load is a
+// coalesced 16-byte access and each TRGSW byte is read once.
+#include "extprod.cuh"
+#include "fft_f32.cuh"
+
+namespace cfdb {
+
+namespace {
+
+__device__ __forceinline__ void digits_f64(double2 v[16], const uint32_t *poly, int d, int lane, const Fft512Tables &T)
+{
+    const int sh = 32 - BGBIT1 * (d + 1);
+#pragma unroll
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int m = lane + 32 * m2;
+        int d0 = (int)(((poly[m] + DEC1_OFFSET + DEC1_ROUND) >> sh) & 63u) - 32;
+        int d1 = (int)(((poly[m + 512] + DEC1_OFFSET + DEC1_ROUND) >> sh) & 63u) - 32;
+        v[m2] = cmul(make_double2((double)d0, (double)d1), T.twist[m2 * 32 + lane]);
+    }
+}
+
+__device__ __forceinline__ void digits_f32(float2 v[16], const uint32_t *poly, int d, int lane, const Fft512TablesF &T)
+{
+    const int sh = 32 - BGBIT1 * (d + 1);
+#pragma unroll
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int m = lane + 32 * m2;
+        int d0 = (int)(((poly[m] + DEC1_OFFSET + DEC1_ROUND) >> sh) & 63u) - 32;
+        int d1 = (int)(((poly[m + 512] + DEC1_OFFSET + DEC1_ROUND) >> sh) & 63u) - 32;
+        v[m2] = fcmul(make_float2((float)d0, (float)d1), T.twist[m2 * 32 + lane]);
+    }
+}
+
+__global__ void __launch_bounds__(128) extprod1_f64_kernel(ExtProdArgs a)
+{
+    __shared__ double2 xp_s[4][512];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int p = blockIdx.x * 4 + w;
+    if (p >= a.B) return;
+    const Fft512Tables &T = *reinterpret_cast<const Fft512Tables *>(a.tables);
+    const uint32_t *in = a.trlwe + (size_t)p * 2 * N1;
+    const double2 *g = reinterpret_cast<const double2 *>(a.trgsw) + (a.shared ? 0 : (size_t)p * 6 * 1024);
+    double2 f0[16], f1[16];
+#pragma unroll 1
+    for (int r = 0; r < 2 * L1; ++r) {
+        double2 v[16];
+        digits_f64(v, in + (r / L1) * N1, r % L1, lane, T);
+        fft512_fwd(v, xp_s[w], T, lane);
+        const double2 *gc = g + (size_t)r * 1024;
+        if (r == 0) {
+#pragma unroll
+            for (int s = 0; s < 16; ++s) {
+                f0[s] = cmul(v[s], gc[(2 * s) * 32 + lane]);
+                f1[s] = cmul(v[s], gc[(2 * s + 1) * 32 + lane]);
+            }
+        } else {
+#pragma unroll
+            for (int s = 0; s < 16; ++s) {
+                cfma(f0[s], v[s], gc[(2 * s) * 32 + lane]);
+                cfma(f1[s], v[s], gc[(2 * s + 1) * 32 + lane]);
+            }
+        }
+    }
+    uint32_t *o = a.out + (size_t)p * 2 * N1;
+    fft512_inv(f0, xp_s[w], T, lane);
+#pragma unroll
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int m = lane + 32 * m2;
+        const double2 y = cmulc(f0[m2], T.twist[m2 * 32 + lane]);
+        o[m] = f64_to_torus32(y.x * (1.0 / 512.0));
+        o[m + 512] = f64_to_torus32(y.y * (1.0 / 512.0));
+    }
+    fft512_inv(f1, xp_s[w], T, lane);
+#pragma unroll
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int m = lane + 32 * m2;
+        const double2 y = cmulc(f1[m2], T.twist[m2 * 32 + lane]);
+        o[N1 + m] = f64_to_torus32(y.x * (1.0 / 512.0));
+        o[N1 + m + 512] = f64_to_torus32(y.y * (1.0 / 512.0));
+    }
+}
+
+__device__ __forceinline__ void store_split(uint32_t *o, float2 hi[16], float2 lo[16], float2 *xp, int lane,
+                                            const Fft512TablesF &T)
+{
+    ffft512_inv(hi, xp, T, lane);
+    ffft512_inv(lo, xp, T, lane);
+#pragma unroll
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int m = lane + 32 * m2;
+        const float2 yh = fcmulc(hi[m2], T.twist[m2 * 32 + lane]);
+        const float2 yl = fcmulc(lo[m2], T.twist[m2 * 32 + lane]);
+        o[m] = ((uint32_t)__float2int_rn(yh.x * (1.0f / 512.0f)) << 24) +
+               (uint32_t)__float2ll_rn(yl.x * (1.0f / 512.0f));
+        o[m + 512] = ((uint32_t)__float2int_rn(yh.y * (1.0f / 512.0f)) << 24) +
+                     (uint32_t)__float2ll_rn(yl.y * (1.0f / 512.0f));
+    }
+}
+
+__global__ void __launch_bounds__(128) extprod1_split_kernel(ExtProdArgs a)
+{
+    __shared__ float2 xp_s[4][512];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int p = blockIdx.x * 4 + w;
+    if (p >= a.B) return;
+    const Fft512TablesF &T = *reinterpret_cast<const Fft512TablesF *>(a.tables);
+    const uint32_t *in = a.trlwe + (size_t)p * 2 * N1;
+    const float4 *g = reinterpret_cast<const float4 *>(a.trgsw) + (a.shared ? 0 : (size_t)p * 6 * 1024);
+    float2 f0h[16], f0l[16], f1h[16], f1l[16];
+#pragma unroll 1
+    for (int r = 0; r < 2 * L1; ++r) {
+        float2 v[16];
+        digits_f32(v, in + (r / L1) * N1, r % L1, lane, T);
+        ffft512_fwd(v, xp_s[w], T, lane);
+        const float4 *gc = g + (size_t)r * 1024;
+        if (r == 0) {
+#pragma unroll
+            for (int s = 0; s < 16; ++s) {
+                const float4 k0 = gc[(2 * s) * 32 + lane], k1 = gc[(2 * s + 1) * 32 + lane];
+                f0h[s] = fcmul(v[s], make_float2(k0.x, k0.y));
+                f0l[s] = fcmul(v[s], make_float2(k0.z, k0.w));
+                f1h[s] = fcmul(v[s], make_float2(k1.x, k1.y));
+                f1l[s] = fcmul(v[s], make_float2(k1.z, k1.w));
+            }
+        } else {
+#pragma unroll
+            for (int s = 0; s < 16; ++s) {
+                const float4 k0 = gc[(2 * s) * 32 + lane], k1 = gc[(2 * s + 1) * 32 + lane];
+                fcfma(f0h[s], v[s], make_float2(k0.x, k0.y));
+                fcfma(f0l[s], v[s], make_float2(k0.z, k0.w));
+                fcfma(f1h[s], v[s], make_float2(k1.x, k1.y));
+                fcfma(f1l[s], v[s], make_float2(k1.z, k1.w));
+            }
+        }
+    }
+    uint32_t *o = a.out + (size_t)p * 2 * N1;
+    store_split(o, f0h, f0l, xp_s[w], lane, T);
+    store_split(o + N1, f1h, f1l, xp_s[w], lane, T);
+}
+
+}  // namespace
+
+cudaError_t launch_extprod1(const ExtProdArgs &a, int precision, cudaStream_t st)
+{
+    if (a.B <= 0) return cudaSuccess;
+    if (precision == 0) extprod1_f64_kernel<<<(a.B + 3) / 4, 128, 0, st>>>(a);
+    else extprod1_split_kernel<<<(a.B + 3) / 4, 128, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace cfdb

@@ -11,6 +11,7 @@
 // cryptographic generator; production keys come from TFHEpp and are loaded
 // with the cufhedb_load_* entry points.
 #include "keys.cuh"
+#include "fft_f32.cuh"
 
 namespace cfdb {
 
@@ -179,6 +180,59 @@ __global__ void bk_permute1_kernel(double2 *dst, const double *src, int rows)
     dst[e] = make_double2(p[idx], p[idx + 512]);
 }
 
+// integer key polynomials [rows][2][1024] -> two limbs hi = round(b / 2^24),
+// lo = b - hi * 2^24, each transformed in FP64 and stored as FP32 in the
+// split-precision chunk layout [rows][16 s][2 o][32 lane] float4(hi, lo)
+__global__ void bk_split1_kernel(float4 *dst, const uint32_t *src, int rows, const Fft512Tables *T)
+{
+    __shared__ double2 xp_s[4][512];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int poly = blockIdx.x * 4 + w;
+    if (poly >= rows * 2) return;
+    const int row = poly >> 1, o = poly & 1;
+    const uint32_t *p = src + (size_t)poly * N1;
+    double2 vh[16], vl[16];
+#pragma unroll
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int m = lane + 32 * m2;
+        const int32_t b0 = (int32_t)p[m], b1 = (int32_t)p[m + 512];
+        const int32_t h0 = (int32_t)(((int64_t)b0 + (1 << 23)) >> 24), h1 = (int32_t)(((int64_t)b1 + (1 << 23)) >> 24);
+        const int32_t l0 = (int32_t)((int64_t)b0 - ((int64_t)h0 << 24)), l1 = (int32_t)((int64_t)b1 - ((int64_t)h1 << 24));
+        vh[m2] = cmul(make_double2((double)h0, (double)h1), T->twist[m2 * 32 + lane]);
+        vl[m2] = cmul(make_double2((double)l0, (double)l1), T->twist[m2 * 32 + lane]);
+    }
+    fft512_fwd(vh, xp_s[w], *T, lane);
+    __syncwarp();
+    fft512_fwd(vl, xp_s[w], *T, lane);
+    float4 *d = dst + (size_t)row * 1024;
+#pragma unroll
+    for (int s = 0; s < 16; ++s)
+        d[(2 * s + o) * 32 + lane] = make_float4((float)vh[s].x, (float)vh[s].y, (float)vl[s].x, (float)vl[s].y);
+}
+
+// FFT-domain key in the FP64 chunk layout -> integer polynomials (the inverse
+// transform, rounded: exact for keys that are transforms of 32-bit integers)
+__global__ void bk_fft1_to_int_kernel(uint32_t *dst, const double2 *src, int rows, const Fft512Tables *T)
+{
+    __shared__ double2 xp_s[4][512];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int poly = blockIdx.x * 4 + w;
+    if (poly >= rows * 2) return;
+    const int row = poly >> 1, o = poly & 1;
+    double2 v[16];
+#pragma unroll
+    for (int s = 0; s < 16; ++s) v[s] = src[(size_t)row * 1024 + (2 * s + o) * 32 + lane];
+    fft512_inv(v, xp_s[w], *T, lane);
+    uint32_t *p = dst + (size_t)poly * N1;
+#pragma unroll
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int m = lane + 32 * m2;
+        const double2 y = cmulc(v[m2], T->twist[m2 * 32 + lane]);
+        p[m] = (uint32_t)__double2ll_rn(y.x * (1.0 / 512.0));
+        p[m + 512] = (uint32_t)__double2ll_rn(y.y * (1.0 / 512.0));
+    }
+}
+
 }  // namespace
 
 cudaError_t gen_ksk(uint32_t *out, int kind, uint64_t seed, const void *key_dom_d, const uint32_t *key_tgt_d,
@@ -239,6 +293,18 @@ cudaError_t encrypt_tlwe64(uint64_t *out, const uint64_t *msg_d, int B, int n, c
 cudaError_t bk01_to_fft(double2 *dst, const uint32_t *src, int rows, const Fft512Tables *T, cudaStream_t st)
 {
     bk_fft1_kernel<<<(rows * 2 + 3) / 4, 128, 0, st>>>(dst, src, rows, T);
+    return cudaGetLastError();
+}
+
+cudaError_t bk01_to_split(float4 *dst, const uint32_t *src, int rows, const Fft512Tables *T, cudaStream_t st)
+{
+    bk_split1_kernel<<<(rows * 2 + 3) / 4, 128, 0, st>>>(dst, src, rows, T);
+    return cudaGetLastError();
+}
+
+cudaError_t bk01_fft_to_int(uint32_t *dst, const double2 *src, int rows, const Fft512Tables *T, cudaStream_t st)
+{
+    bk_fft1_to_int_kernel<<<(rows * 2 + 3) / 4, 128, 0, st>>>(dst, src, rows, T);
     return cudaGetLastError();
 }
 

@@ -32,5 +32,7 @@ cudaError_t encrypt_tlwe64(uint64_t *out, const uint64_t *msg_d, int B, int n, c
                            uint64_t seed, uint64_t stream, uint64_t idx0, cudaStream_t st);
 cudaError_t bk01_to_fft(double2 *dst, const uint32_t *src, int rows, const Fft512Tables *T, cudaStream_t st);
 cudaError_t bkfft01_permute(double2 *dst, const double *src, int rows, cudaStream_t st);
+cudaError_t bk01_to_split(float4 *dst, const uint32_t *src, int rows, const Fft512Tables *T, cudaStream_t st);
+cudaError_t bk01_fft_to_int(uint32_t *dst, const double2 *src, int rows, const Fft512Tables *T, cudaStream_t st);
 
 }  // namespace cfdb

@@ -1,0 +1,227 @@
+// Batched lvl0 -> lvl1 programmable bootstrapping, split-precision FP32 path.
+//
+// Same algorithm as pbs01_f64.cu (TFHEpp GateBootstrappingTLWE2TLWEFFT
+// <lvl01param>, src/gatebootstrapping.cpp:14-23), with every transform and
+// product in FP32.  Precision plan (the 32-bit torus needs products exact to
+// well below the bootstrapping noise, which FP32 alone cannot give):
+//   * each integer key polynomial b is split into limbs
+//       hi = round(b / 2^24) in [-128, 128],  lo = b - hi * 2^24 in [-2^23, 2^23);
+//     both are transformed in FP64 on the device at key-load time and stored
+//     as FP32 frequency values;
+//   * per CMux the 6 digit polynomials (|d| <= 32) are transformed in FP32 and
+//     multiplied into four FP32 accumulators (hi/lo x 2 output polynomials);
+//   * the hi accumulators' inverse transforms are rounded to integers, which is
+//     exact: sum_r d_r * hi_r has rms magnitude ~2^16.7, so FP32 round-off
+//     (~2^-21.5 relative) leaves an error ~0.04, a 12-sigma margin below 1/2;
+//     then hi * 2^24 is taken modulo 2^32;
+//   * the lo accumulators' inverse transforms (rms ~2^32.7) are rounded to
+//     64-bit integers; their FP32 round-off (~2^11) is ~2^-6 of the per-CMux
+//     bootstrapping noise standard deviation (~2^17.8), i.e. it adds about
+//     0.03 % to the noise variance.
+// Kernel layout and key streaming are those of the FP64 kernel; the key ring
+// slots hold (hi, lo) float pairs in the same 16 KB per TRGSW row.
+#include "fft_f32.cuh"
+#include "pbs_common.cuh"
+
+namespace cfdb {
+
+template <int W, int S>
+struct Pbs01SplitSmem {
+    static constexpr int RING_OFF = 128;
+    static constexpr int CHUNK_BYTES = 16384;   // 16 slots x 2 outputs x 32 lanes x float4(hi, lo)
+    static constexpr int TAB_OFF = RING_OFF + S * CHUNK_BYTES;
+    static constexpr int WARP_OFF = TAB_OFF + ((int)sizeof(Fft512TablesF) + 127) / 128 * 128;
+    static constexpr int XP_BYTES = 512 * 8;
+    static constexpr int ACC_BYTES = 2 * N1 * 4;
+    static constexpr int ABAR_BYTES = ((N0 * 2) + 127) / 128 * 128;
+    static constexpr int PER_WARP = XP_BYTES + ACC_BYTES + ABAR_BYTES;
+    static constexpr int TOTAL = WARP_OFF + W * PER_WARP;
+};
+
+__device__ __forceinline__ void load_digit_poly1_f(float2 v[16], const uint32_t *poly, uint32_t abar, int d,
+                                                   int lane, const Fft512TablesF &T)
+{
+    const int sh = 32 - BGBIT1 * (d + 1);
+#pragma unroll
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int m = lane + 32 * m2;
+        uint32_t t0 = rot_coef<N1>(poly, m, abar) - poly[m];
+        uint32_t t1 = rot_coef<N1>(poly, m + 512, abar) - poly[m + 512];
+        int d0 = (int)(((t0 + DEC1_OFFSET + DEC1_ROUND) >> sh) & 63u) - 32;
+        int d1 = (int)(((t1 + DEC1_OFFSET + DEC1_ROUND) >> sh) & 63u) - 32;
+        v[m2] = fcmul(make_float2((float)d0, (float)d1), T.twist[m2 * 32 + lane]);
+    }
+}
+
+// poly[m] += round(a_m) * 2^24 (hi limb, exact) from v[m2] = 512 z_m
+__device__ __forceinline__ void add_inverse_hi(uint32_t *poly, const float2 v[16], int lane, const Fft512TablesF &T)
+{
+#pragma unroll
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int m = lane + 32 * m2;
+        float2 y = fcmulc(v[m2], T.twist[m2 * 32 + lane]);
+        poly[m] += (uint32_t)__float2int_rn(y.x * (1.0f / 512.0f)) << 24;
+        poly[m + 512] += (uint32_t)__float2int_rn(y.y * (1.0f / 512.0f)) << 24;
+    }
+}
+
+// poly[m] += round(a_m) (lo limb, modulo 2^32)
+__device__ __forceinline__ void add_inverse_lo(uint32_t *poly, const float2 v[16], int lane, const Fft512TablesF &T)
+{
+#pragma unroll
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int m = lane + 32 * m2;
+        float2 y = fcmulc(v[m2], T.twist[m2 * 32 + lane]);
+        poly[m] += (uint32_t)__float2ll_rn(y.x * (1.0f / 512.0f));
+        poly[m + 512] += (uint32_t)__float2ll_rn(y.y * (1.0f / 512.0f));
+    }
+}
+
+template <int W, int S>
+__global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_split_kernel(Pbs01Args a)
+{
+    using L = Pbs01SplitSmem<W, S>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+    uint64_t *empty = full + S;
+    float4 *ring = reinterpret_cast<float4 *>(smem + L::RING_OFF);
+    Fft512TablesF *T = reinterpret_cast<Fft512TablesF *>(smem + L::TAB_OFF);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], W);
+        }
+        fence_barrier_init();
+    }
+    {
+        const float4 *src = reinterpret_cast<const float4 *>(a.tables);
+        float4 *dst = reinterpret_cast<float4 *>(T);
+        for (int i = threadIdx.x; i < (int)(sizeof(Fft512TablesF) / 16); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+
+    const int ngroups = (a.B + W - 1) / W;
+    constexpr int CHUNKS = N0 * 2 * L1;
+    const float4 *bk = reinterpret_cast<const float4 *>(a.bk);
+
+    if (warp == W) {
+        if (lane == 0) {
+            uint32_t c = 0;
+            bool ok = true;
+            for (int g = blockIdx.x; g < ngroups && ok; g += gridDim.x) {
+                for (int ch = 0; ch < CHUNKS; ++ch, ++c) {
+                    const int slot = c % S;
+                    if (c >= (uint32_t)S && !mbar_wait(&empty[slot], ((c / S) - 1) & 1)) {
+                        report_error(a.err, DEV_TIMEOUT_EMPTY);
+                        ok = false;
+                        break;
+                    }
+                    mbar_arrive_expect_tx(&full[slot], L::CHUNK_BYTES);
+                    bulk_g2s(ring + slot * 1024, bk + (size_t)ch * 1024, L::CHUNK_BYTES, &full[slot]);
+                }
+            }
+            for (uint32_t k = (c > (uint32_t)S ? c - S : 0); k < c; ++k)
+                if (!mbar_wait(&full[k % S], (k / S) & 1)) report_error(a.err, DEV_TIMEOUT_DRAIN);
+        }
+        return;
+    }
+
+    unsigned char *wb = smem + L::WARP_OFF + warp * L::PER_WARP;
+    float2 *xp = reinterpret_cast<float2 *>(wb);
+    uint32_t *acc = reinterpret_cast<uint32_t *>(wb + L::XP_BYTES);
+    uint16_t *abar_s = reinterpret_cast<uint16_t *>(wb + L::XP_BYTES + L::ACC_BYTES);
+
+    uint32_t c = 0;
+    for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
+        const int ct = g * W + warp;
+        const bool valid = ct < a.B;
+        uint32_t bbar = 2 * N1;
+        if (valid) {
+            const uint32_t *in = a.in + (size_t)ct * (N0 + 1);
+            for (int i = lane; i < N0; i += 32) abar_s[i] = (uint16_t)((in[i] + (1u << 20)) >> 21);
+            bbar = 2 * N1 - (in[N0] >> 21);
+        }
+        for (int j = lane; j < N1; j += 32) {
+            acc[j] = 0;
+            acc[N1 + j] = testvec_rot1(a.tv, j, bbar);
+        }
+        __syncwarp();
+
+        for (int i = 0; i < N0; ++i) {
+            const uint32_t ab = valid ? abar_s[i] : 0u;
+            const bool active = ab != 0;
+            float2 f0h[16], f0l[16], f1h[16], f1l[16];
+#pragma unroll 1
+            for (int r = 0; r < 2 * L1; ++r, ++c) {
+                const int slot = c % S;
+                if (!mbar_wait(&full[slot], (c / S) & 1)) {
+                    report_error(a.err, DEV_TIMEOUT_FULL);
+                    return;
+                }
+                if (active) {
+                    float2 v[16];
+                    load_digit_poly1_f(v, acc + (r / L1) * N1, ab, r % L1, lane, *T);
+                    ffft512_fwd(v, xp, *T, lane);
+                    const float4 *bkc = ring + slot * 1024;
+                    if (r == 0) {
+#pragma unroll
+                        for (int s = 0; s < 16; ++s) {
+                            const float4 k0 = bkc[(2 * s) * 32 + lane], k1 = bkc[(2 * s + 1) * 32 + lane];
+                            f0h[s] = fcmul(v[s], make_float2(k0.x, k0.y));
+                            f0l[s] = fcmul(v[s], make_float2(k0.z, k0.w));
+                            f1h[s] = fcmul(v[s], make_float2(k1.x, k1.y));
+                            f1l[s] = fcmul(v[s], make_float2(k1.z, k1.w));
+                        }
+                    } else {
+#pragma unroll
+                        for (int s = 0; s < 16; ++s) {
+                            const float4 k0 = bkc[(2 * s) * 32 + lane], k1 = bkc[(2 * s + 1) * 32 + lane];
+                            fcfma(f0h[s], v[s], make_float2(k0.x, k0.y));
+                            fcfma(f0l[s], v[s], make_float2(k0.z, k0.w));
+                            fcfma(f1h[s], v[s], make_float2(k1.x, k1.y));
+                            fcfma(f1l[s], v[s], make_float2(k1.z, k1.w));
+                        }
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&empty[slot]);
+            }
+            if (active) {
+                ffft512_inv(f0h, xp, *T, lane);
+                add_inverse_hi(acc, f0h, lane, *T);
+                ffft512_inv(f0l, xp, *T, lane);
+                add_inverse_lo(acc, f0l, lane, *T);
+                ffft512_inv(f1h, xp, *T, lane);
+                add_inverse_hi(acc + N1, f1h, lane, *T);
+                ffft512_inv(f1l, xp, *T, lane);
+                add_inverse_lo(acc + N1, f1l, lane, *T);
+                __syncwarp();
+            }
+        }
+        if (valid) {
+            uint32_t *o = a.out + (size_t)ct * (N1 + 1);
+            for (int j = lane; j < N1; j += 32) o[j] = j == 0 ? acc[0] : (uint32_t)(0u - acc[N1 - j]);
+            if (lane == 0) o[N1] = acc[N1];
+        }
+        __syncwarp();
+    }
+}
+
+constexpr int PBS01S_W = 7, PBS01S_S = 6;
+
+cudaError_t launch_pbs01_split(const Pbs01Args &a, int num_sms, cudaStream_t st)
+{
+    if (a.B <= 0) return cudaSuccess;
+    using L = Pbs01SplitSmem<PBS01S_W, PBS01S_S>;
+    cudaError_t e = cudaFuncSetAttribute(pbs01_split_kernel<PBS01S_W, PBS01S_S>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL);
+    if (e != cudaSuccess) return e;
+    const int groups = (a.B + PBS01S_W - 1) / PBS01S_W;
+    pbs01_split_kernel<PBS01S_W, PBS01S_S>
+        <<<groups < num_sms ? groups : num_sms, (PBS01S_W + 1) * 32, L::TOTAL, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace cfdb

@@ -68,5 +68,7 @@ struct Pbs01Args {
 };
 
 cudaError_t launch_pbs01_f64(const Pbs01Args &a, int num_sms, cudaStream_t st);
+// bk: split-precision key (float4 hi/lo chunk layout), tables: Fft512TablesF
+cudaError_t launch_pbs01_split(const Pbs01Args &a, int num_sms, cudaStream_t st);
 
 }  // namespace cfdb

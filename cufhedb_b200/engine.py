@@ -153,6 +153,32 @@ class Engine:
         check(self.lib.cufhedb_gate_lvl1_noalloc(self.ctx, _lib.GATES[gate], _ptr(ca_dev), _ptr(cb_dev),
                                                  _ptr(out_dev), B, precision, _stream(stream)))
 
+    def trgsw_prepare_lvl1(self, trgsw_dev, out_dev, precision: int = _lib.FP64, stream=None):
+        """integer TRGSWs (B x 6 x 2 x 1024 words) -> prepared frequency-domain
+        TRGSWs (B x 98,304 bytes, e.g. a float64 tensor of B x 12,288)"""
+        B = trgsw_dev.numel() // (2 * L1 * 2 * N1)
+        check(self.lib.cufhedb_trgsw_prepare_lvl1(self.ctx, _ptr(trgsw_dev), _ptr(out_dev), B, precision,
+                                                  _stream(stream)))
+
+    def trgswfft_prepare_lvl1(self, trgswfft_dev, out_dev, stream=None):
+        B = trgswfft_dev.numel() // (2 * L1 * 2 * N1)
+        check(self.lib.cufhedb_trgswfft_prepare_lvl1(self.ctx, _ptr(trgswfft_dev), _ptr(out_dev), B,
+                                                     _stream(stream)))
+
+    def extprod_lvl1(self, trlwe_dev, trgsw_prepared, out_dev, shared: bool = False, precision: int = _lib.FP64,
+                     stream=None):
+        B = trlwe_dev.numel() // (2 * N1)
+        check(self.lib.cufhedb_extprod_lvl1(self.ctx, _ptr(trlwe_dev), _ptr(trgsw_prepared), _ptr(out_dev), B,
+                                            int(shared), precision, _stream(stream)))
+
+    def extprod_lvl1_host(self, trlwe: np.ndarray, trgswfft: np.ndarray, shared: bool = False) -> np.ndarray:
+        trlwe = np.ascontiguousarray(trlwe, np.uint32).reshape(-1, 2, N1)
+        trgswfft = np.ascontiguousarray(trgswfft, np.float64)
+        out = np.zeros_like(trlwe)
+        check(self.lib.cufhedb_extprod_lvl1_host(self.ctx, _ptr(trlwe), _ptr(trgswfft), _ptr(out), trlwe.shape[0],
+                                                 int(shared)))
+        return out
+
     def twist_ifft_lvl1(self, in_dev, out_dev, stream=None):
         B = in_dev.numel() // N1
         check(self.lib.cufhedb_twist_ifft_lvl1(self.ctx, _ptr(in_dev), _ptr(out_dev), B, _stream(stream)))

@@ -165,6 +165,19 @@ CUFHEDB_API int cufhedb_gate_lvl1(cufhedb_ctx *ctx, int gate, const uint32_t *ca
  * call on a device looks the array up (make it before any stream capture). */
 CUFHEDB_API int cufhedb_gate_lvl1_noalloc(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint32_t *cb,
                                           uint32_t *out, int B, int precision, cufhedb_stream_t stream);
+/* Prepared (frequency-domain) TRGSWs for the external product: 98,304 bytes
+ * each, in the engine's layout for the given precision.  From integer
+ * TRGSW<lvl1param> ([6][2][1024] uint32, device memory), or (FP64 only) from
+ * TFHEpp's TRGSWFFT<lvl1param> ([6][2][1024] double, device memory). */
+CUFHEDB_API int cufhedb_trgsw_prepare_lvl1(cufhedb_ctx *ctx, const uint32_t *trgsw, void *out, int B, int precision,
+                                           cufhedb_stream_t stream);
+CUFHEDB_API int cufhedb_trgswfft_prepare_lvl1(cufhedb_ctx *ctx, const double *trgswfft, void *out, int B,
+                                              cufhedb_stream_t stream);
+/* B x trgswfftExternalProduct<lvl1param> (TFHEpp src/trgsw.cpp:77-103; the
+ * reference's ExternalProduct_st, cufft_gpu.cuh:228-248): out_i = trgsw_i (x) trlwe_i,
+ * trlwe / out = B x [2][1024] uint32; `shared` != 0 uses one TRGSW for all. */
+CUFHEDB_API int cufhedb_extprod_lvl1(cufhedb_ctx *ctx, const uint32_t *trlwe, const void *trgsw, uint32_t *out,
+                                     int B, int shared, int precision, cufhedb_stream_t stream);
 /* B TwistIFFT<lvl1param> / TwistFFT<lvl1param> in TFHEpp's frequency layout
  * (include/mulfft.hpp:57-121; the reference's ifft_st / fft_st, cufft_gpu.cuh:187-211) */
 CUFHEDB_API int cufhedb_twist_ifft_lvl1(cufhedb_ctx *ctx, const uint32_t *in, double *out, int B, cufhedb_stream_t stream);
@@ -173,6 +186,9 @@ CUFHEDB_API int cufhedb_twist_fft_lvl1(cufhedb_ctx *ctx, const double *in, uint3
 /* ---- host-buffer entry points (synchronous; the _st calls of cufft_gpu.cuh) ---- */
 CUFHEDB_API int cufhedb_pbs_lvl01_host(cufhedb_ctx *ctx, const uint32_t *in_lvl0, uint32_t *out_lvl1, int B,
                            const cufhedb_testvec *tv, int precision);
+/* host-memory external products with TFHEpp TRGSWFFT<lvl1param> operands (FP64) */
+CUFHEDB_API int cufhedb_extprod_lvl1_host(cufhedb_ctx *ctx, const uint32_t *trlwe, const double *trgswfft,
+                                          uint32_t *out, int B, int shared);
 CUFHEDB_API int cufhedb_gate_lvl1_host(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint32_t *cb, uint32_t *out, int B,
                            int precision);
 

@@ -209,3 +209,64 @@ def test_api_errors(engine):
     assert e.value.code == 2
     fresh.close()
     engine.sync()
+
+
+def test_split32_pbs_decrypts_with_fp64_noise_level(engine, oracle, keys):
+    """Split-precision FP32 path: every output decrypts, and its output noise
+    (phase minus the encoded +-mu) has the variance of the FP64 path's.  The
+    two paths' outputs are not compared with each other: a few-unit difference
+    in the accumulator changes which way the gadget decomposition rounds, so
+    two correct runs carry independent rounding noise.  With 1,029 samples per
+    path the variance ratio of two equal-variance noises lies within
+    [0.88, 1.13] at 95 %; the bound 1.25 leaves room for that spread."""
+    from cufhedb_b200 import FP64, SPLIT32, testvec_const
+    s0, s1, _ = keys
+    B = 7 * 147
+    bits = np.random.default_rng(31).integers(0, 2, B)
+    x = np.stack([oracle.tlwe32(MU if b else (-MU) & 0xFFFFFFFF, s0, NS_LVL0, SEED, 0x52, i) for i, b in enumerate(bits)])
+    xd = dev(x)
+    o64, o32 = empty_dev(B * (N1 + 1)), empty_dev(B * (N1 + 1))
+    engine.pbs_lvl01(xd, o64, testvec_const(MU), FP64)
+    engine.pbs_lvl01(xd, o32, testvec_const(MU), SPLIT32)
+    engine.sync()
+    s1u = s1.astype(np.uint64)
+
+    def phases(o):
+        o = host(o).reshape(B, N1 + 1).astype(np.uint64)
+        ph = (o[:, N1] - (o[:, :N1] @ s1u)) & 0xFFFFFFFF
+        return np.where(ph >= 2 ** 31, ph.astype(np.float64) - 2 ** 32, ph.astype(np.float64))
+
+    p64, p32 = phases(o64), phases(o32)
+    sign = np.where(bits == 1, 1.0, -1.0)
+    assert np.array_equal((p32 > 0).astype(int), bits)
+    assert np.array_equal((p64 > 0).astype(int), bits)
+    n64, n32 = p64 - sign * MU, p32 - sign * MU
+    ratio = np.var(n32) / np.var(n64)
+    assert ratio < 1.25, ratio
+    assert abs(np.mean(n32)) < 4 * np.std(n32) / np.sqrt(B)
+
+
+def test_split32_gates(engine, oracle, keys):
+    from cufhedb_b200 import SPLIT32
+    _, s1, _ = keys
+    B = 96
+    rng = np.random.default_rng(41)
+    a = rng.integers(0, 2, B); b = rng.integers(0, 2, B)
+    enc = lambda bits, base: np.stack([oracle.tlwe32(MU if t else (-MU) & 0xFFFFFFFF, s1, NS_LVL1, SEED, 0x62, base + i)
+                                       for i, t in enumerate(bits)])
+    ca, cb = enc(a, 0), enc(b, 1000)
+    out = empty_dev(B * (N1 + 1))
+    engine.gate_lvl1("NAND", dev(ca), dev(cb), out, SPLIT32)
+    engine.sync()
+    got = np.array([phase(oracle, o, s1) > 0 for o in host(out).reshape(B, N1 + 1)]).astype(int)
+    assert np.array_equal(got, 1 - (a & b))
+
+
+def test_split_key_from_tfhepp_fft_layout(oracle, keys, bkfft01, bk01):
+    """Loading TFHEpp's FFT-domain key recovers the integer key exactly (the
+    split limbs are derived from it) and gives the same PBS as keygen."""
+    from cufhedb_b200 import Engine
+    eng = Engine(0)
+    eng.load_bkfft_lvl01(bkfft01)
+    assert np.array_equal(eng.export_bk_lvl01(), bk01)
+    eng.close()
