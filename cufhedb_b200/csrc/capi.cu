@@ -97,6 +97,7 @@ void build_tables_f(const Fft512Tables &D, Fft512TablesF &F)
     for (int i = 0; i < 512; ++i) {
         F.tw512[i] = make_float2((float)D.tw512[i].x, (float)D.tw512[i].y);
         F.twist[i] = make_float2((float)D.twist[i].x, (float)D.twist[i].y);
+        F.untwist[i] = make_float2((float)(D.twist[i].x / 512.0), (float)(-D.twist[i].y / 512.0));
     }
     for (int j = 0; j < 16; ++j) F.w32[j] = make_float2((float)D.w32[j].x, (float)D.w32[j].y);
 }

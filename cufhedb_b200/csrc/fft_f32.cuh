@@ -12,6 +12,7 @@ namespace cfdb {
 struct Fft512TablesF {
     float2 tw512[512];
     float2 twist[512];
+    float2 untwist[512];   // conj(twist) / 512: inverse untwist and scaling in one product
     float2 w32[16];
 };
 

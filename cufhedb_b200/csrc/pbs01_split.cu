@@ -33,47 +33,56 @@ struct Pbs01SplitSmem {
     static constexpr int WARP_OFF = TAB_OFF + ((int)sizeof(Fft512TablesF) + 127) / 128 * 128;
     static constexpr int XP_BYTES = 512 * 8;
     static constexpr int ACC_BYTES = 2 * N1 * 4;
+    static constexpr int DIG_BYTES = N1 * 4;   // packed digit words of one polynomial
     static constexpr int ABAR_BYTES = ((N0 * 2) + 127) / 128 * 128;
-    static constexpr int PER_WARP = XP_BYTES + ACC_BYTES + ABAR_BYTES;
+    static constexpr int PER_WARP = XP_BYTES + ACC_BYTES + DIG_BYTES + ABAR_BYTES;
     static constexpr int TOTAL = WARP_OFF + W * PER_WARP;
 };
 
-__device__ __forceinline__ void load_digit_poly1_f(float2 v[16], const uint32_t *poly, uint32_t abar, int d,
-                                                   int lane, const Fft512TablesF &T)
+// packed decomposition words of (X^a - 1) * poly, one per coefficient:
+// dig[m] = ((X^a poly - poly)[m] + offset + round) ^ DEC1_XOR
+__device__ __forceinline__ void pack_digits1(uint32_t *dig, const uint32_t *poly, uint32_t abar, int lane)
+{
+#pragma unroll
+    for (int m2 = 0; m2 < 32; ++m2) {
+        const int m = lane + 32 * m2;
+        dig[m] = ((rot_coef<N1>(poly, m, abar) - poly[m]) + DEC1_OFFSET + DEC1_ROUND) ^ DEC1_XOR;
+    }
+}
+
+// digit d of the packed words, twisted: v[m2] = (dig_d(m) + i dig_d(m+512)) * w^m
+__device__ __forceinline__ void load_digit_poly1_f(float2 v[16], const uint32_t *dig, int d, int lane,
+                                                   const Fft512TablesF &T)
 {
     const int sh = 32 - BGBIT1 * (d + 1);
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int m = lane + 32 * m2;
-        uint32_t t0 = rot_coef<N1>(poly, m, abar) - poly[m];
-        uint32_t t1 = rot_coef<N1>(poly, m + 512, abar) - poly[m + 512];
-        int d0 = (int)(((t0 + DEC1_OFFSET + DEC1_ROUND) >> sh) & 63u) - 32;
-        int d1 = (int)(((t1 + DEC1_OFFSET + DEC1_ROUND) >> sh) & 63u) - 32;
+        const int d0 = bfe_s32(dig[m], sh, BGBIT1), d1 = bfe_s32(dig[m + 512], sh, BGBIT1);
         v[m2] = fcmul(make_float2((float)d0, (float)d1), T.twist[m2 * 32 + lane]);
     }
 }
 
-// poly[m] += round(a_m) * 2^24 (hi limb, exact) from v[m2] = 512 z_m
-__device__ __forceinline__ void add_inverse_hi(uint32_t *poly, const float2 v[16], int lane, const Fft512TablesF &T)
+// poly[m] += round(hi_m) * 2^24 + round(lo_m) (mod 2^32); the hi limb rounds
+// exactly, the lo limb's FP32 error stays far below the bootstrapping noise
+__device__ __forceinline__ void add_inverse_split(uint32_t *poly, float2 hi[16], float2 lo[16], float2 *xp, int lane,
+                                                  const Fft512TablesF &T)
 {
+    ffft512_inv(hi, xp, T, lane);
+    uint32_t hv[32];
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
-        const int m = lane + 32 * m2;
-        float2 y = fcmulc(v[m2], T.twist[m2 * 32 + lane]);
-        poly[m] += (uint32_t)__float2int_rn(y.x * (1.0f / 512.0f)) << 24;
-        poly[m + 512] += (uint32_t)__float2int_rn(y.y * (1.0f / 512.0f)) << 24;
+        const float2 y = fcmul(hi[m2], T.untwist[m2 * 32 + lane]);
+        hv[2 * m2] = (uint32_t)__float2int_rn(y.x) << 24;
+        hv[2 * m2 + 1] = (uint32_t)__float2int_rn(y.y) << 24;
     }
-}
-
-// poly[m] += round(a_m) (lo limb, modulo 2^32)
-__device__ __forceinline__ void add_inverse_lo(uint32_t *poly, const float2 v[16], int lane, const Fft512TablesF &T)
-{
+    ffft512_inv(lo, xp, T, lane);
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int m = lane + 32 * m2;
-        float2 y = fcmulc(v[m2], T.twist[m2 * 32 + lane]);
-        poly[m] += (uint32_t)__float2ll_rn(y.x * (1.0f / 512.0f));
-        poly[m + 512] += (uint32_t)__float2ll_rn(y.y * (1.0f / 512.0f));
+        const float2 y = fcmul(lo[m2], T.untwist[m2 * 32 + lane]);
+        poly[m] += hv[2 * m2] + (uint32_t)__float2ll_rn(y.x);
+        poly[m + 512] += hv[2 * m2 + 1] + (uint32_t)__float2ll_rn(y.y);
     }
 }
 
@@ -131,7 +140,8 @@ __global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_split_kernel(Pbs01Args 
     unsigned char *wb = smem + L::WARP_OFF + warp * L::PER_WARP;
     float2 *xp = reinterpret_cast<float2 *>(wb);
     uint32_t *acc = reinterpret_cast<uint32_t *>(wb + L::XP_BYTES);
-    uint16_t *abar_s = reinterpret_cast<uint16_t *>(wb + L::XP_BYTES + L::ACC_BYTES);
+    uint32_t *dig = reinterpret_cast<uint32_t *>(wb + L::XP_BYTES + L::ACC_BYTES);
+    uint16_t *abar_s = reinterpret_cast<uint16_t *>(wb + L::XP_BYTES + L::ACC_BYTES + L::DIG_BYTES);
 
     uint32_t c = 0;
     for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
@@ -161,8 +171,12 @@ __global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_split_kernel(Pbs01Args 
                     return;
                 }
                 if (active) {
+                    if (r % L1 == 0) {
+                        pack_digits1(dig, acc + (r / L1) * N1, ab, lane);
+                        __syncwarp();
+                    }
                     float2 v[16];
-                    load_digit_poly1_f(v, acc + (r / L1) * N1, ab, r % L1, lane, *T);
+                    load_digit_poly1_f(v, dig, r % L1, lane, *T);
                     ffft512_fwd(v, xp, *T, lane);
                     const float4 *bkc = ring + slot * 1024;
                     if (r == 0) {
@@ -189,14 +203,8 @@ __global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_split_kernel(Pbs01Args 
                 if (lane == 0) mbar_arrive(&empty[slot]);
             }
             if (active) {
-                ffft512_inv(f0h, xp, *T, lane);
-                add_inverse_hi(acc, f0h, lane, *T);
-                ffft512_inv(f0l, xp, *T, lane);
-                add_inverse_lo(acc, f0l, lane, *T);
-                ffft512_inv(f1h, xp, *T, lane);
-                add_inverse_hi(acc + N1, f1h, lane, *T);
-                ffft512_inv(f1l, xp, *T, lane);
-                add_inverse_lo(acc + N1, f1l, lane, *T);
+                add_inverse_split(acc, f0h, f0l, xp, lane, *T);
+                add_inverse_split(acc + N1, f1h, f1l, xp, lane, *T);
                 __syncwarp();
             }
         }
@@ -209,12 +217,13 @@ __global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_split_kernel(Pbs01Args 
     }
 }
 
-constexpr int PBS01S_W = 7, PBS01S_S = 6;
+constexpr int PBS01S_W = 7, PBS01S_S = 5;
 
 cudaError_t launch_pbs01_split(const Pbs01Args &a, int num_sms, cudaStream_t st)
 {
     if (a.B <= 0) return cudaSuccess;
     using L = Pbs01SplitSmem<PBS01S_W, PBS01S_S>;
+    static_assert(L::TOTAL <= 227 * 1024, "shared memory budget");
     cudaError_t e = cudaFuncSetAttribute(pbs01_split_kernel<PBS01S_W, PBS01S_S>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL);
     if (e != cudaSuccess) return e;
