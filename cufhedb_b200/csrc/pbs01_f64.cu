@@ -26,32 +26,24 @@ struct Pbs01Smem {
     static constexpr int WARP_OFF = TAB_OFF + ((int)sizeof(Fft512Tables) + 127) / 128 * 128;
     static constexpr int XP_BYTES = 512 * 16;
     static constexpr int ACC_BYTES = 2 * N1 * 4;
-    static constexpr int DIG_BYTES = N1 * 4;   // packed digit words of one polynomial
     static constexpr int ABAR_BYTES = ((N0 * 2) + 127) / 128 * 128;
-    static constexpr int PER_WARP = XP_BYTES + ACC_BYTES + DIG_BYTES + ABAR_BYTES;
+    static constexpr int PER_WARP = XP_BYTES + ACC_BYTES + ABAR_BYTES;
     static constexpr int TOTAL = WARP_OFF + W * PER_WARP;
 };
 
-// packed decomposition words of (X^a - 1) * poly, one per coefficient:
-// dig[m] = ((X^a poly - poly)[m] + offset + round) ^ DEC1_XOR
-__device__ __forceinline__ void pack_digits1_d(uint32_t *dig, const uint32_t *poly, uint32_t abar, int lane)
-{
-#pragma unroll
-    for (int m2 = 0; m2 < 32; ++m2) {
-        const int m = lane + 32 * m2;
-        dig[m] = ((rot_coef<N1>(poly, m, abar) - poly[m]) + DEC1_OFFSET + DEC1_ROUND) ^ DEC1_XOR;
-    }
-}
-
-// digit d, twisted: v[m2] = (dig_d(m) + i dig_d(m+512)) * w^m,  m = lane + 32 m2
-__device__ __forceinline__ void load_digit_poly1(double2 v[16], const uint32_t *dig, int d, int lane,
-                                                 const Fft512Tables &T)
+// digit d of (X^a - 1) * poly at coefficients m and m+512, twisted:
+// v[m2] = (dig_d(m) + i dig_d(m+512)) * w^m,  m = lane + 32 m2.  The signed
+// digit is one bit-field extraction of (t + offset + round) ^ DEC1_XOR.
+__device__ __forceinline__ void load_digit_poly1(double2 v[16], const uint32_t *poly, uint32_t abar, int d, int lane,
+                                        const Fft512Tables &T)
 {
     const int sh = 32 - BGBIT1 * (d + 1);
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int m = lane + 32 * m2;
-        const int d0 = bfe_s32(dig[m], sh, BGBIT1), d1 = bfe_s32(dig[m + 512], sh, BGBIT1);
+        const uint32_t x0 = ((rot_coef<N1>(poly, m, abar) - poly[m]) + DEC1_OFFSET + DEC1_ROUND) ^ DEC1_XOR;
+        const uint32_t x1 = ((rot_coef<N1>(poly, m + 512, abar) - poly[m + 512]) + DEC1_OFFSET + DEC1_ROUND) ^ DEC1_XOR;
+        const int d0 = bfe_s32(x0, sh, BGBIT1), d1 = bfe_s32(x1, sh, BGBIT1);
         v[m2] = cmul(make_double2((double)d0, (double)d1), T.twist[m2 * 32 + lane]);
     }
 }
@@ -124,8 +116,7 @@ __global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_f64_kernel(Pbs01Args a)
     unsigned char *wb = smem + L::WARP_OFF + warp * L::PER_WARP;
     double2 *xp = reinterpret_cast<double2 *>(wb);
     uint32_t *acc = reinterpret_cast<uint32_t *>(wb + L::XP_BYTES);
-    uint32_t *dig = reinterpret_cast<uint32_t *>(wb + L::XP_BYTES + L::ACC_BYTES);
-    uint16_t *abar_s = reinterpret_cast<uint16_t *>(wb + L::XP_BYTES + L::ACC_BYTES + L::DIG_BYTES);
+    uint16_t *abar_s = reinterpret_cast<uint16_t *>(wb + L::XP_BYTES + L::ACC_BYTES);
 
     uint32_t c = 0;
     for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
@@ -155,12 +146,8 @@ __global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_f64_kernel(Pbs01Args a)
                     return;
                 }
                 if (active) {
-                    if (r % L1 == 0) {
-                        pack_digits1_d(dig, acc + (r / L1) * N1, ab, lane);
-                        __syncwarp();
-                    }
                     double2 v[16];
-                    load_digit_poly1(v, dig, r % L1, lane, *T);
+                    load_digit_poly1(v, acc + (r / L1) * N1, ab, r % L1, lane, *T);
                     fft512_fwd(v, xp, *T, lane);
                     const double2 *bkc = ring + slot * 1024;
                     if (r == 0) {
@@ -213,7 +200,7 @@ static cudaError_t launch_pbs01_f64_t(const Pbs01Args &a, int grid, cudaStream_t
 // each SM sub-partition, so every thread may hold 255 registers (the 16
 // complex FFT values plus two 16-complex frequency accumulators per lane);
 // 1,024 ciphertexts map to 147 CTAs, one wave on 148 SMs.
-constexpr int PBS01_W = 7, PBS01_S = 3;
+constexpr int PBS01_W = 7, PBS01_S = 4;
 
 cudaError_t launch_pbs01_f64(const Pbs01Args &a, int num_sms, cudaStream_t st)
 {

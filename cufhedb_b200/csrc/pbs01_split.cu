@@ -33,32 +33,24 @@ struct Pbs01SplitSmem {
     static constexpr int WARP_OFF = TAB_OFF + ((int)sizeof(Fft512TablesF) + 127) / 128 * 128;
     static constexpr int XP_BYTES = 512 * 8;
     static constexpr int ACC_BYTES = 2 * N1 * 4;
-    static constexpr int DIG_BYTES = N1 * 4;   // packed digit words of one polynomial
     static constexpr int ABAR_BYTES = ((N0 * 2) + 127) / 128 * 128;
-    static constexpr int PER_WARP = XP_BYTES + ACC_BYTES + DIG_BYTES + ABAR_BYTES;
+    static constexpr int PER_WARP = XP_BYTES + ACC_BYTES + ABAR_BYTES;
     static constexpr int TOTAL = WARP_OFF + W * PER_WARP;
 };
 
-// packed decomposition words of (X^a - 1) * poly, one per coefficient:
-// dig[m] = ((X^a poly - poly)[m] + offset + round) ^ DEC1_XOR
-__device__ __forceinline__ void pack_digits1(uint32_t *dig, const uint32_t *poly, uint32_t abar, int lane)
-{
-#pragma unroll
-    for (int m2 = 0; m2 < 32; ++m2) {
-        const int m = lane + 32 * m2;
-        dig[m] = ((rot_coef<N1>(poly, m, abar) - poly[m]) + DEC1_OFFSET + DEC1_ROUND) ^ DEC1_XOR;
-    }
-}
-
-// digit d of the packed words, twisted: v[m2] = (dig_d(m) + i dig_d(m+512)) * w^m
-__device__ __forceinline__ void load_digit_poly1_f(float2 v[16], const uint32_t *dig, int d, int lane,
-                                                   const Fft512TablesF &T)
+// digit d of (X^a - 1) * poly at coefficients m and m+512, twisted:
+// v[m2] = (dig_d(m) + i dig_d(m+512)) * w^m,  m = lane + 32 m2.  The signed
+// digit is one bit-field extraction of (t + offset + round) ^ DEC1_XOR.
+__device__ __forceinline__ void load_digit_poly1_f(float2 v[16], const uint32_t *poly, uint32_t abar, int d, int lane,
+                                        const Fft512TablesF &T)
 {
     const int sh = 32 - BGBIT1 * (d + 1);
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int m = lane + 32 * m2;
-        const int d0 = bfe_s32(dig[m], sh, BGBIT1), d1 = bfe_s32(dig[m + 512], sh, BGBIT1);
+        const uint32_t x0 = ((rot_coef<N1>(poly, m, abar) - poly[m]) + DEC1_OFFSET + DEC1_ROUND) ^ DEC1_XOR;
+        const uint32_t x1 = ((rot_coef<N1>(poly, m + 512, abar) - poly[m + 512]) + DEC1_OFFSET + DEC1_ROUND) ^ DEC1_XOR;
+        const int d0 = bfe_s32(x0, sh, BGBIT1), d1 = bfe_s32(x1, sh, BGBIT1);
         v[m2] = fcmul(make_float2((float)d0, (float)d1), T.twist[m2 * 32 + lane]);
     }
 }
@@ -140,8 +132,7 @@ __global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_split_kernel(Pbs01Args 
     unsigned char *wb = smem + L::WARP_OFF + warp * L::PER_WARP;
     float2 *xp = reinterpret_cast<float2 *>(wb);
     uint32_t *acc = reinterpret_cast<uint32_t *>(wb + L::XP_BYTES);
-    uint32_t *dig = reinterpret_cast<uint32_t *>(wb + L::XP_BYTES + L::ACC_BYTES);
-    uint16_t *abar_s = reinterpret_cast<uint16_t *>(wb + L::XP_BYTES + L::ACC_BYTES + L::DIG_BYTES);
+    uint16_t *abar_s = reinterpret_cast<uint16_t *>(wb + L::XP_BYTES + L::ACC_BYTES);
 
     uint32_t c = 0;
     for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
@@ -171,12 +162,8 @@ __global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_split_kernel(Pbs01Args 
                     return;
                 }
                 if (active) {
-                    if (r % L1 == 0) {
-                        pack_digits1(dig, acc + (r / L1) * N1, ab, lane);
-                        __syncwarp();
-                    }
                     float2 v[16];
-                    load_digit_poly1_f(v, dig, r % L1, lane, *T);
+                    load_digit_poly1_f(v, acc + (r / L1) * N1, ab, r % L1, lane, *T);
                     ffft512_fwd(v, xp, *T, lane);
                     const float4 *bkc = ring + slot * 1024;
                     if (r == 0) {
@@ -217,7 +204,7 @@ __global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_split_kernel(Pbs01Args 
     }
 }
 
-constexpr int PBS01S_W = 7, PBS01S_S = 5;
+constexpr int PBS01S_W = 7, PBS01S_S = 6;
 
 cudaError_t launch_pbs01_split(const Pbs01Args &a, int num_sms, cudaStream_t st)
 {
