@@ -44,6 +44,15 @@ SIGNATURES = {
     "cufhedb_load_bkfft_lvl01": [_vp, _vp],
     "cufhedb_load_bk_lvl01": [_vp, _vp],
     "cufhedb_load_ksk": [_vp, _i32, _vp],
+    "cufhedb_load_bk_lvl02": [_vp, _vp],
+    "cufhedb_load_bkfft_lvl02": [_vp, _vp],
+    "cufhedb_export_bk_lvl02": [_vp, _vp],
+    "cufhedb_pbs_lvl02": [_vp, _vp, _vp, _i32, C.POINTER(TestVec), _vp],
+    "cufhedb_trgsw_prepare_lvl2": [_vp, _vp, _vp, _i32, _vp],
+    "cufhedb_trgswfft_prepare_lvl2": [_vp, _vp, _vp, _i32, _vp],
+    "cufhedb_extprod_lvl2": [_vp, _vp, _vp, _vp, _i32, _i32, _vp],
+    "cufhedb_twist_ifft_lvl2": [_vp, _vp, _vp, _i32, _vp],
+    "cufhedb_twist_fft_lvl2": [_vp, _vp, _vp, _i32, _vp],
     "cufhedb_keygen": [_vp, _u64, C.c_uint],
     "cufhedb_export_bk_lvl01": [_vp, _vp],
     "cufhedb_export_ksk_rows": [_vp, _i32, _vp, _i32, _vp],

@@ -12,6 +12,7 @@
 #include "fftops.cuh"
 #include "iks.cuh"
 #include "keys.cuh"
+#include "lvl2.cuh"
 #include "pbs_common.cuh"
 
 using namespace cfdb;
@@ -22,6 +23,9 @@ struct cufhedb_ctx {
     Fft512Tables *tab512 = nullptr;   // device copy of the lvl1 transform tables
     Fft512TablesF *tab512f = nullptr; // the same tables in FP32 (split-precision path)
     float4 *bk01_split = nullptr;     // split-precision lvl01 key (hi/lo limbs, FP32)
+    Fft1024Tables *tab1024 = nullptr; // lvl2 transform tables
+    double2 *bk02 = nullptr;          // FFT-domain lvl02 key, chunk layout
+    uint64_t *bk02_int = nullptr;     // integer lvl02 key (when loaded or generated)
     double2 *bk01 = nullptr;          // FFT-domain lvl01 key, chunk layout
     uint32_t *bk01_int = nullptr;     // integer lvl01 key (when loaded or generated)
     uint32_t *ksk[3] = {nullptr, nullptr, nullptr};   // lvl10, lvl20, lvl21
@@ -62,6 +66,8 @@ int cuda_fail(cudaError_t e, const char *what)
 
 constexpr size_t BK01_ROWS = (size_t)N0 * 2 * L1;   // TRGSW rows of the lvl01 key
 constexpr size_t BK01_WORDS = BK01_ROWS * 2 * N1;
+constexpr size_t BK02_ROWS = (size_t)N0 * 2 * L2;   // TRGSW rows of the lvl02 key
+constexpr size_t BK02_WORDS = BK02_ROWS * 2 * N2;
 
 size_t ksk_words(int kind)
 {
@@ -89,6 +95,26 @@ void build_tables(Fft512Tables &T)
     for (int j = 0; j < 16; ++j) {
         const long double a = 2.0L * PI * (long double)j / 32.0L;
         T.w32[j] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+}
+
+void build_tables2(Fft1024Tables &T)
+{
+    const long double PI = 3.141592653589793238462643383279502884L;
+    for (int q2 = 0; q2 < 16; ++q2)
+        for (int m1 = 0; m1 < 64; ++m1) {
+            const long double a = 2.0L * PI * (long double)((m1 * q2) % 1024) / 1024.0L;
+            T.tw1024[q2 * 64 + m1] = make_double2((double)cosl(a), (double)sinl(a));
+        }
+    for (int m2 = 0; m2 < 16; ++m2)
+        for (int m1 = 0; m1 < 64; ++m1) {
+            const long double a = 2.0L * PI * (long double)(m1 + 64 * m2) / 4096.0L;
+            T.twist[m2 * 64 + m1] = make_double2((double)cosl(a), (double)sinl(a));
+        }
+    for (int j = 0; j < 16; ++j) {
+        const long double a = 2.0L * PI * (long double)j / 32.0L, b = 2.0L * PI * (long double)j / 64.0L;
+        T.w32[j] = make_double2((double)cosl(a), (double)sinl(a));
+        T.w64[j] = make_double2((double)cosl(b), (double)sinl(b));
     }
 }
 
@@ -252,6 +278,11 @@ int cufhedb_ctx_create(cufhedb_ctx **out, int device)
     build_tables_f(host_tab, host_tabf);
     cudaError_t e = cudaMalloc((void **)&ctx->tab512, sizeof(Fft512Tables));
     if (e == cudaSuccess) e = cudaMemcpy(ctx->tab512, &host_tab, sizeof(Fft512Tables), cudaMemcpyHostToDevice);
+    Fft1024Tables *host_tab2 = new Fft1024Tables;
+    build_tables2(*host_tab2);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&ctx->tab1024, sizeof(Fft1024Tables));
+    if (e == cudaSuccess) e = cudaMemcpy(ctx->tab1024, host_tab2, sizeof(Fft1024Tables), cudaMemcpyHostToDevice);
+    delete host_tab2;
     if (e == cudaSuccess) e = cudaMalloc((void **)&ctx->tab512f, sizeof(Fft512TablesF));
     if (e == cudaSuccess) e = cudaMemcpy(ctx->tab512f, &host_tabf, sizeof(Fft512TablesF), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc((void **)&ctx->err, sizeof(int));
@@ -272,6 +303,9 @@ int cufhedb_ctx_destroy(cufhedb_ctx *ctx)
     if (ctx->io) cudaStreamSynchronize(ctx->io);
     cudaFree(ctx->tab512);
     cudaFree(ctx->tab512f);
+    cudaFree(ctx->tab1024);
+    cudaFree(ctx->bk02);
+    cudaFree(ctx->bk02_int);
     cudaFree(ctx->bk01);
     cudaFree(ctx->bk01_split);
     cudaFree(ctx->bk01_int);
@@ -412,6 +446,25 @@ int cufhedb_keygen(cufhedb_ctx *ctx, uint64_t seed, unsigned flags)
         rc = prepare_split01(ctx);
         if (rc) return rc;
     }
+    if (flags & CUFHEDB_GEN_BK02) {
+        std::vector<int> pos;
+        for (int i = 0; i < N2; ++i)
+            if (s2[i]) pos.push_back(i);
+        int *pos_d = nullptr;
+        CK(cudaMalloc((void **)&pos_d, pos.size() * sizeof(int)));
+        cudaError_t e = cudaMemcpy(pos_d, pos.data(), pos.size() * sizeof(int), cudaMemcpyHostToDevice);
+        rc = ensure_alloc((void **)&ctx->bk02_int, BK02_WORDS * sizeof(uint64_t));
+        if (!rc) rc = ensure_alloc((void **)&ctx->bk02, BK02_ROWS * 2 * 1024 * sizeof(double2));
+        if (rc) {
+            cudaFree(pos_d);
+            return rc;
+        }
+        if (e == cudaSuccess) e = gen_bk02(ctx->bk02_int, seed, ctx->s0_d, pos_d, (int)pos.size(), 0);
+        if (e == cudaSuccess) e = bk02_to_fft(ctx->bk02, ctx->bk02_int, (int)BK02_ROWS, ctx->tab1024, 0);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        cudaFree(pos_d);
+        if (e != cudaSuccess) return cuda_fail(e, "keygen bk02");
+    }
     const int kinds[3] = {10, 20, 21};
     const unsigned kflags[3] = {CUFHEDB_GEN_KSK10, CUFHEDB_GEN_KSK20, CUFHEDB_GEN_KSK21};
     for (int t = 0; t < 3; ++t) {
@@ -432,6 +485,44 @@ int cufhedb_export_bk_lvl01(cufhedb_ctx *ctx, uint32_t *bk)
     if (!ctx->bk01_int) return fail(CUFHEDB_ERR_NOKEY, "no integer lvl01 key on the device");
     DeviceGuard g(ctx->device);
     CK(cudaMemcpy(bk, ctx->bk01_int, BK01_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    return CUFHEDB_OK;
+}
+
+int cufhedb_load_bk_lvl02(cufhedb_ctx *ctx, const uint64_t *bk)
+{
+    NEED(ctx && bk, "null argument");
+    DeviceGuard g(ctx->device);
+    int rc = ensure_alloc((void **)&ctx->bk02, BK02_ROWS * 2 * 1024 * sizeof(double2));
+    if (!rc) rc = ensure_alloc((void **)&ctx->bk02_int, BK02_WORDS * sizeof(uint64_t));
+    if (rc) return rc;
+    CK(cudaMemcpy(ctx->bk02_int, bk, BK02_WORDS * sizeof(uint64_t), cudaMemcpyHostToDevice));
+    CK(bk02_to_fft(ctx->bk02, ctx->bk02_int, (int)BK02_ROWS, ctx->tab1024, 0));
+    CK(cudaDeviceSynchronize());
+    return CUFHEDB_OK;
+}
+
+int cufhedb_load_bkfft_lvl02(cufhedb_ctx *ctx, const double *bkfft)
+{
+    NEED(ctx && bkfft, "null argument");
+    DeviceGuard g(ctx->device);
+    int rc = ensure_alloc((void **)&ctx->bk02, BK02_ROWS * 2 * 1024 * sizeof(double2));
+    if (rc) return rc;
+    double *tmp = nullptr;
+    CK(cudaMalloc((void **)&tmp, BK02_WORDS * sizeof(double)));
+    cudaError_t e = cudaMemcpy(tmp, bkfft, BK02_WORDS * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = bkfft02_permute(ctx->bk02, tmp, (int)BK02_ROWS, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    cudaFree(tmp);
+    if (e != cudaSuccess) return cuda_fail(e, "load_bkfft_lvl02");
+    return CUFHEDB_OK;
+}
+
+int cufhedb_export_bk_lvl02(cufhedb_ctx *ctx, uint64_t *bk)
+{
+    NEED(ctx && bk, "null argument");
+    if (!ctx->bk02_int) return fail(CUFHEDB_ERR_NOKEY, "no integer lvl02 key on the device");
+    DeviceGuard g(ctx->device);
+    CK(cudaMemcpy(bk, ctx->bk02_int, BK02_WORDS * sizeof(uint64_t), cudaMemcpyDeviceToHost));
     return CUFHEDB_OK;
 }
 
@@ -571,6 +662,94 @@ int cufhedb_extprod_lvl1(cufhedb_ctx *ctx, const uint32_t *trlwe, const void *tr
     a.shared = shared ? 1 : 0;
     a.tables = precision == CUFHEDB_FP64 ? (const void *)ctx->tab512 : (const void *)ctx->tab512f;
     CK(launch_extprod1(a, precision == CUFHEDB_FP64 ? 0 : 1, (cudaStream_t)stream));
+    return CUFHEDB_OK;
+}
+
+static int pbs02_enqueue(cufhedb_ctx *ctx, const uint32_t *in, uint64_t *out, int B, const cufhedb_testvec *tv,
+                         cudaStream_t st)
+{
+    if (!ctx->bk02) return fail(CUFHEDB_ERR_NOKEY, "lvl02 bootstrapping key not loaded");
+    Pbs02Args a{};
+    a.in = in;
+    a.out = out;
+    a.B = B;
+    a.bk = ctx->bk02;
+    a.tables = ctx->tab1024;
+    a.tv = to_tv(tv);
+    a.err = ctx->err;
+    CK(launch_pbs02_f64(a, ctx->num_sms, st));
+    return CUFHEDB_OK;
+}
+
+int cufhedb_pbs_lvl02(cufhedb_ctx *ctx, const uint32_t *in_lvl0, uint64_t *out_lvl2, int B, const cufhedb_testvec *tv,
+                      cufhedb_stream_t stream)
+{
+    NEED(ctx != nullptr, "ctx is null");
+    NEED(B >= 0, "negative batch");
+    if (B == 0) return CUFHEDB_OK;
+    NEED(in_lvl0 && out_lvl2, "null buffer");
+    int rc = check_tv(tv, N2);
+    if (rc) return rc;
+    DeviceGuard g(ctx->device);
+    return pbs02_enqueue(ctx, in_lvl0, out_lvl2, B, tv, (cudaStream_t)stream);
+}
+
+int cufhedb_trgsw_prepare_lvl2(cufhedb_ctx *ctx, const uint64_t *trgsw, void *out, int B, cufhedb_stream_t stream)
+{
+    NEED(ctx && B >= 0, "bad argument");
+    if (B == 0) return CUFHEDB_OK;
+    NEED(trgsw && out, "null buffer");
+    DeviceGuard g(ctx->device);
+    CK(bk02_to_fft((double2 *)out, trgsw, B * 2 * L2, ctx->tab1024, (cudaStream_t)stream));
+    return CUFHEDB_OK;
+}
+
+int cufhedb_trgswfft_prepare_lvl2(cufhedb_ctx *ctx, const double *trgswfft, void *out, int B,
+                                  cufhedb_stream_t stream)
+{
+    NEED(ctx && B >= 0, "bad argument");
+    if (B == 0) return CUFHEDB_OK;
+    NEED(trgswfft && out, "null buffer");
+    DeviceGuard g(ctx->device);
+    CK(bkfft02_permute((double2 *)out, trgswfft, B * 2 * L2, (cudaStream_t)stream));
+    return CUFHEDB_OK;
+}
+
+int cufhedb_extprod_lvl2(cufhedb_ctx *ctx, const uint64_t *trlwe, const void *trgsw, uint64_t *out, int B,
+                         int shared, cufhedb_stream_t stream)
+{
+    NEED(ctx && B >= 0, "bad argument");
+    if (B == 0) return CUFHEDB_OK;
+    NEED(trlwe && trgsw && out, "null buffer");
+    DeviceGuard g(ctx->device);
+    ExtProd2Args a{};
+    a.trlwe = trlwe;
+    a.trgsw = (const double2 *)trgsw;
+    a.out = out;
+    a.B = B;
+    a.shared = shared ? 1 : 0;
+    a.tables = ctx->tab1024;
+    CK(launch_extprod2(a, (cudaStream_t)stream));
+    return CUFHEDB_OK;
+}
+
+int cufhedb_twist_ifft_lvl2(cufhedb_ctx *ctx, const uint64_t *in, double *out, int B, cufhedb_stream_t stream)
+{
+    NEED(ctx && B >= 0, "bad argument");
+    if (B == 0) return CUFHEDB_OK;
+    NEED(in && out, "null buffer");
+    DeviceGuard g(ctx->device);
+    CK(launch_twist_ifft2(out, in, B, ctx->tab1024, (cudaStream_t)stream));
+    return CUFHEDB_OK;
+}
+
+int cufhedb_twist_fft_lvl2(cufhedb_ctx *ctx, const double *in, uint64_t *out, int B, cufhedb_stream_t stream)
+{
+    NEED(ctx && B >= 0, "bad argument");
+    if (B == 0) return CUFHEDB_OK;
+    NEED(in && out, "null buffer");
+    DeviceGuard g(ctx->device);
+    CK(launch_twist_fft2(out, in, B, ctx->tab1024, (cudaStream_t)stream));
     return CUFHEDB_OK;
 }
 

@@ -179,6 +179,46 @@ class Engine:
                                                  int(shared)))
         return out
 
+    # ---- lvl2 (64-bit torus, N = 2048), FP64 -----------------------------------
+    def load_bk_lvl02(self, bk: np.ndarray):
+        bk = np.ascontiguousarray(bk, np.uint64)
+        check(self.lib.cufhedb_load_bk_lvl02(self.ctx, _ptr(bk)))
+
+    def load_bkfft_lvl02(self, bkfft: np.ndarray):
+        bkfft = np.ascontiguousarray(bkfft, np.float64)
+        check(self.lib.cufhedb_load_bkfft_lvl02(self.ctx, _ptr(bkfft)))
+
+    def export_bk_lvl02(self) -> np.ndarray:
+        out = np.zeros((N0, 2 * L2, 2, N2), np.uint64)
+        check(self.lib.cufhedb_export_bk_lvl02(self.ctx, _ptr(out)))
+        return out
+
+    def pbs_lvl02(self, in_dev, out_dev, tv: _lib.TestVec, stream=None):
+        B = in_dev.numel() // (N0 + 1)
+        check(self.lib.cufhedb_pbs_lvl02(self.ctx, _ptr(in_dev), _ptr(out_dev), B, C.byref(tv), _stream(stream)))
+
+    def trgsw_prepare_lvl2(self, trgsw_dev, out_dev, stream=None):
+        B = trgsw_dev.numel() // (2 * L2 * 2 * N2)
+        check(self.lib.cufhedb_trgsw_prepare_lvl2(self.ctx, _ptr(trgsw_dev), _ptr(out_dev), B, _stream(stream)))
+
+    def trgswfft_prepare_lvl2(self, trgswfft_dev, out_dev, stream=None):
+        B = trgswfft_dev.numel() // (2 * L2 * 2 * N2)
+        check(self.lib.cufhedb_trgswfft_prepare_lvl2(self.ctx, _ptr(trgswfft_dev), _ptr(out_dev), B,
+                                                     _stream(stream)))
+
+    def extprod_lvl2(self, trlwe_dev, trgsw_prepared, out_dev, shared: bool = False, stream=None):
+        B = trlwe_dev.numel() // (2 * N2)
+        check(self.lib.cufhedb_extprod_lvl2(self.ctx, _ptr(trlwe_dev), _ptr(trgsw_prepared), _ptr(out_dev), B,
+                                            int(shared), _stream(stream)))
+
+    def twist_ifft_lvl2(self, in_dev, out_dev, stream=None):
+        B = in_dev.numel() // N2
+        check(self.lib.cufhedb_twist_ifft_lvl2(self.ctx, _ptr(in_dev), _ptr(out_dev), B, _stream(stream)))
+
+    def twist_fft_lvl2(self, in_dev, out_dev, stream=None):
+        B = in_dev.numel() // N2
+        check(self.lib.cufhedb_twist_fft_lvl2(self.ctx, _ptr(in_dev), _ptr(out_dev), B, _stream(stream)))
+
     def twist_ifft_lvl1(self, in_dev, out_dev, stream=None):
         B = in_dev.numel() // N1
         check(self.lib.cufhedb_twist_ifft_lvl1(self.ctx, _ptr(in_dev), _ptr(out_dev), B, _stream(stream)))

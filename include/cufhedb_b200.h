@@ -121,6 +121,10 @@ CUFHEDB_API int cufhedb_sync(cufhedb_ctx *ctx, cufhedb_stream_t stream);
 CUFHEDB_API int cufhedb_load_bkfft_lvl01(cufhedb_ctx *ctx, const double *bkfft);
 /* integer BootstrappingKey<lvl01param> (TFHEpp bkgen output), host memory */
 CUFHEDB_API int cufhedb_load_bk_lvl01(cufhedb_ctx *ctx, const uint32_t *bk);
+/* the lvl02 key: integer BootstrappingKey<lvl02param> or TFHEpp
+ * BootstrappingKeyFFT<lvl02param> (cufftlvl2.LoadBK), host memory */
+CUFHEDB_API int cufhedb_load_bk_lvl02(cufhedb_ctx *ctx, const uint64_t *bk);
+CUFHEDB_API int cufhedb_load_bkfft_lvl02(cufhedb_ctx *ctx, const double *bkfft);
 /* KeySwitchingKey<lvl10/20/21param>, host memory; kind is cufhedb_ksk_kind.
  * Replaces the host-resident key TFHEpp::IdentityKeySwitch reads (EvalKey::iksklvl*). */
 CUFHEDB_API int cufhedb_load_ksk(cufhedb_ctx *ctx, int kind, const uint32_t *ksk);
@@ -133,6 +137,7 @@ CUFHEDB_API int cufhedb_keygen(cufhedb_ctx *ctx, uint64_t seed, unsigned flags);
  * the integer lvl01 key (when loaded with cufhedb_load_bk_lvl01 or generated),
  * and n rows of a key-switching key (row = (i*t + j)*(2^basebit-1) + k) */
 CUFHEDB_API int cufhedb_export_bk_lvl01(cufhedb_ctx *ctx, uint32_t *bk);
+CUFHEDB_API int cufhedb_export_bk_lvl02(cufhedb_ctx *ctx, uint64_t *bk);
 CUFHEDB_API int cufhedb_export_ksk_rows(cufhedb_ctx *ctx, int kind, const uint64_t *rows, int n, uint32_t *out);
 /* the secret keys of the deterministic key set (host-only computation) */
 CUFHEDB_API int cufhedb_secret_keys(uint64_t seed, uint32_t *s0, uint32_t *s1, uint64_t *s2);
@@ -146,6 +151,10 @@ CUFHEDB_API int cufhedb_encrypt_lvl1(cufhedb_ctx *ctx, uint64_t seed, uint64_t s
  * TFHEpp src/gatebootstrapping.cpp:14-23): lvl0 TLWE in, lvl1 TLWE out */
 CUFHEDB_API int cufhedb_pbs_lvl01(cufhedb_ctx *ctx, const uint32_t *in_lvl0, uint32_t *out_lvl1, int B,
                       const cufhedb_testvec *tv, int precision, cufhedb_stream_t stream);
+/* B x GateBootstrappingTLWE2TLWEFFT<lvl02param> (FP64): lvl0 TLWE in, lvl2
+ * TLWE (2049 x uint64) out; test vectors of 2048 64-bit words */
+CUFHEDB_API int cufhedb_pbs_lvl02(cufhedb_ctx *ctx, const uint32_t *in_lvl0, uint64_t *out_lvl2, int B,
+                                  const cufhedb_testvec *tv, cufhedb_stream_t stream);
 /* B x IdentityKeySwitch<lvl10/20/21param> (TFHEpp src/keyswitch.cpp:11-48).
  * kind 10: in = B x 1025 uint32; kinds 20, 21: in = B x 2049 uint64.
  * out = B x 673 (10, 20) or B x 1025 (21) uint32. */
@@ -178,6 +187,20 @@ CUFHEDB_API int cufhedb_trgswfft_prepare_lvl1(cufhedb_ctx *ctx, const double *tr
  * trlwe / out = B x [2][1024] uint32; `shared` != 0 uses one TRGSW for all. */
 CUFHEDB_API int cufhedb_extprod_lvl1(cufhedb_ctx *ctx, const uint32_t *trlwe, const void *trgsw, uint32_t *out,
                                      int B, int shared, int precision, cufhedb_stream_t stream);
+/* lvl2 external products (FP64): prepared TRGSWs are 262,144 bytes each,
+ * from integer TRGSW<lvl2param> ([8][2][2048] uint64) or TFHEpp's
+ * TRGSWFFT<lvl2param> ([8][2][2048] double); trlwe / out = B x [2][2048] uint64 */
+CUFHEDB_API int cufhedb_trgsw_prepare_lvl2(cufhedb_ctx *ctx, const uint64_t *trgsw, void *out, int B,
+                                           cufhedb_stream_t stream);
+CUFHEDB_API int cufhedb_trgswfft_prepare_lvl2(cufhedb_ctx *ctx, const double *trgswfft, void *out, int B,
+                                              cufhedb_stream_t stream);
+CUFHEDB_API int cufhedb_extprod_lvl2(cufhedb_ctx *ctx, const uint64_t *trlwe, const void *trgsw, uint64_t *out,
+                                     int B, int shared, cufhedb_stream_t stream);
+/* B TwistIFFT<lvl2param> / TwistFFT<lvl2param>, TFHEpp layout */
+CUFHEDB_API int cufhedb_twist_ifft_lvl2(cufhedb_ctx *ctx, const uint64_t *in, double *out, int B,
+                                        cufhedb_stream_t stream);
+CUFHEDB_API int cufhedb_twist_fft_lvl2(cufhedb_ctx *ctx, const double *in, uint64_t *out, int B,
+                                       cufhedb_stream_t stream);
 /* B TwistIFFT<lvl1param> / TwistFFT<lvl1param> in TFHEpp's frequency layout
  * (include/mulfft.hpp:57-121; the reference's ifft_st / fft_st, cufft_gpu.cuh:187-211) */
 CUFHEDB_API int cufhedb_twist_ifft_lvl1(cufhedb_ctx *ctx, const uint32_t *in, double *out, int B, cufhedb_stream_t stream);
