@@ -48,6 +48,10 @@ def parse():
     p.add_argument("--batch", type=int, default=1024)
     p.add_argument("--precision", choices=["fp64", "split32"], default="fp64")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--filter-rows", type=int, default=0,
+                   help="also time the encrypted range filter (20-bit lvl2 column, x <= c at the 30th "
+                        "percentile) over this many rows and report filter rows/s")
+    p.add_argument("--filter-only", action="store_true", help="run only the range-filter measurement")
     p.add_argument("--profile-pbs", action="store_true",
                    help="run only the lvl01 PBS kernel on `--batch` random lvl0 inputs (lvl01 key only, "
                         "~0.1 GB on the device): the small case for ncu captures")
@@ -338,6 +342,56 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def range_filter(eng, rows: int, precision: int, steps: int = 1):
+    """Encrypted range filter x <= c over a synthetic 20-bit column at lvl2
+    (the reference's HomComp / TPC-H filter shape: less_than_equal<Lvl2>, 6 lvl02
+    + 3 lvl01 bootstraps and 10 key switches per row).  Returns (rows/s, ms per
+    pass, decrypt errors, bootstraps per row)."""
+    import numpy as np
+    import torch
+    from cufhedb_b200 import Engine
+    pb = 20
+    g = torch.Generator().manual_seed(77)
+    x = torch.randint(0, 2 ** pb, (rows,), generator=g).numpy().astype(np.uint64)
+    c = int(np.percentile(x, 30))
+    shift = np.uint64(64 - pb - 1)
+    msg = torch.from_numpy((x << shift).view(np.int64)).cuda()
+    thr = torch.from_numpy((np.full(rows, c, np.uint64) << shift).view(np.int64)).cuda()
+    c1 = torch.empty(rows * 2049, dtype=torch.int64, device="cuda")
+    c2 = torch.empty_like(c1)
+    eng.encrypt_lvl2(SEED, 0x7A, 0, msg, c1)
+    eng.encrypt_lvl2(SEED, 0x7A, rows, thr, c2)
+    out = torch.empty(rows * (N1 + 1), dtype=torch.int32, device="cuda")
+    eng.compare("le", 2, c1, c2, out, pb, True, precision)   # warm-up (and pool growth)
+    eng.sync()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for e0, e1 in ev:
+        e0.record()
+        eng.compare("le", 2, c1, c2, out, pb, True, precision)
+        e1.record()
+    eng.sync()
+    ms = statistics.median(e0.elapsed_time(e1) for e0, e1 in ev)
+    _, s1, _ = Engine.secret_keys(SEED)
+    o = out.cpu().numpy().view(np.uint32).reshape(rows, N1 + 1).astype(np.uint64)
+    ph = (o[:, N1] - (o[:, :N1] @ s1.astype(np.uint64))) & 0xFFFFFFFF
+    dec = ((ph > 0) & (ph < 2 ** 31)).astype(int)
+    errors = int(np.sum(dec != (x <= c).astype(int)))
+    return rows / (ms / 1000.0), ms, errors
+
+
+def run_filter_only(args):
+    from cufhedb_b200 import FP64, GEN_ALL, SPLIT32, Engine
+    prec = FP64 if args.precision == "fp64" else SPLIT32
+    eng = Engine(0)
+    eng.keygen(SEED, GEN_ALL)
+    rows = args.filter_rows or 16384
+    rate, ms, errors = range_filter(eng, rows, prec, max(1, args.steps))
+    print(json.dumps({"workload": "range filter x <= c, 20-bit lvl2 column", "rows": rows,
+                      "precision": args.precision, "rows_per_s": rate, "ms": ms, "decrypt_errors": errors,
+                      "pbs_per_row": {"lvl02": 6, "lvl01": 3}}))
+    eng.close()
+
+
 def run_profile_pbs(args):
     """--steps launches of the PBS kernel alone, no key-switching key."""
     import torch
@@ -368,6 +422,8 @@ def main():
     args = parse()
     if args.profile_pbs:
         run_profile_pbs(args)
+    elif args.filter_only:
+        run_filter_only(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -17,6 +17,7 @@ FP64, SPLIT32 = 0, 1
 KSK10, KSK20, KSK21 = 10, 20, 21
 GEN_BK01, GEN_BK02, GEN_KSK10, GEN_KSK20, GEN_KSK21, GEN_ALL = 1, 2, 4, 8, 16, 31
 TV_CONST, TV_STAIRCASE, TV_POLY = 0, 1, 2
+COMPARE = {"gt": 0, "ge": 1, "lt": 2, "le": 3, "eq": 4}
 GATES = {"NAND": 0, "NOR": 1, "XNOR": 2, "AND": 3, "OR": 4, "XOR": 5,
          "ANDNY": 6, "ANDYN": 7, "ORNY": 8, "ORYN": 9}
 
@@ -58,6 +59,7 @@ SIGNATURES = {
     "cufhedb_export_ksk_rows": [_vp, _i32, _vp, _i32, _vp],
     "cufhedb_secret_keys": [_u64, _vp, _vp, _vp],
     "cufhedb_encrypt_lvl1": [_vp, _u64, _u64, _u64, _vp, _vp, _i32, _vp],
+    "cufhedb_encrypt_lvl2": [_vp, _u64, _u64, _u64, _vp, _vp, _i32, _vp],
     "cufhedb_pbs_lvl01": [_vp, _vp, _vp, _i32, C.POINTER(TestVec), _i32, _vp],
     "cufhedb_iks": [_vp, _i32, _vp, _vp, _i32, _vp],
     "cufhedb_gate_lvl1": [_vp, _i32, _vp, _vp, _vp, _i32, _i32, _vp],
@@ -71,6 +73,18 @@ SIGNATURES = {
     "cufhedb_pbs_lvl01_host": [_vp, _vp, _vp, _i32, C.POINTER(TestVec), _i32],
     "cufhedb_gate_lvl1_host": [_vp, _i32, _vp, _vp, _vp, _i32, _i32],
     "cufhedb_measure_fma_peak": [_i32, _i32, C.POINTER(C.c_double)],
+    "cufhedb_msb_bootstrap": [_vp, _i32, _i32, _vp, _vp, _i32, _i32, _i32, _vp],
+    "cufhedb_ide_bootstrap": [_vp, _i32, _i32, _vp, _vp, _i32, _u32, _i32, _vp],
+    "cufhedb_log_to_ari": [_vp, _vp, _vp, _i32, _i32, _vp],
+    "cufhedb_log_rescale": [_vp, _vp, _vp, _i32, _u32, _i32, _vp],
+    "cufhedb_hom_and": [_vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp],
+    "cufhedb_hom_or": [_vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp],
+    "cufhedb_hom_msb": [_vp, _i32, _vp, _vp, _i32, _u32, _i32, _i32, _vp],
+    "cufhedb_compare": [_vp, _i32, _i32, _vp, _vp, _vp, _i32, _u32, _i32, _i32, _vp],
+    "cufhedb_graph_begin": [_vp, _vp],
+    "cufhedb_graph_end": [_vp, _vp, C.POINTER(_vp)],
+    "cufhedb_graph_launch": [_vp, _vp],
+    "cufhedb_graph_destroy": [_vp],
 }
 _RESTYPE = {"cufhedb_last_error": C.c_char_p}
 

@@ -17,25 +17,7 @@
 
 using namespace cfdb;
 
-struct cufhedb_ctx {
-    int device = 0;
-    int num_sms = 0;
-    Fft512Tables *tab512 = nullptr;   // device copy of the lvl1 transform tables
-    Fft512TablesF *tab512f = nullptr; // the same tables in FP32 (split-precision path)
-    float4 *bk01_split = nullptr;     // split-precision lvl01 key (hi/lo limbs, FP32)
-    Fft1024Tables *tab1024 = nullptr; // lvl2 transform tables
-    double2 *bk02 = nullptr;          // FFT-domain lvl02 key, chunk layout
-    uint64_t *bk02_int = nullptr;     // integer lvl02 key (when loaded or generated)
-    double2 *bk01 = nullptr;          // FFT-domain lvl01 key, chunk layout
-    uint32_t *bk01_int = nullptr;     // integer lvl01 key (when loaded or generated)
-    uint32_t *ksk[3] = {nullptr, nullptr, nullptr};   // lvl10, lvl20, lvl21
-    int *err = nullptr;               // device failure word
-    cudaStream_t io = nullptr;        // stream of the host-buffer entry points
-    std::mutex io_mu;
-    bool have_sk = false;
-    uint32_t *s0_d = nullptr, *s1_d = nullptr;
-    uint64_t *s2_d = nullptr;
-};
+#include "ctx.cuh"
 
 namespace {
 
@@ -225,6 +207,78 @@ namespace cfdb {
 
 int set_error(int code, const char *msg) { return fail(code, msg); }
 
+int cuda_error(cudaError_t e, const char *what) { return cuda_fail(e, what); }
+
+int pbs01_run(cufhedb_ctx *ctx, const uint32_t *in, uint32_t *out, int B, const TestVec &tv, uint32_t b_add,
+              int precision, cudaStream_t st)
+{
+    if (B <= 0) return CUFHEDB_OK;
+    if (!ctx->bk01) return fail(CUFHEDB_ERR_NOKEY, "lvl01 bootstrapping key not loaded");
+    if (precision != CUFHEDB_FP64 && precision != CUFHEDB_SPLIT32) return fail(CUFHEDB_ERR_ARG, "unsupported precision");
+    Pbs01Args a{};
+    a.in = in;
+    a.out = out;
+    a.B = B;
+    a.tv = tv;
+    a.out_b_add = b_add;
+    a.err = ctx->err;
+    if (precision == CUFHEDB_FP64) {
+        a.bk = ctx->bk01;
+        a.tables = ctx->tab512;
+        CK(launch_pbs01_f64(a, ctx->num_sms, st));
+    } else {
+        if (!ctx->bk01_split) return fail(CUFHEDB_ERR_NOKEY, "split-precision lvl01 key not prepared");
+        a.bk = reinterpret_cast<const double2 *>(ctx->bk01_split);
+        a.tables = ctx->tab512f;
+        CK(launch_pbs01_split(a, ctx->num_sms, st));
+    }
+    return CUFHEDB_OK;
+}
+
+int pbs02_run(cufhedb_ctx *ctx, const uint32_t *in, uint64_t *out, int B, const TestVec &tv, uint64_t b_add,
+              cudaStream_t st)
+{
+    if (B <= 0) return CUFHEDB_OK;
+    if (!ctx->bk02) return fail(CUFHEDB_ERR_NOKEY, "lvl02 bootstrapping key not loaded");
+    Pbs02Args a{};
+    a.in = in;
+    a.out = out;
+    a.B = B;
+    a.bk = ctx->bk02;
+    a.tables = ctx->tab1024;
+    a.tv = tv;
+    a.out_b_add = b_add;
+    a.err = ctx->err;
+    CK(launch_pbs02_f64(a, ctx->num_sms, st));
+    return CUFHEDB_OK;
+}
+
+int iks_run(cufhedb_ctx *ctx, int kind, const void *in, const uint32_t *in_b, int sa, int sb, uint64_t offset,
+            uint32_t *out, int B, cudaStream_t st)
+{
+    if (B <= 0) return CUFHEDB_OK;
+    const int slot = ksk_slot(kind);
+    if (slot < 0) return fail(CUFHEDB_ERR_ARG, "unknown key-switching kind");
+    if (!ctx->ksk[slot]) return fail(CUFHEDB_ERR_NOKEY, "key-switching key not loaded");
+    IksArgs k{};
+    if (kind == 10) {
+        k.in32 = (const uint32_t *)in;
+        k.in32b = in_b;
+        k.sa = sa;
+        k.sb = sb;
+        k.offset = (uint32_t)offset;
+    } else {
+        k.in64 = (const uint64_t *)in;
+        k.sa = 1;
+        k.offset64 = offset;
+    }
+    k.out = out;
+    k.ksk = ctx->ksk[slot];
+    k.B = B;
+    CK(launch_iks(k, kind, st));
+    return CUFHEDB_OK;
+}
+
 int ctx_device(const cufhedb_ctx *ctx) { return ctx->device; }
 
 // IKS10 of the combined gate input into the caller's lvl0 scratch (B x 673
@@ -288,6 +342,9 @@ int cufhedb_ctx_create(cufhedb_ctx **out, int device)
     if (e == cudaSuccess) e = cudaMalloc((void **)&ctx->err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(ctx->err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->io, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = init_pbs01_f64();
+    if (e == cudaSuccess) e = init_pbs01_split();
+    if (e == cudaSuccess) e = init_pbs02_f64();
     if (e != cudaSuccess) {
         cufhedb_ctx_destroy(ctx);
         return cuda_fail(e, "context set-up");
@@ -549,6 +606,16 @@ int cufhedb_encrypt_lvl1(cufhedb_ctx *ctx, uint64_t seed, uint64_t stream_id, ui
     if (!ctx->have_sk) return fail(CUFHEDB_ERR_NOKEY, "no deterministic key set (call cufhedb_keygen)");
     DeviceGuard g(ctx->device);
     CK(encrypt_tlwe32(out, msg, B, N1, ctx->s1_d, NS_LVL1, seed, stream_id, idx0, (cudaStream_t)stream));
+    return CUFHEDB_OK;
+}
+
+int cufhedb_encrypt_lvl2(cufhedb_ctx *ctx, uint64_t seed, uint64_t stream_id, uint64_t idx0, const uint64_t *msg,
+                         uint64_t *out, int B, cufhedb_stream_t stream)
+{
+    NEED(ctx && msg && out && B >= 0, "bad argument");
+    if (!ctx->have_sk) return fail(CUFHEDB_ERR_NOKEY, "no deterministic key set (call cufhedb_keygen)");
+    DeviceGuard g(ctx->device);
+    CK(encrypt_tlwe64(out, msg, B, N2, ctx->s2_d, NS_LVL2, seed, stream_id, idx0, (cudaStream_t)stream));
     return CUFHEDB_OK;
 }
 

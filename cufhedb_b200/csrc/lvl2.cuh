@@ -12,6 +12,7 @@ struct Pbs02Args {
     const double2 *bk;       // N0 x 8 rows x 2 outputs x 1024 complex (chunk layout [s][t])
     const void *tables;      // Fft1024Tables in global memory
     TestVec tv;
+    uint64_t out_b_add;      // added to the b word of every output
     int *err;
 };
 
@@ -25,6 +26,7 @@ struct ExtProd2Args {
 };
 
 cudaError_t launch_pbs02_f64(const Pbs02Args &a, int num_sms, cudaStream_t st);
+cudaError_t init_pbs02_f64();
 cudaError_t launch_extprod2(const ExtProd2Args &a, cudaStream_t st);
 cudaError_t bk02_to_fft(double2 *dst, const uint64_t *src, int rows, const Fft1024Tables *T, cudaStream_t st);
 cudaError_t bkfft02_permute(double2 *dst, const double *src, int rows, cudaStream_t st);

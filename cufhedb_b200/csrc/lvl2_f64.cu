@@ -210,7 +210,7 @@ __global__ void __launch_bounds__((W + 1) * 32, 1) pbs02_f64_kernel(Pbs02Args a)
         if (valid) {
             uint64_t *o = a.out + (size_t)ct * (N2 + 1);
             for (int j = t; j < N2; j += 64) o[j] = j == 0 ? acc[0] : 0ull - acc[N2 - j];
-            if (t == 0) o[N2] = acc[N2];
+            if (t == 0) o[N2] = acc[N2] + a.out_b_add;
         }
         pair_sync(bar);
     }
@@ -363,13 +363,16 @@ cudaError_t launch_pbs02_f64(const Pbs02Args &a, int num_sms, cudaStream_t st)
     if (a.B <= 0) return cudaSuccess;
     using L = Pbs02Smem<PBS02_W, PBS02_S>;
     static_assert(L::TOTAL <= 227 * 1024, "shared memory budget");
-    cudaError_t e = cudaFuncSetAttribute(pbs02_f64_kernel<PBS02_W, PBS02_S>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL);
-    if (e != cudaSuccess) return e;
     const int groups = (a.B + PBS02_W / 2 - 1) / (PBS02_W / 2);
     pbs02_f64_kernel<PBS02_W, PBS02_S>
         <<<groups < num_sms ? groups : num_sms, (PBS02_W + 1) * 32, L::TOTAL, st>>>(a);
     return cudaGetLastError();
+}
+
+cudaError_t init_pbs02_f64()
+{
+    return cudaFuncSetAttribute(pbs02_f64_kernel<PBS02_W, PBS02_S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                Pbs02Smem<PBS02_W, PBS02_S>::TOTAL);
 }
 
 cudaError_t bk02_to_fft(double2 *dst, const uint64_t *src, int rows, const Fft1024Tables *T, cudaStream_t st)

@@ -178,7 +178,7 @@ __global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_f64_kernel(Pbs01Args a)
         if (valid) {
             uint32_t *o = a.out + (size_t)ct * (N1 + 1);
             for (int j = lane; j < N1; j += 32) o[j] = j == 0 ? acc[0] : (uint32_t)(0u - acc[N1 - j]);
-            if (lane == 0) o[N1] = acc[N1];
+            if (lane == 0) o[N1] = acc[N1] + a.out_b_add;
         }
         __syncwarp();
     }
@@ -188,9 +188,6 @@ template <int W, int S>
 static cudaError_t launch_pbs01_f64_t(const Pbs01Args &a, int grid, cudaStream_t st)
 {
     using L = Pbs01Smem<W, S>;
-    cudaError_t e = cudaFuncSetAttribute(pbs01_f64_kernel<W, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         L::TOTAL);
-    if (e != cudaSuccess) return e;
     pbs01_f64_kernel<W, S><<<grid, (W + 1) * 32, L::TOTAL, st>>>(a);
     return cudaGetLastError();
 }
@@ -208,6 +205,14 @@ cudaError_t launch_pbs01_f64(const Pbs01Args &a, int num_sms, cudaStream_t st)
     static_assert(Pbs01Smem<PBS01_W, PBS01_S>::TOTAL <= 227 * 1024, "shared memory budget");
     const int groups = (a.B + PBS01_W - 1) / PBS01_W;
     return launch_pbs01_f64_t<PBS01_W, PBS01_S>(a, groups < num_sms ? groups : num_sms, st);
+}
+
+// the dynamic shared-memory opt-in, set once per device when a context is
+// created (so no attribute call happens inside a stream capture)
+cudaError_t init_pbs01_f64()
+{
+    return cudaFuncSetAttribute(pbs01_f64_kernel<PBS01_W, PBS01_S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                Pbs01Smem<PBS01_W, PBS01_S>::TOTAL);
 }
 
 size_t pbs01_f64_smem_bytes() { return Pbs01Smem<PBS01_W, PBS01_S>::TOTAL; }

@@ -198,7 +198,7 @@ __global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_split_kernel(Pbs01Args 
         if (valid) {
             uint32_t *o = a.out + (size_t)ct * (N1 + 1);
             for (int j = lane; j < N1; j += 32) o[j] = j == 0 ? acc[0] : (uint32_t)(0u - acc[N1 - j]);
-            if (lane == 0) o[N1] = acc[N1];
+            if (lane == 0) o[N1] = acc[N1] + a.out_b_add;
         }
         __syncwarp();
     }
@@ -211,13 +211,16 @@ cudaError_t launch_pbs01_split(const Pbs01Args &a, int num_sms, cudaStream_t st)
     if (a.B <= 0) return cudaSuccess;
     using L = Pbs01SplitSmem<PBS01S_W, PBS01S_S>;
     static_assert(L::TOTAL <= 227 * 1024, "shared memory budget");
-    cudaError_t e = cudaFuncSetAttribute(pbs01_split_kernel<PBS01S_W, PBS01S_S>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL);
-    if (e != cudaSuccess) return e;
     const int groups = (a.B + PBS01S_W - 1) / PBS01S_W;
     pbs01_split_kernel<PBS01S_W, PBS01S_S>
         <<<groups < num_sms ? groups : num_sms, (PBS01S_W + 1) * 32, L::TOTAL, st>>>(a);
     return cudaGetLastError();
+}
+
+cudaError_t init_pbs01_split()
+{
+    return cudaFuncSetAttribute(pbs01_split_kernel<PBS01S_W, PBS01S_S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                Pbs01SplitSmem<PBS01S_W, PBS01S_S>::TOTAL);
 }
 
 }  // namespace cfdb

@@ -64,11 +64,14 @@ struct Pbs01Args {
     const double2 *bk;       // N0 x 6 chunks x 1024 complex, chunk layout [s][o][lane]
     const void *tables;      // Fft512Tables in global memory
     TestVec tv;
+    uint32_t out_b_add;      // added to the b word of every output (the "+ u" of MSB/gate bootstraps)
     int *err;
 };
 
 cudaError_t launch_pbs01_f64(const Pbs01Args &a, int num_sms, cudaStream_t st);
 // bk: split-precision key (float4 hi/lo chunk layout), tables: Fft512TablesF
 cudaError_t launch_pbs01_split(const Pbs01Args &a, int num_sms, cudaStream_t st);
+cudaError_t init_pbs01_f64();
+cudaError_t init_pbs01_split();
 
 }  // namespace cfdb

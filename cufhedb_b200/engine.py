@@ -129,6 +129,11 @@ class Engine:
         check(self.lib.cufhedb_encrypt_lvl1(self.ctx, seed, stream_id, idx0, _ptr(msg_dev), _ptr(out_dev), B,
                                             _stream(stream)))
 
+    def encrypt_lvl2(self, seed: int, stream_id: int, idx0: int, msg_dev, out_dev, stream=None):
+        B = msg_dev.numel()
+        check(self.lib.cufhedb_encrypt_lvl2(self.ctx, seed, stream_id, idx0, _ptr(msg_dev), _ptr(out_dev), B,
+                                            _stream(stream)))
+
     # ---- batched device operations ---------------------------------------------
     def pbs_lvl01(self, in_dev, out_dev, tv: _lib.TestVec, precision: int = _lib.FP64, stream=None):
         B = in_dev.numel() // (N0 + 1)
@@ -226,6 +231,53 @@ class Engine:
     def twist_fft_lvl1(self, in_dev, out_dev, stream=None):
         B = in_dev.numel() // N1
         check(self.lib.cufhedb_twist_fft_lvl1(self.ctx, _ptr(in_dev), _ptr(out_dev), B, _stream(stream)))
+
+    # ---- operator layer (cuHEDB operators over batches of rows) --------------------
+    @staticmethod
+    def _rows(t, level):
+        return t.numel() // ((N1 + 1) if level == 1 else (N2 + 1))
+
+    def msb_bootstrap(self, in_level, out_level, in_dev, out_dev, logic=True, precision=_lib.FP64, stream=None):
+        check(self.lib.cufhedb_msb_bootstrap(self.ctx, in_level, out_level, _ptr(in_dev), _ptr(out_dev),
+                                             self._rows(in_dev, in_level), int(logic), precision, _stream(stream)))
+
+    def ide_bootstrap(self, in_level, out_level, in_dev, out_dev, scale_bits, precision=_lib.FP64, stream=None):
+        check(self.lib.cufhedb_ide_bootstrap(self.ctx, in_level, out_level, _ptr(in_dev), _ptr(out_dev),
+                                             self._rows(in_dev, in_level), scale_bits, precision, _stream(stream)))
+
+    def log_to_ari(self, in_dev, out_dev, precision=_lib.FP64, stream=None):
+        check(self.lib.cufhedb_log_to_ari(self.ctx, _ptr(in_dev), _ptr(out_dev), self._rows(in_dev, 1), precision,
+                                          _stream(stream)))
+
+    def hom_and(self, ca, cb, out, logic=True, precision=_lib.FP64, stream=None):
+        check(self.lib.cufhedb_hom_and(self.ctx, _ptr(ca), _ptr(cb), _ptr(out), self._rows(ca, 1), int(logic),
+                                       precision, _stream(stream)))
+
+    def hom_or(self, ca, cb, out, logic=True, precision=_lib.FP64, stream=None):
+        check(self.lib.cufhedb_hom_or(self.ctx, _ptr(ca), _ptr(cb), _ptr(out), self._rows(ca, 1), int(logic),
+                                      precision, _stream(stream)))
+
+    def hom_msb(self, in_level, in_dev, out_dev, plain_bits, logic=True, precision=_lib.FP64, stream=None):
+        check(self.lib.cufhedb_hom_msb(self.ctx, in_level, _ptr(in_dev), _ptr(out_dev), self._rows(in_dev, in_level),
+                                       plain_bits, int(logic), precision, _stream(stream)))
+
+    def compare(self, op: str, level: int, c1, c2, out, plain_bits, logic=True, precision=_lib.FP64, stream=None):
+        check(self.lib.cufhedb_compare(self.ctx, _lib.COMPARE[op], level, _ptr(c1), _ptr(c2), _ptr(out),
+                                       self._rows(c1, level), plain_bits, int(logic), precision, _stream(stream)))
+
+    def graph_begin(self, stream):
+        check(self.lib.cufhedb_graph_begin(self.ctx, _stream(stream)))
+
+    def graph_end(self, stream):
+        g = C.c_void_p()
+        check(self.lib.cufhedb_graph_end(self.ctx, _stream(stream), C.byref(g)))
+        return g
+
+    def graph_launch(self, graph, stream):
+        check(self.lib.cufhedb_graph_launch(graph, _stream(stream)))
+
+    def graph_destroy(self, graph):
+        check(self.lib.cufhedb_graph_destroy(graph))
 
     # ---- host-buffer entry points --------------------------------------------------
     def pbs_lvl01_host(self, in_lvl0: np.ndarray, tv: _lib.TestVec, precision: int = _lib.FP64) -> np.ndarray:

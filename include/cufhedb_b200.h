@@ -145,6 +145,9 @@ CUFHEDB_API int cufhedb_secret_keys(uint64_t seed, uint32_t *s0, uint32_t *s1, u
  * blocks idx0.. of generator stream `stream_id` (test/benchmark inputs) */
 CUFHEDB_API int cufhedb_encrypt_lvl1(cufhedb_ctx *ctx, uint64_t seed, uint64_t stream_id, uint64_t idx0, const uint32_t *msg,
                          uint32_t *out, int B, cufhedb_stream_t stream);
+/* the same for lvl2 TLWEs (2049 x uint64) under the lvl2 key */
+CUFHEDB_API int cufhedb_encrypt_lvl2(cufhedb_ctx *ctx, uint64_t seed, uint64_t stream_id, uint64_t idx0,
+                                     const uint64_t *msg, uint64_t *out, int B, cufhedb_stream_t stream);
 
 /* ---- batched operations on device memory ------------------------------------- */
 /* B x GateBootstrappingTLWE2TLWEFFT<lvl01param> (cufft_gpu.cuh:250-294;
@@ -205,6 +208,46 @@ CUFHEDB_API int cufhedb_twist_fft_lvl2(cufhedb_ctx *ctx, const double *in, uint6
  * (include/mulfft.hpp:57-121; the reference's ifft_st / fft_st, cufft_gpu.cuh:187-211) */
 CUFHEDB_API int cufhedb_twist_ifft_lvl1(cufhedb_ctx *ctx, const uint32_t *in, double *out, int B, cufhedb_stream_t stream);
 CUFHEDB_API int cufhedb_twist_fft_lvl1(cufhedb_ctx *ctx, const double *in, uint32_t *out, int B, cufhedb_stream_t stream);
+
+/* ---- batched operator layer (cuHEDB, src/cuHEDB/gatebootstrap_gpu.cuh,
+ *      msb_gpu.cuh, HomCompare_gpu.cuh): every call applies the operator to B
+ *      rows; lvl1 ciphertexts are 1025 x uint32, lvl2 ciphertexts 2049 x uint64;
+ *      `logic` != 0 is the reference's LOGIC result type (+-1/8), 0 ARITHMETIC;
+ *      `precision` selects the lvl0 -> lvl1 bootstraps' path (lvl2 is FP64). */
+/* MSBGateBootstrapping (gatebootstrap_gpu.cuh:31-78): level pairs 1->1, 2->1, 2->2 */
+CUFHEDB_API int cufhedb_msb_bootstrap(cufhedb_ctx *ctx, int in_level, int out_level, const void *in, void *out,
+                                      int B, int logic, int precision, cufhedb_stream_t stream);
+/* IdeGateBootstrapping (gatebootstrap_gpu.cuh:80-117): level pairs 1->1, 2->1, 2->2 */
+CUFHEDB_API int cufhedb_ide_bootstrap(cufhedb_ctx *ctx, int in_level, int out_level, const void *in, void *out,
+                                      int B, uint32_t scale_bits, int precision, cufhedb_stream_t stream);
+/* LOG_to_ARI and log_rescale (gatebootstrap_gpu.cuh:154-168) */
+CUFHEDB_API int cufhedb_log_to_ari(cufhedb_ctx *ctx, const uint32_t *in, uint32_t *out, int B, int precision,
+                                   cufhedb_stream_t stream);
+CUFHEDB_API int cufhedb_log_rescale(cufhedb_ctx *ctx, const uint32_t *in, uint32_t *out, int B,
+                                    uint32_t scale_bits, int precision, cufhedb_stream_t stream);
+/* HomAND / HomOR of LOGIC inputs (gatebootstrap_gpu.cuh:124-152) */
+CUFHEDB_API int cufhedb_hom_and(cufhedb_ctx *ctx, const uint32_t *ca, const uint32_t *cb, uint32_t *out, int B,
+                                int logic, int precision, cufhedb_stream_t stream);
+CUFHEDB_API int cufhedb_hom_or(cufhedb_ctx *ctx, const uint32_t *ca, const uint32_t *cb, uint32_t *out, int B,
+                               int logic, int precision, cufhedb_stream_t stream);
+/* HomMSB (msb_gpu.cuh:57-62 for lvl1 input, :175-193 for lvl2 input); plain_bits
+ * beyond 10 (lvl1) or 33 (lvl2) fail with CUFHEDB_ERR_ARG ("Plain bits out.") */
+CUFHEDB_API int cufhedb_hom_msb(cufhedb_ctx *ctx, int in_level, const void *in, uint32_t *out_lvl1, int B,
+                                uint32_t plain_bits, int logic, int precision, cufhedb_stream_t stream);
+/* greater_than (op 0), greater_than_equal (1), less_than (2), less_than_equal (3),
+ * equal (4) of level-`level` ciphertexts c1, c2 (HomCompare_gpu.cuh:13-76) */
+CUFHEDB_API int cufhedb_compare(cufhedb_ctx *ctx, int op, int level, const void *c1, const void *c2,
+                                uint32_t *out_lvl1, int B, uint32_t plain_bits, int logic, int precision,
+                                cufhedb_stream_t stream);
+
+/* ---- CUDA-graph capture of an operator DAG: everything enqueued on `stream`
+ *      between begin and end (which must be a non-default stream) becomes one
+ *      graph, replayed by cufhedb_graph_launch. */
+typedef struct cufhedb_graph cufhedb_graph;
+CUFHEDB_API int cufhedb_graph_begin(cufhedb_ctx *ctx, cufhedb_stream_t stream);
+CUFHEDB_API int cufhedb_graph_end(cufhedb_ctx *ctx, cufhedb_stream_t stream, cufhedb_graph **out);
+CUFHEDB_API int cufhedb_graph_launch(cufhedb_graph *graph, cufhedb_stream_t stream);
+CUFHEDB_API int cufhedb_graph_destroy(cufhedb_graph *graph);
 
 /* ---- host-buffer entry points (synchronous; the _st calls of cufft_gpu.cuh) ---- */
 CUFHEDB_API int cufhedb_pbs_lvl01_host(cufhedb_ctx *ctx, const uint32_t *in_lvl0, uint32_t *out_lvl1, int B,
