@@ -137,14 +137,20 @@ struct Ops {
     {
         return ks20_pbs02(out, in, 1ull << 57, tv_stair(scale_bits), 0ull);
     }
+    // LOG_to_ARI / log_rescale use the CPU twins' test vector, the constant
+    // +2^30 (resp. +2^(scale_bits-1)) that mu_polygen(-mu) builds
+    // (src/HEDB/comparison/tfhepp_utils.cpp:19-37), then add 2^29 (resp.
+    // 2^(scale_bits-1)) to b: a logic 1 (phase ~ +1/8) ends at 3/8 and decodes to
+    // 1, a logic 0 ends at -1/8 and decodes to 0.  The reference's GPU wrappers
+    // (gatebootstrap_gpu.cuh:154-168) pass -2^30 instead, which inverts the result.
     int log_to_ari(uint32_t *out, const uint32_t *in)
     {
-        return ks10_pbs01(out, in, nullptr, 1, 0, 0u, tv_const((uint32_t)(0u - (MU1 << 1))), MU1);
+        return ks10_pbs01(out, in, nullptr, 1, 0, 0u, tv_const(MU1 << 1), MU1);
     }
     int log_rescale(uint32_t *out, const uint32_t *in, uint32_t scale_bits)
     {
         const uint32_t mu = 1u << (scale_bits - 1);
-        return ks10_pbs01(out, in, nullptr, 1, 0, 0u, tv_const((uint32_t)(0u - mu)), mu);
+        return ks10_pbs01(out, in, nullptr, 1, 0, 0u, tv_const(mu), mu);
     }
     // c0 + c1 -/+ 1/8, bootstrapped to +-offset (HomAND / HomOR)
     int hom_andor(uint32_t *out, const uint32_t *ca, const uint32_t *cb, bool arith, bool is_or)
