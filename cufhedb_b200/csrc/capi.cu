@@ -619,6 +619,26 @@ int cufhedb_encrypt_lvl2(cufhedb_ctx *ctx, uint64_t seed, uint64_t stream_id, ui
     return CUFHEDB_OK;
 }
 
+int cufhedb_phase_lvl1(cufhedb_ctx *ctx, const uint32_t *ct, const uint32_t *key, uint32_t *phase, int B,
+                       cufhedb_stream_t stream)
+{
+    NEED(ctx && ct && phase && B >= 0, "bad argument");
+    if (!key && !ctx->have_sk) return fail(CUFHEDB_ERR_NOKEY, "no key given and no deterministic key set");
+    DeviceGuard g(ctx->device);
+    CK(tlwe_phase32(phase, ct, B, N1, key ? key : ctx->s1_d, (cudaStream_t)stream));
+    return CUFHEDB_OK;
+}
+
+int cufhedb_phase_lvl2(cufhedb_ctx *ctx, const uint64_t *ct, const uint64_t *key, uint64_t *phase, int B,
+                       cufhedb_stream_t stream)
+{
+    NEED(ctx && ct && phase && B >= 0, "bad argument");
+    if (!key && !ctx->have_sk) return fail(CUFHEDB_ERR_NOKEY, "no key given and no deterministic key set");
+    DeviceGuard g(ctx->device);
+    CK(tlwe_phase64(phase, ct, B, N2, key ? key : ctx->s2_d, (cudaStream_t)stream));
+    return CUFHEDB_OK;
+}
+
 // ---- batched operations --------------------------------------------------
 
 int cufhedb_pbs_lvl01(cufhedb_ctx *ctx, const uint32_t *in_lvl0, uint32_t *out_lvl1, int B,

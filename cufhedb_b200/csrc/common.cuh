@@ -19,10 +19,10 @@ constexpr int KS21_BASEBIT = 3, KS21_T = 10;
 // gadget decomposition constants (thirdparty/TFHEpp/src/trgsw.cpp:9-39)
 constexpr uint32_t DEC1_OFFSET = (32u << 26) + (32u << 20) + (32u << 14);   // sum Bg/2 * 2^(32-i*Bgbit)
 constexpr uint32_t DEC1_ROUND = 1u << (32 - L1 * BGBIT1 - 1);
-// Signed digit extraction in one bit-field instruction: with
-// x = (t + DEC1_OFFSET + DEC1_ROUND) ^ DEC1_XOR, digit d of t is the sign-
-// extended 6-bit field of x at bit 32 - 6 (d + 1).  ((u ^ 32) read as a signed
-// 6-bit number is u - 32 for every 6-bit u, the "- Bg/2" of trgsw.cpp:31.)
+// Signed digit extraction: with x = (t + DEC1_OFFSET + DEC1_ROUND) ^ DEC1_XOR,
+// digit d of t is the sign-extended 6-bit field of x at bit 32 - 6 (d + 1).
+// ((u ^ 32) read as a signed 6-bit number is u - 32 for every 6-bit u, the
+// "- Bg/2" of trgsw.cpp:31.)
 constexpr uint32_t DEC1_XOR = (32u << 26) | (32u << 20) | (32u << 14);
 constexpr uint64_t DEC2_OFFSET = (256ull << 55) + (256ull << 46) + (256ull << 37) + (256ull << 28);
 constexpr uint64_t DEC2_ROUND = 1ull << (64 - L2 * BGBIT2 - 1);
@@ -97,11 +97,11 @@ __device__ __forceinline__ void bulk_g2s(void *smem_dst, const void *gsrc, uint3
         : "memory");
 }
 
-__device__ __forceinline__ int bfe_s32(uint32_t x, int pos, int len)
+// signed Bg-bit field d (0 = most significant) of x: two plain shifts, the
+// field moved to the top and sign-extended back down
+__device__ __forceinline__ int digit_field1(uint32_t x, int d)
 {
-    int r;
-    asm("bfe.s32 %0, %1, %2, %3;" : "=r"(r) : "r"(x), "r"(pos), "r"(len));
-    return r;
+    return (int)(x << (BGBIT1 * d)) >> (32 - BGBIT1);
 }
 
 __device__ __forceinline__ void report_error(int *err, int code)

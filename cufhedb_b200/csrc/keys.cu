@@ -143,6 +143,24 @@ __global__ void tlwe_encrypt_kernel(T *out, const T *msg, int B, int n, const T 
     if (lane == 0) o[n] = msg[c] + (T)noise_k(skey, base + n, ns) + part;
 }
 
+// decryption phases b - <a, key> (mod 2^w) of B TLWEs of width n, one warp each
+template <typename T>
+__global__ void tlwe_phase_kernel(T *phase, const T *ct, int B, int n, const T *key)
+{
+    const int c = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (c >= B) return;
+    const T *x = ct + (size_t)c * (n + 1);
+    T part = 0;
+    for (int i = lane; i < n; i += 32) part += x[i] * key[i];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        if constexpr (sizeof(T) == 8) part += (T)__shfl_xor_sync(0xffffffffu, (unsigned long long)part, off);
+        else part += __shfl_xor_sync(0xffffffffu, part, off);
+    }
+    if (lane == 0) phase[c] = x[n] - part;
+}
+
 // forward FFT of integer polynomials into the engine's chunk layout.
 // src: [rows][2][1024] 32-bit torus; dst: [rows][16 s][2 o][32 lane] complex
 __global__ void bk_fft1_kernel(double2 *dst, const uint32_t *src, int rows, const Fft512Tables *T)
@@ -278,6 +296,20 @@ cudaError_t encrypt_tlwe32(uint32_t *out, const uint32_t *msg_d, int B, int n, c
     if (B <= 0) return cudaSuccess;
     tlwe_encrypt_kernel<uint32_t><<<(B + 7) / 8, 256, 0, st>>>(out, msg_d, B, n, key_d, stream_key(seed, stream), ns,
                                                                idx0, CB_TLWE32);
+    return cudaGetLastError();
+}
+
+cudaError_t tlwe_phase32(uint32_t *phase, const uint32_t *ct, int B, int n, const uint32_t *key_d, cudaStream_t st)
+{
+    if (B <= 0) return cudaSuccess;
+    tlwe_phase_kernel<uint32_t><<<(B + 7) / 8, 256, 0, st>>>(phase, ct, B, n, key_d);
+    return cudaGetLastError();
+}
+
+cudaError_t tlwe_phase64(uint64_t *phase, const uint64_t *ct, int B, int n, const uint64_t *key_d, cudaStream_t st)
+{
+    if (B <= 0) return cudaSuccess;
+    tlwe_phase_kernel<uint64_t><<<(B + 7) / 8, 256, 0, st>>>(phase, ct, B, n, key_d);
     return cudaGetLastError();
 }
 

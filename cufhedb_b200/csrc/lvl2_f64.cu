@@ -24,11 +24,10 @@ namespace {
 
 constexpr uint64_t DEC2_XOR = (256ull << 55) | (256ull << 46) | (256ull << 37) | (256ull << 28);
 
-__device__ __forceinline__ long long bfe_s64(uint64_t x, int pos, int len)
+// signed 9-bit field d (0 = most significant) of x, sign-extended by two shifts
+__device__ __forceinline__ long long digit_field2(uint64_t x, int d)
 {
-    long long r;
-    asm("bfe.s64 %0, %1, %2, %3;" : "=l"(r) : "l"(x), "r"(pos), "r"(len));
-    return r;
+    return (long long)(x << (BGBIT2 * d)) >> (64 - BGBIT2);
 }
 
 // digit d of (X^a - 1) * poly (or of poly when a == 0 and plain), twisted:
@@ -37,7 +36,6 @@ template <bool ROT>
 __device__ __forceinline__ void digits2(double2 v[16], const uint64_t *poly, uint32_t abar, int d, int t,
                                         const Fft1024Tables &T)
 {
-    const int sh = 64 - BGBIT2 * (d + 1);
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int m = t + 64 * m2;
@@ -46,8 +44,8 @@ __device__ __forceinline__ void digits2(double2 v[16], const uint64_t *poly, uin
             c0 = rot_coef<N2>(poly, m, abar) - c0;
             c1 = rot_coef<N2>(poly, m + 1024, abar) - c1;
         }
-        const long long d0 = bfe_s64((c0 + DEC2_OFFSET + DEC2_ROUND) ^ DEC2_XOR, sh, BGBIT2);
-        const long long d1 = bfe_s64((c1 + DEC2_OFFSET + DEC2_ROUND) ^ DEC2_XOR, sh, BGBIT2);
+        const long long d0 = digit_field2((c0 + DEC2_OFFSET + DEC2_ROUND) ^ DEC2_XOR, d);
+        const long long d1 = digit_field2((c1 + DEC2_OFFSET + DEC2_ROUND) ^ DEC2_XOR, d);
         v[m2] = cmul(make_double2((double)d0, (double)d1), T.twist[m2 * 64 + t]);
     }
 }

@@ -33,17 +33,16 @@ struct Pbs01Smem {
 
 // digit d of (X^a - 1) * poly at coefficients m and m+512, twisted:
 // v[m2] = (dig_d(m) + i dig_d(m+512)) * w^m,  m = lane + 32 m2.  The signed
-// digit is one bit-field extraction of (t + offset + round) ^ DEC1_XOR.
+// digit is the sign-extended field d of (t + offset + round) ^ DEC1_XOR.
 __device__ __forceinline__ void load_digit_poly1(double2 v[16], const uint32_t *poly, uint32_t abar, int d, int lane,
                                         const Fft512Tables &T)
 {
-    const int sh = 32 - BGBIT1 * (d + 1);
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int m = lane + 32 * m2;
         const uint32_t x0 = ((rot_coef<N1>(poly, m, abar) - poly[m]) + DEC1_OFFSET + DEC1_ROUND) ^ DEC1_XOR;
         const uint32_t x1 = ((rot_coef<N1>(poly, m + 512, abar) - poly[m + 512]) + DEC1_OFFSET + DEC1_ROUND) ^ DEC1_XOR;
-        const int d0 = bfe_s32(x0, sh, BGBIT1), d1 = bfe_s32(x1, sh, BGBIT1);
+        const int d0 = digit_field1(x0, d), d1 = digit_field1(x1, d);
         v[m2] = cmul(make_double2((double)d0, (double)d1), T.twist[m2 * 32 + lane]);
     }
 }

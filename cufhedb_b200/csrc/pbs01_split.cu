@@ -40,41 +40,46 @@ struct Pbs01SplitSmem {
 
 // digit d of (X^a - 1) * poly at coefficients m and m+512, twisted:
 // v[m2] = (dig_d(m) + i dig_d(m+512)) * w^m,  m = lane + 32 m2.  The signed
-// digit is one bit-field extraction of (t + offset + round) ^ DEC1_XOR.
+// digit is the sign-extended field d of (t + offset + round) ^ DEC1_XOR.
 __device__ __forceinline__ void load_digit_poly1_f(float2 v[16], const uint32_t *poly, uint32_t abar, int d, int lane,
                                         const Fft512TablesF &T)
 {
-    const int sh = 32 - BGBIT1 * (d + 1);
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int m = lane + 32 * m2;
         const uint32_t x0 = ((rot_coef<N1>(poly, m, abar) - poly[m]) + DEC1_OFFSET + DEC1_ROUND) ^ DEC1_XOR;
         const uint32_t x1 = ((rot_coef<N1>(poly, m + 512, abar) - poly[m + 512]) + DEC1_OFFSET + DEC1_ROUND) ^ DEC1_XOR;
-        const int d0 = bfe_s32(x0, sh, BGBIT1), d1 = bfe_s32(x1, sh, BGBIT1);
+        const int d0 = digit_field1(x0, d), d1 = digit_field1(x1, d);
         v[m2] = fcmul(make_float2((float)d0, (float)d1), T.twist[m2 * 32 + lane]);
     }
 }
 
-// poly[m] += round(hi_m) * 2^24 + round(lo_m) (mod 2^32); the hi limb rounds
-// exactly, the lo limb's FP32 error stays far below the bootstrapping noise
-__device__ __forceinline__ void add_inverse_split(uint32_t *poly, float2 hi[16], float2 lo[16], float2 *xp, int lane,
-                                                  const Fft512TablesF &T)
+// poly[m] += round(hi_m) * 2^24 (mod 2^32): the hi limb's products round exactly
+__device__ __forceinline__ void add_inverse_hi(uint32_t *poly, float2 v[16], float2 *xp, int lane,
+                                               const Fft512TablesF &T)
 {
-    ffft512_inv(hi, xp, T, lane);
-    uint32_t hv[32];
-#pragma unroll
-    for (int m2 = 0; m2 < 16; ++m2) {
-        const float2 y = fcmul(hi[m2], T.untwist[m2 * 32 + lane]);
-        hv[2 * m2] = (uint32_t)__float2int_rn(y.x) << 24;
-        hv[2 * m2 + 1] = (uint32_t)__float2int_rn(y.y) << 24;
-    }
-    ffft512_inv(lo, xp, T, lane);
+    ffft512_inv(v, xp, T, lane);
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int m = lane + 32 * m2;
-        const float2 y = fcmul(lo[m2], T.untwist[m2 * 32 + lane]);
-        poly[m] += hv[2 * m2] + (uint32_t)__float2ll_rn(y.x);
-        poly[m + 512] += hv[2 * m2 + 1] + (uint32_t)__float2ll_rn(y.y);
+        const float2 y = fcmul(v[m2], T.untwist[m2 * 32 + lane]);
+        poly[m] += (uint32_t)__float2int_rn(y.x) << 24;
+        poly[m + 512] += (uint32_t)__float2int_rn(y.y) << 24;
+    }
+}
+
+// poly[m] += round(lo_m) (mod 2^32); the lo limb's FP32 error stays far below
+// the bootstrapping noise
+__device__ __forceinline__ void add_inverse_lo(uint32_t *poly, float2 v[16], float2 *xp, int lane,
+                                               const Fft512TablesF &T)
+{
+    ffft512_inv(v, xp, T, lane);
+#pragma unroll
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int m = lane + 32 * m2;
+        const float2 y = fcmul(v[m2], T.untwist[m2 * 32 + lane]);
+        poly[m] += (uint32_t)__float2ll_rn(y.x);
+        poly[m + 512] += (uint32_t)__float2ll_rn(y.y);
     }
 }
 
@@ -190,8 +195,10 @@ __global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_split_kernel(Pbs01Args 
                 if (lane == 0) mbar_arrive(&empty[slot]);
             }
             if (active) {
-                add_inverse_split(acc, f0h, f0l, xp, lane, *T);
-                add_inverse_split(acc + N1, f1h, f1l, xp, lane, *T);
+                add_inverse_hi(acc, f0h, xp, lane, *T);
+                add_inverse_lo(acc, f0l, xp, lane, *T);
+                add_inverse_hi(acc + N1, f1h, xp, lane, *T);
+                add_inverse_lo(acc + N1, f1l, xp, lane, *T);
                 __syncwarp();
             }
         }

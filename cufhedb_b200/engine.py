@@ -134,6 +134,17 @@ class Engine:
         check(self.lib.cufhedb_encrypt_lvl2(self.ctx, seed, stream_id, idx0, _ptr(msg_dev), _ptr(out_dev), B,
                                             _stream(stream)))
 
+    def phase_lvl1(self, ct_dev, phase_dev, key_dev=None, stream=None):
+        """decryption phases b - <a, s1> of lvl1 TLWEs (key: device words, or the key set's)"""
+        B = ct_dev.numel() // (N1 + 1)
+        check(self.lib.cufhedb_phase_lvl1(self.ctx, _ptr(ct_dev), _ptr(key_dev) if key_dev is not None else None,
+                                          _ptr(phase_dev), B, _stream(stream)))
+
+    def phase_lvl2(self, ct_dev, phase_dev, key_dev=None, stream=None):
+        B = ct_dev.numel() // (N2 + 1)
+        check(self.lib.cufhedb_phase_lvl2(self.ctx, _ptr(ct_dev), _ptr(key_dev) if key_dev is not None else None,
+                                          _ptr(phase_dev), B, _stream(stream)))
+
     # ---- batched device operations ---------------------------------------------
     def pbs_lvl01(self, in_dev, out_dev, tv: _lib.TestVec, precision: int = _lib.FP64, stream=None):
         B = in_dev.numel() // (N0 + 1)

@@ -149,6 +149,15 @@ CUFHEDB_API int cufhedb_encrypt_lvl1(cufhedb_ctx *ctx, uint64_t seed, uint64_t s
 CUFHEDB_API int cufhedb_encrypt_lvl2(cufhedb_ctx *ctx, uint64_t seed, uint64_t stream_id, uint64_t idx0,
                                      const uint64_t *msg, uint64_t *out, int B, cufhedb_stream_t stream);
 
+/* decryption phases b - <a, key> (mod 2^32 / 2^64) of B lvl1 / lvl2 TLWEs, the
+ * quantity tlweSymDecrypt / tlweSymInt32Decrypt round (TFHEpp src/tlwe.cpp:
+ * 18-91, src/HEDB/comparison/tfhepp_utils.h:32-45); `key` is a device array of
+ * 1024 (lvl1) / 2048 (lvl2) key words, or NULL for the deterministic key set's */
+CUFHEDB_API int cufhedb_phase_lvl1(cufhedb_ctx *ctx, const uint32_t *ct, const uint32_t *key, uint32_t *phase, int B,
+                                   cufhedb_stream_t stream);
+CUFHEDB_API int cufhedb_phase_lvl2(cufhedb_ctx *ctx, const uint64_t *ct, const uint64_t *key, uint64_t *phase, int B,
+                                   cufhedb_stream_t stream);
+
 /* ---- batched operations on device memory ------------------------------------- */
 /* B x GateBootstrappingTLWE2TLWEFFT<lvl01param> (cufft_gpu.cuh:250-294;
  * TFHEpp src/gatebootstrapping.cpp:14-23): lvl0 TLWE in, lvl1 TLWE out */
