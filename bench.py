@@ -1,13 +1,20 @@
 #!/usr/bin/env python
-"""Benchmark: lvl1 gate bootstraps per second on B200 (one process per GPU).
+"""Benchmark: lvl1 bootstraps per second on B200, split-FP32 vs FP64 path,
+plus encrypted-filter rows per second (one process per GPU).
 
-Workload (one step): 1,024 independent lvl1 HomNAND gates over pairs of
+Gate workload (one step): 1,024 independent lvl1 HomNAND gates over pairs of
 uniformly random bits -- per gate one lvl1->lvl0 identity key switch and one
 lvl0->lvl1 programmable bootstrap (TFHEpp HomNAND, thirdparty/TFHEpp/src/
 gate.cpp:50-65) -- with the reference's default parameters
-(params/128bit.hpp: n=672, N=1024, l=3, Bg=2^6, IKS basebit 10, t=2).
-Keys and inputs come from the deterministic generator; inputs are encrypted
-on the device, so `value` is measured with inputs resident in HBM.
+(params/128bit.hpp: n=672, N=1024, l=3, Bg=2^6, IKS basebit 10, t=2).  Keys
+and inputs come from the deterministic generator; inputs are encrypted on the
+device, so `value` is measured with inputs resident in HBM.  `value` is the
+split-precision path; the same steps are timed on the FP64 path (`fp64`).
+
+Filter workload (1 GPU): the 20-bit range filter x <= c at the 30th
+percentile over 16,384 rows encrypted at lvl2 (less_than_equal<Lvl2>, 6 lvl02
++ 3 lvl01 bootstraps and 10 key switches per row).  Error-rate workload (1
+GPU): HomNAND over fresh encryptions on both paths, every output decrypted.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -31,31 +38,41 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 SEED = 0x5EED_B200
-N0, N1 = 672, 1024
+N0, N1, N2 = 672, 1024, 2048
 MU = 1 << 29
 F1 = 156_893_184            # algorithmic flop per lvl01 PBS (672 CMux x 233,472)
-METRIC = "lvl1 PBS/s (HomNAND gate bootstraps: IKS10 + PBS01), 1 B200"
-WORKLOAD = ("1,024 lvl1 HomNAND gate bootstraps over uniform random bit pairs, TFHEpp 128-bit "
-            "params (n=672, N=1024, l=3, Bg=2^6, IKS10 basebit 10 t 2)")
+F2 = 432_144_384            # algorithmic flop per lvl02 PBS (672 CMux x 643,072)
+METRIC = "lvl1 PBS/s, 1 B200: split-FP32 vs FP64 path at 0 decrypt errors; filter rows/s"
+WORKLOAD = ("1,024 lvl1 HomNAND gate bootstraps (IKS10 + PBS01 each) over uniform random bit pairs, "
+            "TFHEpp 128-bit params (n=672, N=1024, l=3, Bg=2^6, IKS10 basebit 10 t 2)")
+# DRAM bytes (read + write) of one 1,024-ciphertext PBS launch, from the ncu
+# captures summarised under profiles/ (pbs01_*_batch1024.md)
+TRAFFIC = {"split32": 69_178_624 + 3_230_464, "fp64": 69_528_064 + 4_634_880}
 
 
-def parse():
+def parse(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--batch", type=int, default=1024)
-    p.add_argument("--precision", choices=["fp64", "split32"], default="fp64")
+    p.add_argument("--precision", choices=["fp64", "split32"], default="split32",
+                   help="headline path (the other one is timed alongside)")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--filter-rows", type=int, default=0,
-                   help="also time the encrypted range filter (20-bit lvl2 column, x <= c at the 30th "
-                        "percentile) over this many rows and report filter rows/s")
+    p.add_argument("--filter-rows", type=int, default=16384,
+                   help="rows of the encrypted range filter timed at N=1 (0: skip)")
+    p.add_argument("--error-bootstraps", type=int, default=262144,
+                   help="HomNAND bootstraps per path decrypted for the error rate at N=1 (0: skip)")
     p.add_argument("--filter-only", action="store_true", help="run only the range-filter measurement")
+    p.add_argument("--error-only", action="store_true", help="run only the error-rate / noise measurement")
+    p.add_argument("--extprod", action="store_true",
+                   help="external-product microbenchmark: 4,096 products at lvl1 (both paths) and lvl2")
     p.add_argument("--profile-pbs", action="store_true",
-                   help="run only the lvl01 PBS kernel on `--batch` random lvl0 inputs (lvl01 key only, "
-                        "~0.1 GB on the device): the small case for ncu captures")
-    return p.parse_args()
+                   help="run only the PBS kernel on `--batch` random lvl0 inputs (bootstrapping key only, "
+                        "a few hundred MB on the device): the small case for ncu captures")
+    p.add_argument("--level", type=int, choices=[1, 2], default=1, help="PBS level for --profile-pbs")
+    return p.parse_args(argv)
 
 
 def dist_env():
@@ -63,6 +80,26 @@ def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", str(rank)))
     return rank, world, local
+
+
+def reduce_over_ranks(max_vals, sum_vals, device):
+    """Max of the timings and sum of the counters over all ranks (identity
+    without a process group).  Works on gloo (CPU tensors) and nccl."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return list(max_vals), list(sum_vals)
+    t = torch.tensor(list(max_vals) + list(sum_vals), dtype=torch.float64, device=device)
+    m = t[:len(max_vals)].clone()
+    s = t[len(max_vals):].clone()
+    dist.all_reduce(m, op=dist.ReduceOp.MAX)
+    dist.all_reduce(s, op=dist.ReduceOp.SUM)
+    return [float(x) for x in m], [float(x) for x in s]
+
+
+def whole_job_rate(world: int, units_per_rank: int, steps: int, max_total_ms: float) -> float:
+    """units per second over all ranks, timed by the slowest rank"""
+    return world * units_per_rank * steps / (max_total_ms / 1000.0)
 
 
 class ClockSampler:
@@ -176,6 +213,108 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def _events(n):
+    import torch
+    return [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+
+
+def _timed(fn, steps, flush, stream):
+    """CUDA-event time (ms) of each of `steps` calls of fn, L2 flushed (untimed) before each"""
+    ev = _events(steps)
+    for e0, e1 in ev:
+        flush.zero_()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+    stream.synchronize()
+    return [e0.elapsed_time(e1) for e0, e1 in ev]
+
+
+def _gate_errors(eng, out, want_bits, stream):
+    """decrypt every HomNAND output on the device: (errors, noise sum, noise sum of squares)"""
+    import torch
+    B = want_bits.numel()
+    ph = torch.empty(B, dtype=torch.int32, device="cuda")
+    eng.phase_lvl1(out, ph, stream=stream)
+    sign = (ph > 0).to(torch.int64)
+    errors = int((sign != want_bits).sum())
+    noise = ph.to(torch.float64) - torch.where(want_bits == 1, float(MU), float(-MU)).to(torch.float64)
+    return errors, float(noise.sum()), float((noise * noise).sum())
+
+
+def error_rate(eng, nboot: int, stream, chunk: int = 8192):
+    """HomNAND over fresh encryptions on both paths, same inputs; every output
+    decrypted.  Returns per path: bootstraps, decrypt errors, output noise
+    variance (torus units^2 of 2^32), and the split / fp64 variance ratio."""
+    import torch
+    from cufhedb_b200 import FP64, SPLIT32
+    g = torch.Generator(device="cuda").manual_seed(4242)
+    ca = torch.empty(chunk * (N1 + 1), dtype=torch.int32, device="cuda")
+    cb = torch.empty_like(ca)
+    out = torch.empty_like(ca)
+    res = {p: {"bootstraps": 0, "errors": 0, "s1": 0.0, "s2": 0.0} for p in ("split32", "fp64")}
+    done = 0
+    while done < nboot:
+        B = min(chunk, nboot - done)
+        bits = torch.randint(0, 2, (2, B), generator=g, device="cuda")
+        msg = torch.where(bits == 1, MU, -MU).to(torch.int32)
+        eng.encrypt_lvl1(SEED, 0x7E, 2 * done, msg[0].contiguous(), ca[:B * (N1 + 1)], stream)
+        eng.encrypt_lvl1(SEED, 0x7E, 2 * done + B, msg[1].contiguous(), cb[:B * (N1 + 1)], stream)
+        want = (1 - bits[0] * bits[1]).to(torch.int64)
+        for name, prec in (("split32", SPLIT32), ("fp64", FP64)):
+            eng.gate_lvl1("NAND", ca[:B * (N1 + 1)], cb[:B * (N1 + 1)], out[:B * (N1 + 1)], prec, stream)
+            e, s1, s2 = _gate_errors(eng, out[:B * (N1 + 1)], want, stream)
+            r = res[name]
+            r["bootstraps"] += B
+            r["errors"] += e
+            r["s1"] += s1
+            r["s2"] += s2
+        done += B
+    outd = {}
+    for name, r in res.items():
+        n = r["bootstraps"]
+        mean = r["s1"] / n
+        outd[name] = {"bootstraps": n, "decrypt_errors": r["errors"], "noise_var": r["s2"] / n - mean * mean,
+                      "noise_mean": mean}
+    outd["split_over_fp64_noise_var"] = outd["split32"]["noise_var"] / outd["fp64"]["noise_var"]
+    return outd
+
+
+def range_filter(eng, rows: int, precision: int, steps: int = 1):
+    """Encrypted range filter x <= c over a synthetic 20-bit column at lvl2
+    (the reference's HomComp / TPC-H filter shape: less_than_equal<Lvl2>, 6 lvl02
+    + 3 lvl01 bootstraps and 10 key switches per row).  Returns (rows/s, ms per
+    pass, decrypt errors)."""
+    import numpy as np
+    import torch
+    pb = 20
+    g = torch.Generator().manual_seed(77)
+    x = torch.randint(0, 2 ** pb, (rows,), generator=g).numpy().astype(np.uint64)
+    c = int(np.percentile(x, 30))
+    shift = np.uint64(64 - pb - 1)
+    msg = torch.from_numpy((x << shift).view(np.int64)).cuda()
+    thr = torch.from_numpy((np.full(rows, c, np.uint64) << shift).view(np.int64)).cuda()
+    c1 = torch.empty(rows * (N2 + 1), dtype=torch.int64, device="cuda")
+    c2 = torch.empty_like(c1)
+    eng.encrypt_lvl2(SEED, 0x7A, 0, msg, c1)
+    eng.encrypt_lvl2(SEED, 0x7A, rows, thr, c2)
+    out = torch.empty(rows * (N1 + 1), dtype=torch.int32, device="cuda")
+    eng.compare("le", 2, c1, c2, out, pb, True, precision)   # warm-up (and pool growth)
+    eng.sync()
+    ev = _events(steps)
+    for e0, e1 in ev:
+        e0.record()
+        eng.compare("le", 2, c1, c2, out, pb, True, precision)
+        e1.record()
+    eng.sync()
+    ms = statistics.median(e0.elapsed_time(e1) for e0, e1 in ev)
+    ph = torch.empty(rows, dtype=torch.int32, device="cuda")
+    eng.phase_lvl1(out, ph)
+    got = (ph > 0).cpu().numpy().astype(int)
+    errors = int(np.sum(got != (x <= c).astype(int)))
+    return rows / (ms / 1000.0), ms, errors
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -186,13 +325,16 @@ def run_ours(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
-    from cufhedb_b200 import FP64, GEN_BK01, GEN_KSK10, SPLIT32, Engine, _lib
+    from cufhedb_b200 import FP64, GEN_ALL, GEN_BK01, GEN_KSK10, SPLIT32, Engine, _lib, testvec_const
 
-    prec = FP64 if args.precision == "fp64" else SPLIT32
+    head = args.precision
+    other = "fp64" if head == "split32" else "split32"
+    PREC = {"fp64": FP64, "split32": SPLIT32}
     B = args.batch
+    single = world == 1
     eng = Engine(local)
     seed = SEED + rank
-    eng.keygen(seed, GEN_BK01 | GEN_KSK10)
+    eng.keygen(seed, GEN_ALL if (single and args.filter_rows) else GEN_BK01 | GEN_KSK10)
     g = torch.Generator().manual_seed(1234 + rank)
     bits = torch.randint(0, 2, (2, B), generator=g)
     msg = np.where(bits.numpy() == 1, MU, (-MU) & 0xFFFFFFFF).astype(np.uint32).view(np.int32)
@@ -204,13 +346,8 @@ def run_ours(args):
     out = torch.empty_like(ca)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")
     stream = torch.cuda.current_stream()
-
-    def step():
-        eng.gate_lvl1("NAND", ca, cb, out, prec, stream)
-
-    for _ in range(max(3, args.warmup)):
-        step()
-    eng.sync(stream)
+    want = (1 - bits[0] * bits[1]).to(torch.int64).cuda()
+    W = max(3, args.warmup)
 
     def barrier():
         if world > 1:
@@ -218,107 +355,109 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    clocks = ClockSampler(local)
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    barrier()
-    clocks.start()
-    for e0, e1 in ev:
-        flush.zero_()                 # evict L2 between timed steps (untimed)
-        e0.record(stream)
-        step()
-        e1.record(stream)
-    barrier()
-    clk = clocks.stop()
-    eng.sync(stream)
-    total_ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
+    # ---- the timed gate steps, headline path then the other path ----------------
+    res = {}
+    clk = None
+    for name in (head, other):
+        prec = PREC[name]
+        step = lambda: eng.gate_lvl1("NAND", ca, cb, out, prec, stream)
+        for _ in range(W):
+            step()
+        barrier()
+        clocks = ClockSampler(local) if name == head else None
+        if clocks:
+            clocks.start()
+        ms = _timed(step, args.steps, flush, stream)
+        barrier()
+        if clocks:
+            clk = clocks.stop()
+        errors, _, _ = _gate_errors(eng, out, want, stream)
+        res[name] = {"total_ms": sum(ms), "errors": errors}
 
-    # correctness of the last step: decrypt every output with the lvl1 secret key
-    _, s1, _ = Engine.secret_keys(seed)
-    o = out.cpu().numpy().view(np.uint32).reshape(B, N1 + 1).astype(np.uint64)
-    ph = (o[:, N1] - (o[:, :N1] @ s1.astype(np.uint64))) & 0xFFFFFFFF
-    dec = (ph.astype(np.int64) - ((ph >= 2 ** 31) * 2 ** 32) > 0).astype(int)
-    want = 1 - (bits[0].numpy() & bits[1].numpy())
-    errors = int(np.sum(dec != want))
-
-    # dominant kernel alone: the PBS over the key-switched batch
+    # ---- dominant kernel alone: the PBS over the key-switched batch -------------
     lvl0 = torch.empty(B * (N0 + 1), dtype=torch.int32, device="cuda")
-    from cufhedb_b200 import testvec_const
     eng.iks(10, ca, lvl0)
     tv = testvec_const(MU)
-    k_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(5)]
-    for e0, e1 in k_ev:
-        flush.zero_()
-        e0.record(stream)
-        eng.pbs_lvl01(lvl0, out, tv, prec, stream)
-        e1.record(stream)
-    torch.cuda.synchronize()
-    pbs_ms = statistics.median(e0.elapsed_time(e1) for e0, e1 in k_ev)
-    iks_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(5)]
-    for e0, e1 in iks_ev:
-        flush.zero_()
-        e0.record(stream)
-        eng.iks(10, ca, lvl0, stream)
-        e1.record(stream)
-    torch.cuda.synchronize()
-    iks_ms = statistics.median(e0.elapsed_time(e1) for e0, e1 in iks_ev)
+    for name in (head, other):
+        prec = PREC[name]
+        res[name]["pbs_ms"] = statistics.median(
+            _timed(lambda: eng.pbs_lvl01(lvl0, out, tv, prec, stream), 5, flush, stream))
+    iks_ms = statistics.median(_timed(lambda: eng.iks(10, ca, lvl0, stream), 5, flush, stream))
 
-    # end to end through the C ABI with host buffers: pinned H2D + gate + D2H
+    # ---- end to end through the C ABI with host buffers: pinned H2D + gate + D2H --
     ca_h = ca.cpu().pin_memory()
     cb_h = cb.cpu().pin_memory()
     out_h = torch.empty_like(ca_h).pin_memory()
     ca2, cb2, out2 = torch.empty_like(ca), torch.empty_like(cb), torch.empty_like(out)
-    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(args.steps)]
-    barrier()
-    for e0, e1 in e2e_ev:
-        flush.zero_()
-        e0.record(stream)
+
+    def e2e_step():
         ca2.copy_(ca_h, non_blocking=True)
         cb2.copy_(cb_h, non_blocking=True)
-        eng.gate_lvl1("NAND", ca2, cb2, out2, prec, stream)
+        eng.gate_lvl1("NAND", ca2, cb2, out2, PREC[head], stream)
         out_h.copy_(out2, non_blocking=True)
-        e1.record(stream)
+
     barrier()
-    eng.sync(stream)
-    e2e_ms = sum(e0.elapsed_time(e1) for e0, e1 in e2e_ev)
+    e2e_ms = sum(_timed(e2e_step, args.steps, flush, stream))
 
     import ctypes
-    pk = ctypes.c_double(0.0)
-    _lib.check(eng.lib.cufhedb_measure_fma_peak(local, 1 if prec == FP64 else 0, ctypes.byref(pk)))
+    peaks = {}
+    for name, fp64 in (("fp64", 1), ("split32", 0)):
+        pk = ctypes.c_double(0.0)
+        _lib.check(eng.lib.cufhedb_measure_fma_peak(local, fp64, ctypes.byref(pk)))
+        peaks[name] = pk.value
 
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([total_ms, e2e_ms, float(errors)], device="cuda")
-        dist.all_reduce(t[:2], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[2:], op=dist.ReduceOp.SUM)
-        total_ms, e2e_ms, errors = float(t[0]), float(t[1]), int(t[2])
+    (t_head, t_other, t_e2e), (err_head, err_other) = reduce_over_ranks(
+        [res[head]["total_ms"], res[other]["total_ms"], e2e_ms], [res[head]["errors"], res[other]["errors"]],
+        "cuda")
+
+    extra = {}
+    if single and rank == 0:
+        if args.filter_rows:
+            rate, ms, ferr = range_filter(eng, args.filter_rows, PREC[head])
+            extra["filter"] = {"rows": args.filter_rows, "rows_per_s": rate, "ms": ms, "decrypt_errors": ferr,
+                               "workload": "x <= c (30th percentile), 20-bit column at lvl2, less_than_equal<Lvl2>",
+                               "bootstraps_per_row": {"lvl02": 6, "lvl01": 3},
+                               "lvl01_path": head}
+        if args.error_bootstraps:
+            extra["error_rate"] = error_rate(eng, args.error_bootstraps, stream)
 
     if rank == 0:
-        value = world * B * args.steps / (total_ms / 1000.0)
-        e2e_value = world * B * args.steps / (e2e_ms / 1000.0)
-        achieved = B * F1 / (pbs_ms / 1000.0) / 1e12
+        value = whole_job_rate(world, B, args.steps, t_head)
+        v_other = whole_job_rate(world, B, args.steps, t_other)
+        e2e_value = whole_job_rate(world, B, args.steps, t_e2e)
+
+        def roof(name):
+            ach = B * F1 / (res[name]["pbs_ms"] / 1000.0) / 1e12
+            return {"bound": name.replace("split32", "fp32"), "kernel": f"pbs01 ({name})", "achieved": ach,
+                    "peak": peaks[name], "unit": "TFLOP/s", "frac": ach / peaks[name] if peaks[name] else None,
+                    "traffic": TRAFFIC[name], "algorithmic_bytes": 66_060_288 + B * (2692 + 4100),
+                    "peak_source": f"measured {'FP64' if name == 'fp64' else 'FP32'} CUDA-core FMA throughput "
+                                   "(cufhedb_measure_fma_peak), this GPU, this run",
+                    "algorithmic_flop_per_launch": B * F1}
+
         line = {
             "metric": METRIC, "value": value, "unit": "PBS/s", "n_gpus": world, "steps": args.steps,
-            "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == FP64 else "f32",
+            "warmup": W, "ms_per_step": t_head / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if head == "split32" else "f64",
             "data": "synthetic (deterministic keys and encryptions of uniform random bits)",
-            "config": {"workload": WORKLOAD, "batch_per_gpu": B, "precision": args.precision,
+            "config": {"workload": WORKLOAD, "batch_per_gpu": B, "precision": head,
                        "l2": "flushed (256 MB write, untimed) before every timed step",
                        "parallelism": f"independent rows, {world} GPU(s)"},
-            "decrypt_errors": errors,
-            "pbs_kernel_ms": pbs_ms, "iks_kernel_ms": iks_ms,
-            "roofline": {"bound": "fp64" if prec == FP64 else "fp32", "kernel": "pbs01",
-                         "achieved": achieved, "peak": pk.value, "unit": "TFLOP/s",
-                         "frac": achieved / pk.value if pk.value else None, "traffic": None,
-                         "peak_source": "measured CUDA-core FMA microbenchmark (cufhedb_measure_fma_peak), "
-                                        "this GPU, this run",
-                         "algorithmic_flop_per_launch": B * F1},
+            "decrypt_errors": int(err_head),
+            other: {"value": v_other, "unit": "PBS/s", "ms_per_step": t_other / args.steps,
+                    "decrypt_errors": int(err_other), "pbs_kernel_ms": res[other]["pbs_ms"],
+                    "roofline": roof(other)},
+            "split_over_fp64": (value / v_other) if head == "split32" else (v_other / value),
+            "split_over_fp64_kernel": (res["fp64"]["pbs_ms"] / res["split32"]["pbs_ms"]),
+            "pbs_kernel_ms": res[head]["pbs_ms"], "iks_kernel_ms": iks_ms,
+            "roofline": roof(head),
             "gpu_launches": 2 * args.steps,
             "clocks": clk,
             "e2e": {"value": e2e_value, "unit": "PBS/s",
                     "h2d_bytes_per_step": 2 * B * (N1 + 1) * 4, "d2h_bytes_per_step": B * (N1 + 1) * 4},
         }
-        if world == 1 and not args.no_cpu_baseline:
+        line.update(extra)
+        if single and not args.no_cpu_baseline:
             try:
                 nthreads = os.cpu_count() or 1
                 n = cpu_sample_size(nthreads)
@@ -342,43 +481,6 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def range_filter(eng, rows: int, precision: int, steps: int = 1):
-    """Encrypted range filter x <= c over a synthetic 20-bit column at lvl2
-    (the reference's HomComp / TPC-H filter shape: less_than_equal<Lvl2>, 6 lvl02
-    + 3 lvl01 bootstraps and 10 key switches per row).  Returns (rows/s, ms per
-    pass, decrypt errors, bootstraps per row)."""
-    import numpy as np
-    import torch
-    from cufhedb_b200 import Engine
-    pb = 20
-    g = torch.Generator().manual_seed(77)
-    x = torch.randint(0, 2 ** pb, (rows,), generator=g).numpy().astype(np.uint64)
-    c = int(np.percentile(x, 30))
-    shift = np.uint64(64 - pb - 1)
-    msg = torch.from_numpy((x << shift).view(np.int64)).cuda()
-    thr = torch.from_numpy((np.full(rows, c, np.uint64) << shift).view(np.int64)).cuda()
-    c1 = torch.empty(rows * 2049, dtype=torch.int64, device="cuda")
-    c2 = torch.empty_like(c1)
-    eng.encrypt_lvl2(SEED, 0x7A, 0, msg, c1)
-    eng.encrypt_lvl2(SEED, 0x7A, rows, thr, c2)
-    out = torch.empty(rows * (N1 + 1), dtype=torch.int32, device="cuda")
-    eng.compare("le", 2, c1, c2, out, pb, True, precision)   # warm-up (and pool growth)
-    eng.sync()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-    for e0, e1 in ev:
-        e0.record()
-        eng.compare("le", 2, c1, c2, out, pb, True, precision)
-        e1.record()
-    eng.sync()
-    ms = statistics.median(e0.elapsed_time(e1) for e0, e1 in ev)
-    _, s1, _ = Engine.secret_keys(SEED)
-    o = out.cpu().numpy().view(np.uint32).reshape(rows, N1 + 1).astype(np.uint64)
-    ph = (o[:, N1] - (o[:, :N1] @ s1.astype(np.uint64))) & 0xFFFFFFFF
-    dec = ((ph > 0) & (ph < 2 ** 31)).astype(int)
-    errors = int(np.sum(dec != (x <= c).astype(int)))
-    return rows / (ms / 1000.0), ms, errors
-
-
 def run_filter_only(args):
     from cufhedb_b200 import FP64, GEN_ALL, SPLIT32, Engine
     prec = FP64 if args.precision == "fp64" else SPLIT32
@@ -392,29 +494,118 @@ def run_filter_only(args):
     eng.close()
 
 
+def run_error_only(args):
+    import torch
+    from cufhedb_b200 import GEN_BK01, GEN_KSK10, Engine
+    eng = Engine(0)
+    eng.keygen(SEED, GEN_BK01 | GEN_KSK10)
+    r = error_rate(eng, args.error_bootstraps, torch.cuda.current_stream())
+    print(json.dumps({"workload": "HomNAND over fresh encryptions of uniform random bits, every output decrypted",
+                      **r}))
+    eng.close()
+
+
+def run_extprod(args):
+    """4,096 external products TRGSW(random bit) x TRLWE(uniform) at lvl1 (FP64
+    and split) and lvl2 (FP64), one TRGSW per product; computation error
+    against the exact integer product (oracle) on a sample."""
+    import numpy as np
+    import torch
+    from cufhedb_b200 import FP64, GEN_BK01, SPLIT32, Engine
+    from oracle.oracle import Oracle
+    B = 4096
+    eng = Engine(0)
+    eng.keygen(SEED, GEN_BK01)
+    o = Oracle()
+    _, s1, s2 = o.secret_keys(SEED)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")
+    rng = np.random.default_rng(5)
+    out = {}
+    # lvl1: TRGSWs are encryptions of random bits (oracle, a sample) tiled to B
+    nsamp = 16
+    g1 = np.stack([o.trgsw32(int(m), s1, SEED, 0x35, i) for i, m in enumerate(rng.integers(0, 2, nsamp))])
+    g1_all = np.tile(g1, (B // nsamp, 1, 1, 1))
+    trl1 = rng.integers(0, 2 ** 32, (B, 2, N1), dtype=np.uint64).astype(np.uint32)
+    g_d = torch.from_numpy(g1_all.view(np.int32).copy()).cuda()
+    t_d = torch.from_numpy(trl1.view(np.int32).copy()).cuda()
+    o_d = torch.empty(B * 2 * N1, dtype=torch.int32, device="cuda")
+    for name, prec in (("fp64", FP64), ("split32", SPLIT32)):
+        prep = torch.empty(B * 98304 // 8, dtype=torch.float64, device="cuda")
+        eng.trgsw_prepare_lvl1(g_d, prep, prec)
+        fn = lambda: eng.extprod_lvl1(t_d, prep, o_d, precision=prec, stream=stream)
+        for _ in range(3):
+            fn()
+        ms = statistics.median(_timed(fn, max(3, args.steps), flush, stream))
+        got = o_d.cpu().numpy().view(np.uint32).reshape(B, 2, N1)
+        err = np.concatenate([((got[i].astype(np.int64) - o.extprod32_exact(trl1[i], g1_all[i]).astype(np.int64)
+                                + 2 ** 31) % 2 ** 32 - 2 ** 31).ravel() for i in range(nsamp)])
+        out[f"lvl1_{name}"] = {"products": B, "ms": ms, "products_per_s": B / (ms / 1000.0),
+                               "achieved_tflops": B * 233_472 / (ms / 1000.0) / 1e12,
+                               "algorithmic_bytes": B * (98_304 + 2 * 8192),
+                               "err_vs_exact": {"samples": int(err.size), "max_abs": int(np.max(np.abs(err))),
+                                                "var": float(np.var(err.astype(np.float64)))}}
+        del prep
+    # lvl2
+    nsamp2 = 4
+    g2 = np.stack([o.trgsw64(int(m), s2, SEED, 0x36, i) for i, m in enumerate(rng.integers(0, 2, nsamp2))])
+    g2_all = np.tile(g2, (B // nsamp2, 1, 1, 1))
+    trl2 = rng.integers(0, 2 ** 64, (B, 2, N2), dtype=np.uint64)
+    g_d = torch.from_numpy(g2_all.view(np.int64).copy()).cuda()
+    t_d = torch.from_numpy(trl2.view(np.int64).copy()).cuda()
+    o_d = torch.empty(B * 2 * N2, dtype=torch.int64, device="cuda")
+    prep = torch.empty(B * 262144 // 8, dtype=torch.float64, device="cuda")
+    eng.trgsw_prepare_lvl2(g_d, prep)
+    fn = lambda: eng.extprod_lvl2(t_d, prep, o_d, stream=stream)
+    for _ in range(3):
+        fn()
+    ms = statistics.median(_timed(fn, max(3, args.steps), flush, stream))
+    got = o_d.cpu().numpy().view(np.uint64).reshape(B, 2, N2)
+    errs = []
+    for i in range(nsamp2):
+        d = (got[i] - o.extprod64_exact(trl2[i], g2_all[i])).view(np.int64)
+        errs.append(d.astype(np.float64).ravel())
+    err = np.concatenate(errs)
+    out["lvl2_fp64"] = {"products": B, "ms": ms, "products_per_s": B / (ms / 1000.0),
+                        "achieved_tflops": B * 643_072 / (ms / 1000.0) / 1e12,
+                        "algorithmic_bytes": B * (262_144 + 2 * 32768),
+                        "err_vs_exact": {"samples": int(err.size), "max_abs": float(np.max(np.abs(err))),
+                                         "var": float(np.var(err))}}
+    print(json.dumps({"workload": "external products, 4,096 per level, one TRGSW(random bit) per product", **out}))
+    eng.close()
+
+
 def run_profile_pbs(args):
     """--steps launches of the PBS kernel alone, no key-switching key."""
     import torch
-    from cufhedb_b200 import FP64, GEN_BK01, SPLIT32, Engine, testvec_const
+    from cufhedb_b200 import FP64, GEN_BK01, GEN_BK02, SPLIT32, Engine, testvec_const
     prec = FP64 if args.precision == "fp64" else SPLIT32
     eng = Engine(0)
-    eng.keygen(SEED, GEN_BK01)
+    eng.keygen(SEED, GEN_BK01 if args.level == 1 else GEN_BK02)
     g = torch.Generator(device="cuda").manual_seed(99)
     x = torch.randint(-2 ** 31, 2 ** 31, (args.batch * (N0 + 1),), generator=g, device="cuda", dtype=torch.int64)
     x = x.to(torch.int32)
-    out = torch.empty(args.batch * (N1 + 1), dtype=torch.int32, device="cuda")
-    tv = testvec_const(MU)
+    if args.level == 1:
+        out = torch.empty(args.batch * (N1 + 1), dtype=torch.int32, device="cuda")
+        tv = testvec_const(MU)
+        fn = lambda: eng.pbs_lvl01(x, out, tv, prec)
+    else:
+        out = torch.empty(args.batch * (N2 + 1), dtype=torch.int64, device="cuda")
+        tv = testvec_const(1 << 61)
+        fn = lambda: eng.pbs_lvl02(x, out, tv)
     for _ in range(args.warmup):
-        eng.pbs_lvl01(x, out, tv, prec)
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        fn()
+    ev = _events(args.steps)
     for e0, e1 in ev:
         e0.record()
-        eng.pbs_lvl01(x, out, tv, prec)
+        fn()
         e1.record()
     eng.sync()
     ms = [e0.elapsed_time(e1) for e0, e1 in ev]
-    print(json.dumps({"profile": "pbs01", "batch": args.batch, "precision": args.precision,
-                      "ms": ms, "pbs_per_s": args.batch / (statistics.median(ms) / 1000.0) if ms else None}))
+    rate = args.batch / (statistics.median(ms) / 1000.0) if ms else None
+    print(json.dumps({"profile": f"pbs0{args.level}", "batch": args.batch,
+                      "precision": args.precision if args.level == 1 else "fp64", "ms": ms, "pbs_per_s": rate,
+                      "achieved_tflops": rate * (F1 if args.level == 1 else F2) / 1e12 if rate else None}))
     eng.close()
 
 
@@ -424,6 +615,10 @@ def main():
         run_profile_pbs(args)
     elif args.filter_only:
         run_filter_only(args)
+    elif args.error_only:
+        run_error_only(args)
+    elif args.extprod:
+        run_extprod(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(128) extprod2_kernel(ExtProd2Args a)
     }
 }
 
-constexpr int PBS02_W = 4, PBS02_S = 4;
+constexpr int PBS02_W = 6, PBS02_S = 2;
 
 }  // namespace
 
