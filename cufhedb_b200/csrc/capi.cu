@@ -80,25 +80,7 @@ void build_tables(Fft512Tables &T)
     }
 }
 
-void build_tables2(Fft1024Tables &T)
-{
-    const long double PI = 3.141592653589793238462643383279502884L;
-    for (int q2 = 0; q2 < 16; ++q2)
-        for (int m1 = 0; m1 < 64; ++m1) {
-            const long double a = 2.0L * PI * (long double)((m1 * q2) % 1024) / 1024.0L;
-            T.tw1024[q2 * 64 + m1] = make_double2((double)cosl(a), (double)sinl(a));
-        }
-    for (int m2 = 0; m2 < 16; ++m2)
-        for (int m1 = 0; m1 < 64; ++m1) {
-            const long double a = 2.0L * PI * (long double)(m1 + 64 * m2) / 4096.0L;
-            T.twist[m2 * 64 + m1] = make_double2((double)cosl(a), (double)sinl(a));
-        }
-    for (int j = 0; j < 16; ++j) {
-        const long double a = 2.0L * PI * (long double)j / 32.0L, b = 2.0L * PI * (long double)j / 64.0L;
-        T.w32[j] = make_double2((double)cosl(a), (double)sinl(a));
-        T.w64[j] = make_double2((double)cosl(b), (double)sinl(b));
-    }
-}
+void build_tables2(Fft1024Tables &T) { build_fft8x_tables<T2>(T); }
 
 void build_tables_f(const Fft512Tables &D, Fft512TablesF &F)
 {

@@ -85,6 +85,26 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
     return false;
 }
 
+// orders this thread's earlier generic-proxy shared-memory accesses before
+// its later async-proxy ones (a bulk copy into memory just read)
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Release of a key-ring slot by one consumer warp (called by one lane): the
+// slot's counter counts releases; true for the last of the `consumers`
+// releases of the slot's `use`-th chunk, whose caller then refills the slot.
+// The fences order every warp's reads of the slot before the refill.
+__device__ __forceinline__ bool ring_release(int *cnt, uint32_t use, int consumers)
+{
+    __threadfence_block();
+    const int old = atomicAdd(cnt, 1);
+    const bool last = old == (int)(use + 1) * consumers - 1;
+    if (last) __threadfence_block();
+    return last;
+}
+
 // one bulk (TMA-engine) copy global -> this CTA's shared memory, completing
 // `bytes` of transaction count on `bar`.  Both addresses 16-byte aligned,
 // bytes a multiple of 16.

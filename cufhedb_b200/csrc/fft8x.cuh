@@ -1,0 +1,318 @@
+// Negacyclic FFT of M = 8 T complex points spread over T threads (8 values
+// per thread), FP64 (double2) or FP32 (float2).  Used with T = 128 for the
+// lvl2 ring (N = 2048, M = 1024: four warps per polynomial) and T = 64 for
+// the lvl1 ring (N = 1024, M = 512: two warps per polynomial).
+//
+// Transform (TFHEpp TwistIFFT / TwistFFT, thirdparty/TFHEpp/include/
+// mulfft.hpp:57-121, spqlios layout restated in oracle/tfhe_oracle.c):
+//   forward  V(q) = sum_m z_m W_M^{mq},  z_m = (a_m + i a_{m+M}) w^m,
+//            W_P = exp(2 pi i / P), w = exp(2 pi i / 4M)
+//   inverse  M z_m = sum_q V(q) W_M^{-mq}
+//
+// Factorisation (L = T / 8 lanes per group):
+//   A. thread t holds z_{t + T j}, j < 8: 8-point DFT over j in registers
+//      (output k), twiddle W_M^{t k};
+//   B. one shared-memory transpose: thread u = a + L k (a < L) receives the
+//      values of threads t = a + L b, b < 8, for its k; 8-point DFT over b
+//      (output q1), twiddle W_T^{a q1};
+//   C. L-point DFT over a across the L lanes of each group: log2(L) radix-2
+//      decimation-in-frequency steps through warp shuffles.  In step i
+//      (lane bit h = L >> (i+1), register bit beta_i = 4 >> (i mod 3)) each
+//      thread trades the half of its registers selected by beta_i with lane
+//      u ^ h and then owns both inputs of 4 butterflies.
+// The frequency q = k + 8 (q1 + 8 q2) then sits in register slot s of thread
+// u as given by fft8x_freq() below; the bootstrapping key is stored in the
+// same [s][u] order, so the per-frequency products need no data exchange and
+// the inverse transform (the same steps in reverse) starts from the same
+// registers.
+#pragma once
+#include "common.cuh"
+
+namespace cfdb {
+
+// ---- complex arithmetic for both precisions ------------------------------------
+__device__ __forceinline__ double2 cx_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 cx_sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cx_mul(double2 a, double2 b)
+{
+    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 cx_mulc(double2 a, double2 b)   // a * conj(b)
+{
+    return make_double2(fma(a.x, b.x, a.y * b.y), fma(a.y, b.x, -a.x * b.y));
+}
+__device__ __forceinline__ void cx_fma(double2 &acc, double2 a, double2 b)
+{
+    acc.x = fma(a.x, b.x, acc.x);
+    acc.x = fma(-a.y, b.y, acc.x);
+    acc.y = fma(a.x, b.y, acc.y);
+    acc.y = fma(a.y, b.x, acc.y);
+}
+__device__ __forceinline__ double2 cx_shfl_xor(double2 v, int m)
+{
+    return make_double2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+__device__ __forceinline__ double2 cx_scale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+
+__device__ __forceinline__ unsigned long long fx_bits(float2 a) { return *reinterpret_cast<unsigned long long *>(&a); }
+__device__ __forceinline__ float2 fx_from(unsigned long long a) { return *reinterpret_cast<float2 *>(&a); }
+// FP32 complex additions as one packed two-lane instruction (add/sub.rn.f32x2)
+__device__ __forceinline__ float2 cx_add(float2 a, float2 b)
+{
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(fx_bits(a)), "l"(fx_bits(b)));
+    return fx_from(r);
+}
+__device__ __forceinline__ float2 cx_sub(float2 a, float2 b)
+{
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(fx_bits(a)), "l"(fx_bits(b)));
+    return fx_from(r);
+}
+__device__ __forceinline__ float2 cx_mul(float2 a, float2 b)
+{
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cx_mulc(float2 a, float2 b)
+{
+    return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
+}
+__device__ __forceinline__ void cx_fma(float2 &acc, float2 a, float2 b)
+{
+    acc.x = fmaf(a.x, b.x, acc.x);
+    acc.x = fmaf(-a.y, b.y, acc.x);
+    acc.y = fmaf(a.x, b.y, acc.y);
+    acc.y = fmaf(a.y, b.x, acc.y);
+}
+__device__ __forceinline__ float2 cx_shfl_xor(float2 v, int m)
+{
+    return fx_from(__shfl_xor_sync(0xffffffffu, fx_bits(v), m));
+}
+__device__ __forceinline__ float2 cx_scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+
+template <typename C> struct cx_real;
+template <> struct cx_real<double2> { using type = double; };
+template <> struct cx_real<float2> { using type = float; };
+
+// multiply by i^S (S = +1) or (-i) (S = -1)
+template <int S, typename C>
+__device__ __forceinline__ C cx_mul_i(C a)
+{
+    C r;
+    if constexpr (S > 0) { r.x = -a.y; r.y = a.x; }
+    else { r.x = a.y; r.y = -a.x; }
+    return r;
+}
+
+// multiply by exp(S 2 pi i e / 8), e = 1, 2, 3
+template <int S, int E, typename C>
+__device__ __forceinline__ C cx_w8(C a)
+{
+    using R = typename cx_real<C>::type;
+    constexpr R H = (R)0.70710678118654752440;
+    if constexpr (E == 2) {
+        return cx_mul_i<S>(a);
+    } else {
+        C r;
+        if constexpr (E == 1) {   // (1 + S i) / sqrt2
+            if constexpr (S > 0) { r.x = H * (a.x - a.y); r.y = H * (a.x + a.y); }
+            else { r.x = H * (a.x + a.y); r.y = H * (a.y - a.x); }
+        } else {                  // (-1 + S i) / sqrt2
+            if constexpr (S > 0) { r.x = -H * (a.x + a.y); r.y = H * (a.x - a.y); }
+            else { r.x = H * (a.y - a.x); r.y = -H * (a.x + a.y); }
+        }
+        return r;
+    }
+}
+
+// y_k = sum_n a_n i^{S n k}, natural order in and out
+template <int S, typename C>
+__device__ __forceinline__ void cx_dft4(C &a0, C &a1, C &a2, C &a3)
+{
+    const C s02 = cx_add(a0, a2), d02 = cx_sub(a0, a2);
+    const C s13 = cx_add(a1, a3), d13 = cx_sub(a1, a3);
+    const C t = cx_mul_i<S>(d13);
+    a0 = cx_add(s02, s13);
+    a2 = cx_sub(s02, s13);
+    a1 = cx_add(d02, t);
+    a3 = cx_sub(d02, t);
+}
+
+// in-place 8-point DFT X[k] = sum x[n] exp(S 2 pi i nk / 8), natural order
+template <int S, typename C>
+__device__ __forceinline__ void cx_dft8(C v[8])
+{
+    // n = n1 + 2 n2, k = k2 + 4 k1
+    cx_dft4<S>(v[0], v[2], v[4], v[6]);
+    cx_dft4<S>(v[1], v[3], v[5], v[7]);
+    v[3] = cx_w8<S, 1>(v[3]);
+    v[5] = cx_w8<S, 2>(v[5]);
+    v[7] = cx_w8<S, 3>(v[7]);
+    C x[8];
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) {
+        x[k2] = cx_add(v[2 * k2], v[2 * k2 + 1]);
+        x[k2 + 4] = cx_sub(v[2 * k2], v[2 * k2 + 1]);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = x[i];
+}
+
+// ---- tables ---------------------------------------------------------------------
+//   twist[j T + t] = w^{t + T j}          (M entries)
+//   twA[k T + t]   = W_M^{t k}            (M entries, k < 8)
+//   twB[q1 L + a]  = W_T^{a q1}           (8 L = T entries)
+//   wC[j]          = W_L^j, j < L / 2
+template <typename C, int T>
+struct Fft8xTables {
+    static constexpr int M = 8 * T, L = T / 8;
+    C twist[M];
+    C twA[M];
+    C twB[T];
+    C wC[L / 2];
+};
+
+// host: the FP64 tables, computed in long double
+template <int T>
+inline void build_fft8x_tables(Fft8xTables<double2, T> &tab)
+{
+    constexpr int M = 8 * T, L = T / 8;
+    const long double PI = 3.141592653589793238462643383279502884L;
+    auto cis = [&](long long num, long long den) {
+        const long double a = 2.0L * PI * (long double)num / (long double)den;
+        return make_double2((double)cosl(a), (double)sinl(a));
+    };
+    for (int j = 0; j < 8; ++j)
+        for (int t = 0; t < T; ++t) {
+            tab.twist[j * T + t] = cis(t + T * j, 4 * M);
+            tab.twA[j * T + t] = cis((long long)(t * j) % M, M);
+        }
+    for (int q1 = 0; q1 < 8; ++q1)
+        for (int a = 0; a < L; ++a) tab.twB[q1 * L + a] = cis((long long)(a * q1) % T, T);
+    for (int j = 0; j < L / 2; ++j) tab.wC[j] = cis(j, L);
+}
+
+__host__ __device__ constexpr int ilog2c(int x) { return x <= 1 ? 0 : 1 + ilog2c(x >> 1); }
+
+// frequency held in register slot s of thread u after the forward transform
+template <int T>
+__host__ __device__ __forceinline__ int fft8x_freq(int u, int s)
+{
+    constexpr int L = T / 8, NST = ilog2c(L);
+    const int a = u % L, k = u / L;
+    // meaning of each register bit / lane bit: (is_q2, bit position)
+    int slot_kind[3] = {0, 0, 0}, slot_pos[3] = {0, 1, 2};
+    int lane_kind[4] = {0, 0, 0, 0}, lane_pos[4] = {0, 0, 0, 0};
+    for (int i = 0; i < NST; ++i) {
+        const int hb = NST - 1 - i;               // lane bit index of h = L >> (i+1)
+        const int rb = 2 - (i % 3);               // register bit index of beta = 4 >> (i mod 3)
+        lane_kind[hb] = slot_kind[rb];
+        lane_pos[hb] = slot_pos[rb];
+        slot_kind[rb] = 1;
+        slot_pos[rb] = i;
+    }
+    int q1 = 0, q2 = 0;
+    for (int b = 0; b < 3; ++b)
+        if (s & (1 << b)) {
+            if (slot_kind[b]) q2 |= 1 << slot_pos[b];
+            else q1 |= 1 << slot_pos[b];
+        }
+    for (int b = 0; b < NST; ++b)
+        if (a & (1 << b)) {
+            if (lane_kind[b]) q2 |= 1 << lane_pos[b];
+            else q1 |= 1 << lane_pos[b];
+        }
+    return k + 8 * (q1 + 8 * q2);
+}
+
+// synchronises the T threads of one polynomial (named barrier `id`)
+template <int T>
+__device__ __forceinline__ void group_sync(int id)
+{
+    if constexpr (T == 32) __syncwarp();
+    else asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(T) : "memory");
+}
+
+// transpose scratch index: row t (the thread of stage A), column k; the XOR
+// swizzle keeps both the row-wise write and the column-wise read conflict-free
+template <typename C>
+__device__ __forceinline__ int fft8x_xp(int t, int k)
+{
+    if constexpr (sizeof(C) == 16) return t * 8 + (k ^ (t & 7));
+    else return t * 8 + (k ^ ((t >> 1) & 7));
+}
+
+// forward: v[j] = z_{t + T j} in, v[s] = V(fft8x_freq<T>(t, s)) out.
+// xp: M-entry scratch shared by the group; bar: its named barrier.
+template <typename C, int T>
+__device__ __forceinline__ void fft8x_fwd(C v[8], C *xp, const Fft8xTables<C, T> &tab, int t, int bar)
+{
+    constexpr int L = T / 8, NST = ilog2c(L);
+    cx_dft8<1>(v);
+#pragma unroll
+    for (int k = 1; k < 8; ++k) v[k] = cx_mul(v[k], tab.twA[k * T + t]);
+    group_sync<T>(bar);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) xp[fft8x_xp<C>(t, k)] = v[k];
+    group_sync<T>(bar);
+    const int a = t % L, k = t / L;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) v[b] = xp[fft8x_xp<C>(a + L * b, k)];
+    cx_dft8<1>(v);
+#pragma unroll
+    for (int q1 = 1; q1 < 8; ++q1) v[q1] = cx_mul(v[q1], tab.twB[q1 * L + a]);
+#pragma unroll
+    for (int i = 0; i < NST; ++i) {
+        const int h = L >> (i + 1), beta = 4 >> (i % 3);
+        const bool hi_lane = (a & h) != 0;
+        const C tw = tab.wC[(a & (h - 1)) * (L / (2 * h))];
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+            if (s & beta) continue;
+            const C send = hi_lane ? v[s] : v[s | beta];
+            const C recv = cx_shfl_xor(send, h);
+            const C lo = hi_lane ? recv : v[s];
+            const C hi = hi_lane ? v[s | beta] : recv;
+            v[s] = cx_add(lo, hi);
+            v[s | beta] = cx_mul(cx_sub(lo, hi), tw);
+        }
+    }
+}
+
+// inverse: v[s] = V(fft8x_freq<T>(t, s)) in, v[j] = M z_{t + T j} out
+template <typename C, int T>
+__device__ __forceinline__ void fft8x_inv(C v[8], C *xp, const Fft8xTables<C, T> &tab, int t, int bar)
+{
+    constexpr int L = T / 8, NST = ilog2c(L);
+    const int a = t % L, k = t / L;
+#pragma unroll
+    for (int i = NST - 1; i >= 0; --i) {
+        const int h = L >> (i + 1), beta = 4 >> (i % 3);
+        const bool hi_lane = (a & h) != 0;
+        const C tw = tab.wC[(a & (h - 1)) * (L / (2 * h))];
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+            if (s & beta) continue;
+            const C y0 = v[s], y1 = cx_mulc(v[s | beta], tw);
+            const C lo = cx_add(y0, y1), hi = cx_sub(y0, y1);
+            const C send = hi_lane ? lo : hi;
+            const C recv = cx_shfl_xor(send, h);
+            v[s] = hi_lane ? recv : lo;
+            v[s | beta] = hi_lane ? hi : recv;
+        }
+    }
+#pragma unroll
+    for (int q1 = 1; q1 < 8; ++q1) v[q1] = cx_mulc(v[q1], tab.twB[q1 * L + a]);
+    cx_dft8<-1>(v);
+    group_sync<T>(bar);
+#pragma unroll
+    for (int b = 0; b < 8; ++b) xp[fft8x_xp<C>(a + L * b, k)] = v[b];
+    group_sync<T>(bar);
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) v[kk] = xp[fft8x_xp<C>(t, kk)];
+#pragma unroll
+    for (int kk = 1; kk < 8; ++kk) v[kk] = cx_mulc(v[kk], tab.twA[kk * T + t]);
+    cx_dft8<-1>(v);
+}
+
+}  // namespace cfdb
