@@ -355,6 +355,14 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    # ---- launch-shape autotuning (untimed): one pass with 7 and with 8 ----------
+    tune = {}
+    for name in (head, other):
+        ms7, ms8 = eng.autotune_pbs01(PREC[name])
+        passes = lambda w: -(-(-(-B // w)) // eng.num_sms)
+        w = 8 if passes(8) * ms8 < passes(7) * ms7 else 7
+        tune[name] = {"pass_ms_w7": ms7, "pass_ms_w8": ms8, "ciphertexts_per_cta": w}
+
     # ---- the timed gate steps, headline path then the other path ----------------
     res = {}
     clk = None
@@ -450,6 +458,7 @@ def run_ours(args):
             "split_over_fp64": (value / v_other) if head == "split32" else (v_other / value),
             "split_over_fp64_kernel": (res["fp64"]["pbs_ms"] / res["split32"]["pbs_ms"]),
             "pbs_kernel_ms": res[head]["pbs_ms"], "iks_kernel_ms": iks_ms,
+            "autotune": tune,
             "roofline": roof(head),
             "gpu_launches": 2 * args.steps,
             "clocks": clk,

@@ -141,12 +141,12 @@ int pbs01_enqueue(cufhedb_ctx *ctx, const uint32_t *in, uint32_t *out, int B, co
     if (precision == CUFHEDB_FP64) {
         a.bk = ctx->bk01;
         a.tables = ctx->tab512;
-        CK(launch_pbs01_f64(a, ctx->num_sms, st));
+        CK(launch_pbs01_f64(a, ctx->num_sms, pbs01_choose_w(B, ctx->num_sms, ctx->pbs01_pass_ms[0]), st));
     } else {
         if (!ctx->bk01_split) return fail(CUFHEDB_ERR_NOKEY, "split-precision lvl01 key not prepared");
         a.bk = reinterpret_cast<const double2 *>(ctx->bk01_split);
         a.tables = ctx->tab512f;
-        CK(launch_pbs01_split(a, ctx->num_sms, st));
+        CK(launch_pbs01_split(a, ctx->num_sms, pbs01_choose_w(B, ctx->num_sms, ctx->pbs01_pass_ms[1]), st));
     }
     return CUFHEDB_OK;
 }
@@ -207,12 +207,12 @@ int pbs01_run(cufhedb_ctx *ctx, const uint32_t *in, uint32_t *out, int B, const 
     if (precision == CUFHEDB_FP64) {
         a.bk = ctx->bk01;
         a.tables = ctx->tab512;
-        CK(launch_pbs01_f64(a, ctx->num_sms, st));
+        CK(launch_pbs01_f64(a, ctx->num_sms, pbs01_choose_w(B, ctx->num_sms, ctx->pbs01_pass_ms[0]), st));
     } else {
         if (!ctx->bk01_split) return fail(CUFHEDB_ERR_NOKEY, "split-precision lvl01 key not prepared");
         a.bk = reinterpret_cast<const double2 *>(ctx->bk01_split);
         a.tables = ctx->tab512f;
-        CK(launch_pbs01_split(a, ctx->num_sms, st));
+        CK(launch_pbs01_split(a, ctx->num_sms, pbs01_choose_w(B, ctx->num_sms, ctx->pbs01_pass_ms[1]), st));
     }
     return CUFHEDB_OK;
 }
@@ -634,6 +634,69 @@ int cufhedb_pbs_lvl01(cufhedb_ctx *ctx, const uint32_t *in_lvl0, uint32_t *out_l
     if (rc) return rc;
     DeviceGuard g(ctx->device);
     return pbs01_enqueue(ctx, in_lvl0, out_lvl1, B, tv, precision, (cudaStream_t)stream);
+}
+
+int cufhedb_autotune_pbs01(cufhedb_ctx *ctx, int precision, float *ms_w7, float *ms_w8)
+{
+    NEED(ctx != nullptr, "ctx is null");
+    NEED(precision == CUFHEDB_FP64 || precision == CUFHEDB_SPLIT32, "unsupported precision");
+    if (!ctx->bk01) return fail(CUFHEDB_ERR_NOKEY, "lvl01 bootstrapping key not loaded");
+    DeviceGuard g(ctx->device);
+    const int Bmax = 8 * ctx->num_sms;
+    uint32_t *in = nullptr, *out = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    float best[2] = {0.0f, 0.0f};
+    int rc = CUFHEDB_OK;
+    cudaError_t e = cudaMalloc((void **)&in, (size_t)Bmax * (N0 + 1) * 4);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&out, (size_t)Bmax * (N1 + 1) * 4);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = fill_random32(in, (size_t)Bmax * (N0 + 1), 0x7A5E, 1, st);
+    if (e != cudaSuccess) rc = cuda_fail(e, "autotune setup");
+    const cufhedb_testvec tv{CUFHEDB_TV_CONST, 0, 1u << 29, nullptr};
+    for (int w = 7; w <= 8 && rc == CUFHEDB_OK; ++w) {
+        // one full pass: w ciphertexts on every SM
+        Pbs01Args a{};
+        a.in = in;
+        a.out = out;
+        a.B = w * ctx->num_sms;
+        a.tv = to_tv(&tv);
+        a.err = ctx->err;
+        a.bk = precision == CUFHEDB_FP64 ? ctx->bk01 : reinterpret_cast<const double2 *>(ctx->bk01_split);
+        a.tables = precision == CUFHEDB_FP64 ? (const void *)ctx->tab512 : (const void *)ctx->tab512f;
+        if (!a.bk) {
+            rc = fail(CUFHEDB_ERR_NOKEY, "split-precision lvl01 key not prepared");
+            break;
+        }
+        float t_best = 0.0f;
+        for (int it = 0; it < 3 && rc == CUFHEDB_OK; ++it) {
+            e = cudaEventRecord(e0, st);
+            if (e == cudaSuccess)
+                e = precision == CUFHEDB_FP64 ? launch_pbs01_f64(a, ctx->num_sms, w, st)
+                                              : launch_pbs01_split(a, ctx->num_sms, w, st);
+            if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float ms = 0.0f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (e != cudaSuccess) rc = cuda_fail(e, "autotune run");
+            else if (it > 0 && (t_best == 0.0f || ms < t_best)) t_best = ms;   // first run warms up
+        }
+        best[w - 7] = t_best;
+    }
+    if (rc == CUFHEDB_OK) rc = cufhedb_sync(ctx, st);
+    if (st) cudaStreamDestroy(st);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(in);
+    cudaFree(out);
+    if (rc != CUFHEDB_OK) return rc;
+    ctx->pbs01_pass_ms[precision][0] = best[0];
+    ctx->pbs01_pass_ms[precision][1] = best[1];
+    if (ms_w7) *ms_w7 = best[0];
+    if (ms_w8) *ms_w8 = best[1];
+    return CUFHEDB_OK;
 }
 
 int cufhedb_iks(cufhedb_ctx *ctx, int kind, const void *in, uint32_t *out, int B, cufhedb_stream_t stream)

@@ -28,6 +28,9 @@ struct cufhedb_ctx {
     cudaStream_t io = nullptr;        // stream of the host-buffer entry points
     std::mutex io_mu;
     bool have_sk = false;
+    // measured time of one pass of the lvl01 PBS kernel with 7 / 8 ciphertexts
+    // per CTA, per precision (FP64, split); equal until cufhedb_autotune runs
+    float pbs01_pass_ms[2][2] = {{1.0f, 1.0f}, {1.0f, 1.0f}};
     uint32_t *s0_d = nullptr, *s1_d = nullptr;
     uint64_t *s2_d = nullptr;
 };

@@ -143,6 +143,14 @@ __global__ void tlwe_encrypt_kernel(T *out, const T *msg, int B, int n, const T 
     if (lane == 0) o[n] = msg[c] + (T)noise_k(skey, base + n, ns) + part;
 }
 
+// n pseudo-random words (generator stream `stream` of `seed`), e.g. lvl0
+// ciphertexts with uniform coefficients for timing runs
+__global__ void fill_random_kernel(uint32_t *out, size_t n, uint64_t skey)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (uint32_t)draw_k(skey, i);
+}
+
 // decryption phases b - <a, key> (mod 2^w) of B TLWEs of width n, one warp each
 template <typename T>
 __global__ void tlwe_phase_kernel(T *phase, const T *ct, int B, int n, const T *key)
@@ -296,6 +304,13 @@ cudaError_t encrypt_tlwe32(uint32_t *out, const uint32_t *msg_d, int B, int n, c
     if (B <= 0) return cudaSuccess;
     tlwe_encrypt_kernel<uint32_t><<<(B + 7) / 8, 256, 0, st>>>(out, msg_d, B, n, key_d, stream_key(seed, stream), ns,
                                                                idx0, CB_TLWE32);
+    return cudaGetLastError();
+}
+
+cudaError_t fill_random32(uint32_t *out, size_t n, uint64_t seed, uint64_t stream, cudaStream_t st)
+{
+    if (n == 0) return cudaSuccess;
+    fill_random_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(out, n, stream_key(seed, stream));
     return cudaGetLastError();
 }
 

@@ -30,6 +30,7 @@ cudaError_t encrypt_tlwe32(uint32_t *out, const uint32_t *msg_d, int B, int n, c
                            uint64_t seed, uint64_t stream, uint64_t idx0, cudaStream_t st);
 cudaError_t encrypt_tlwe64(uint64_t *out, const uint64_t *msg_d, int B, int n, const uint64_t *key_d, int64_t ns,
                            uint64_t seed, uint64_t stream, uint64_t idx0, cudaStream_t st);
+cudaError_t fill_random32(uint32_t *out, size_t n, uint64_t seed, uint64_t stream, cudaStream_t st);
 cudaError_t tlwe_phase32(uint32_t *phase, const uint32_t *ct, int B, int n, const uint32_t *key_d, cudaStream_t st);
 cudaError_t tlwe_phase64(uint64_t *phase, const uint64_t *ct, int B, int n, const uint64_t *key_d, cudaStream_t st);
 cudaError_t bk01_to_fft(double2 *dst, const uint32_t *src, int rows, const Fft512Tables *T, cudaStream_t st);

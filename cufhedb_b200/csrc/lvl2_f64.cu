@@ -18,6 +18,7 @@
 // [slot s][thread u], so each thread reads exactly the frequencies it owns.
 #include "fft1024_f64.cuh"
 #include "lvl2.cuh"
+#include "ring.cuh"
 
 namespace cfdb {
 
@@ -65,11 +66,8 @@ __device__ __forceinline__ void add_inverse2(uint64_t *poly, const double2 v[8],
 
 template <int P, int S>
 struct Pbs02Smem {
-    static constexpr int CNT_OFF = 64;         // int[S]: releases per ring slot
-    static constexpr int ISSUED_OFF = 80;      // int[S]: chunks issued into each ring slot
-    static constexpr int ABORT_OFF = 96;       // int: set when any wait gave up
-    static constexpr int RING_OFF = 128;
     static constexpr int CHUNK_BYTES = 16384;   // one (row, output): 1024 complex
+    static constexpr int RING_OFF = RING_HEADER_BYTES;
     static constexpr int TAB_OFF = RING_OFF + S * CHUNK_BYTES;
     static constexpr int GROUP_OFF = TAB_OFF + ((int)sizeof(Fft1024Tables) + 127) / 128 * 128;
     static constexpr int XP_BYTES = 1024 * 16;
@@ -77,59 +75,32 @@ struct Pbs02Smem {
     static constexpr int ABAR_BYTES = ((N0 * 2) + 127) / 128 * 128;
     static constexpr int PER_GROUP = XP_BYTES + ACC_BYTES + ABAR_BYTES;
     static constexpr int TOTAL = GROUP_OFF + P * PER_GROUP;
-    static_assert(S <= 4, "mbarriers and counters must fit below CNT_OFF / ABORT_OFF");
 };
 
-// Key ring without a producer warp: thread 0 issues the first S chunks, and
-// afterwards the last consumer warp to release a slot refills it with the
-// chunk S positions further on.  Every warp therefore runs the math, and the
-// block's registers are shared by the consumer warps alone.
+// Key ring without a producer warp (ring.cuh): every warp runs the math, and
+// the block's registers are shared by the consumer warps alone.
 template <int P, int S>
 __global__ void __launch_bounds__(4 * P * 32, 1) pbs02_f64_kernel(Pbs02Args a)
 {
     using L = Pbs02Smem<P, S>;
     constexpr int W = 4 * P;   // warps, all consumers
     extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem);
-    int *relcnt = reinterpret_cast<int *>(smem + L::CNT_OFF);
-    int *issued = reinterpret_cast<int *>(smem + L::ISSUED_OFF);
-    double2 *ring = reinterpret_cast<double2 *>(smem + L::RING_OFF);
     Fft1024Tables *T = reinterpret_cast<Fft1024Tables *>(smem + L::TAB_OFF);
-    // The four warps of a ciphertext meet at named barriers, so a warp that
-    // gives up a bounded wait must not leave: it raises `abort`, after which
-    // every warp skips the remaining waits, no further chunk is issued, and
-    // all warps run to the end of the kernel.
-    volatile int *abort_flag = reinterpret_cast<volatile int *>(smem + L::ABORT_OFF);
-
     const int ngroups = (a.B + P - 1) / P;
-    const int nmine = (int)blockIdx.x < ngroups ? (ngroups - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     constexpr int CHUNKS = N0 * 2 * L2 * 2;
-    const uint32_t total = (uint32_t)nmine * CHUNKS;
-    auto issue = [&](uint32_t ch) {
-        const int slot = ch % S;
-        ++issued[slot];
-        mbar_arrive_expect_tx(&full[slot], L::CHUNK_BYTES);
-        bulk_g2s(ring + slot * 1024, a.bk + (size_t)(ch % CHUNKS) * 1024, L::CHUNK_BYTES, &full[slot]);
-    };
+    KeyRing<S, L::CHUNK_BYTES, W> ring{reinterpret_cast<RingHeader *>(smem), smem + L::RING_OFF,
+                                    reinterpret_cast<const unsigned char *>(a.bk), (uint32_t)CHUNKS,
+                                    (uint32_t)groups_of_block(ngroups, blockIdx.x, gridDim.x) * CHUNKS};
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) {
-        *abort_flag = 0;
-        for (int s = 0; s < S; ++s) {
-            mbar_init(&full[s], 1);
-            relcnt[s] = 0;
-            issued[s] = 0;
-        }
-        fence_barrier_init();
-    }
+    if (threadIdx.x == 0) ring.init_by_thread0();
     {
         const double2 *src = reinterpret_cast<const double2 *>(a.tables);
         double2 *dst = reinterpret_cast<double2 *>(T);
         for (int i = threadIdx.x; i < (int)(sizeof(Fft1024Tables) / 16); i += blockDim.x) dst[i] = src[i];
     }
     __syncthreads();
-    if (threadIdx.x == 0)
-        for (uint32_t ch = 0; ch < (uint32_t)S && ch < total; ++ch) issue(ch);
+    if (threadIdx.x == 0) ring.prologue_by_thread0();
 
     const int gr = warp >> 2, t = threadIdx.x & (T2 - 1), bar = 1 + gr;
     unsigned char *pb = smem + L::GROUP_OFF + gr * L::PER_GROUP;
@@ -166,13 +137,8 @@ __global__ void __launch_bounds__(4 * P * 32, 1) pbs02_f64_kernel(Pbs02Args a)
                 }
 #pragma unroll
                 for (int o = 0; o < 2; ++o, ++c) {
-                    const int slot = c % S;
-                    if (!*abort_flag && !mbar_wait(&full[slot], (c / S) & 1)) {
-                        report_error(a.err, DEV_TIMEOUT_FULL);
-                        *abort_flag = 1;
-                    }
+                    const double2 *bkc = reinterpret_cast<const double2 *>(ring.acquire(c, a.err));
                     if (active) {
-                        const double2 *bkc = ring + slot * 1024;
                         if (o == 0) {
                             if (r == 0) {
 #pragma unroll
@@ -191,11 +157,7 @@ __global__ void __launch_bounds__(4 * P * 32, 1) pbs02_f64_kernel(Pbs02Args a)
                             }
                         }
                     }
-                    __syncwarp();
-                    if (lane == 0 && ring_release(&relcnt[slot], c / S, W) && c + S < total && !*abort_flag) {
-                        fence_proxy_async_smem();
-                        issue(c + S);
-                    }
+                    ring.release(c, lane);
                 }
             }
             if (active) {
@@ -213,14 +175,8 @@ __global__ void __launch_bounds__(4 * P * 32, 1) pbs02_f64_kernel(Pbs02Args a)
         }
         group_sync<T2>(bar);
     }
-    // After an abort some issued copies may still be landing: wait for the
-    // last chunk issued into every slot before the block's memory is released
-    // (each slot's copies complete in issue order).
     __syncthreads();
-    if (threadIdx.x == 0 && *abort_flag)
-        for (int s = 0; s < S; ++s)
-            if (issued[s] > 0 && !mbar_wait(&full[s], (uint32_t)(issued[s] - 1) & 1))
-                report_error(a.err, DEV_TIMEOUT_DRAIN);
+    if (threadIdx.x == 0) ring.drain_by_thread0(a.err);
 }
 
 // integer polynomials [rows][2][2048] (64-bit torus) -> chunk layout

@@ -15,12 +15,13 @@
 // key chunk, and 2 inverse transforms whose output is added into the
 // accumulator.  No grid-wide barrier: CTAs are independent.
 #include "pbs_common.cuh"
+#include "ring.cuh"
 
 namespace cfdb {
 
 template <int W, int S>
 struct Pbs01Smem {
-    static constexpr int RING_OFF = 128;
+    static constexpr int RING_OFF = RING_HEADER_BYTES;
     static constexpr int CHUNK_BYTES = 16384;  // one TRGSW row: 2 outputs x 512 complex x 16 B
     static constexpr int TAB_OFF = RING_OFF + S * CHUNK_BYTES;
     static constexpr int WARP_OFF = TAB_OFF + ((int)sizeof(Fft512Tables) + 127) / 128 * 128;
@@ -61,56 +62,27 @@ __device__ __forceinline__ void add_inverse_poly1(uint32_t *poly, const double2 
 }
 
 template <int W, int S>
-__global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_f64_kernel(Pbs01Args a)
+__global__ void __launch_bounds__(W * 32, 1) pbs01_f64_kernel(Pbs01Args a)
 {
     using L = Pbs01Smem<W, S>;
     extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem);
-    uint64_t *empty = full + S;
-    double2 *ring = reinterpret_cast<double2 *>(smem + L::RING_OFF);
     Fft512Tables *T = reinterpret_cast<Fft512Tables *>(smem + L::TAB_OFF);
+    const int ngroups = (a.B + W - 1) / W;
+    constexpr int CHUNKS = N0 * 2 * L1;
+    // key ring without a producer warp (ring.cuh)
+    KeyRing<S, L::CHUNK_BYTES, W> ring{reinterpret_cast<RingHeader *>(smem), smem + L::RING_OFF,
+                                    reinterpret_cast<const unsigned char *>(a.bk), (uint32_t)CHUNKS,
+                                    (uint32_t)groups_of_block(ngroups, blockIdx.x, gridDim.x) * CHUNKS};
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < S; ++s) {
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], W);
-        }
-        fence_barrier_init();
-    }
+    if (threadIdx.x == 0) ring.init_by_thread0();
     {
-        const double2 *src = reinterpret_cast<const double2 *>(a.tables);
-        double2 *dst = reinterpret_cast<double2 *>(T);
+        const float4 *src = reinterpret_cast<const float4 *>(a.tables);
+        float4 *dst = reinterpret_cast<float4 *>(T);
         for (int i = threadIdx.x; i < (int)(sizeof(Fft512Tables) / 16); i += blockDim.x) dst[i] = src[i];
     }
     __syncthreads();
-
-    const int ngroups = (a.B + W - 1) / W;
-    constexpr int CHUNKS = N0 * 2 * L1;
-
-    if (warp == W) {
-        // producer: one elected lane streams the key, chunk by chunk
-        if (lane == 0) {
-            uint32_t c = 0;
-            bool ok = true;
-            for (int g = blockIdx.x; g < ngroups && ok; g += gridDim.x) {
-                for (int ch = 0; ch < CHUNKS; ++ch, ++c) {
-                    const int slot = c % S;
-                    if (c >= (uint32_t)S && !mbar_wait(&empty[slot], ((c / S) - 1) & 1)) {
-                        report_error(a.err, DEV_TIMEOUT_EMPTY);
-                        ok = false;
-                        break;
-                    }
-                    mbar_arrive_expect_tx(&full[slot], L::CHUNK_BYTES);
-                    bulk_g2s(ring + slot * 1024, a.bk + (size_t)ch * 1024, L::CHUNK_BYTES, &full[slot]);
-                }
-            }
-            // no copy may still be in flight when the CTA exits
-            for (uint32_t k = (c > (uint32_t)S ? c - S : 0); k < c; ++k)
-                if (!mbar_wait(&full[k % S], (k / S) & 1)) report_error(a.err, DEV_TIMEOUT_DRAIN);
-        }
-        return;
-    }
+    if (threadIdx.x == 0) ring.prologue_by_thread0();
 
     unsigned char *wb = smem + L::WARP_OFF + warp * L::PER_WARP;
     double2 *xp = reinterpret_cast<double2 *>(wb);
@@ -139,16 +111,13 @@ __global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_f64_kernel(Pbs01Args a)
             double2 f0[16], f1[16];
 #pragma unroll 1
             for (int r = 0; r < 2 * L1; ++r, ++c) {
-                const int slot = c % S;
-                if (!mbar_wait(&full[slot], (c / S) & 1)) {
-                    report_error(a.err, DEV_TIMEOUT_FULL);
-                    return;
-                }
+                double2 v[16];
                 if (active) {
-                    double2 v[16];
                     load_digit_poly1(v, acc + (r / L1) * N1, ab, r % L1, lane, *T);
                     fft512_fwd(v, xp, *T, lane);
-                    const double2 *bkc = ring + slot * 1024;
+                }
+                const double2 *bkc = reinterpret_cast<const double2 *>(ring.acquire(c, a.err));
+                if (active) {
                     if (r == 0) {
 #pragma unroll
                         for (int s = 0; s < 16; ++s) {
@@ -163,8 +132,7 @@ __global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_f64_kernel(Pbs01Args a)
                         }
                     }
                 }
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&empty[slot]);
+                ring.release(c, lane);
             }
             if (active) {
                 fft512_inv(f0, xp, *T, lane);
@@ -181,39 +149,43 @@ __global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_f64_kernel(Pbs01Args a)
         }
         __syncwarp();
     }
+    __syncthreads();
+    if (threadIdx.x == 0) ring.drain_by_thread0(a.err);
 }
 
 template <int W, int S>
 static cudaError_t launch_pbs01_f64_t(const Pbs01Args &a, int grid, cudaStream_t st)
 {
     using L = Pbs01Smem<W, S>;
-    pbs01_f64_kernel<W, S><<<grid, (W + 1) * 32, L::TOTAL, st>>>(a);
+    pbs01_f64_kernel<W, S><<<grid, W * 32, L::TOTAL, st>>>(a);
     return cudaGetLastError();
 }
 
-// Persistent grid: min(groups, SMs) CTAs of W = 7 consumer warps + 1 producer
-// warp, each looping over groups of 7 ciphertexts.  8 warps put 2 warps on
-// each SM sub-partition, so every thread may hold 255 registers (the 16
-// complex FFT values plus two 16-complex frequency accumulators per lane);
-// 1,024 ciphertexts map to 147 CTAs, one wave on 148 SMs.
-constexpr int PBS01_W = 7, PBS01_S = 4;
+// Persistent grid: min(groups, SMs) CTAs of W warps (one ciphertext each, no
+// producer warp), each looping over groups of W ciphertexts.  At most 8 warps
+// keep 2 warps per SM sub-partition, so every thread may hold 255 registers
+// (the 16 complex FFT values plus two 16-complex frequency accumulators per
+// lane).  W = 7 or 8 is chosen per launch (pbs01_choose_w).
+constexpr int PBS01_S = 4;
 
-cudaError_t launch_pbs01_f64(const Pbs01Args &a, int num_sms, cudaStream_t st)
+cudaError_t launch_pbs01_f64(const Pbs01Args &a, int num_sms, int w, cudaStream_t st)
 {
     if (a.B <= 0) return cudaSuccess;
-    static_assert(Pbs01Smem<PBS01_W, PBS01_S>::TOTAL <= 227 * 1024, "shared memory budget");
-    const int groups = (a.B + PBS01_W - 1) / PBS01_W;
-    return launch_pbs01_f64_t<PBS01_W, PBS01_S>(a, groups < num_sms ? groups : num_sms, st);
+    static_assert(Pbs01Smem<8, PBS01_S>::TOTAL <= 227 * 1024, "shared memory budget");
+    const int groups = (a.B + w - 1) / w;
+    const int grid = groups < num_sms ? groups : num_sms;
+    return w == 7 ? launch_pbs01_f64_t<7, PBS01_S>(a, grid, st) : launch_pbs01_f64_t<8, PBS01_S>(a, grid, st);
 }
 
 // the dynamic shared-memory opt-in, set once per device when a context is
 // created (so no attribute call happens inside a stream capture)
 cudaError_t init_pbs01_f64()
 {
-    return cudaFuncSetAttribute(pbs01_f64_kernel<PBS01_W, PBS01_S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                Pbs01Smem<PBS01_W, PBS01_S>::TOTAL);
+    cudaError_t e = cudaFuncSetAttribute(pbs01_f64_kernel<7, PBS01_S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         Pbs01Smem<7, PBS01_S>::TOTAL);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(pbs01_f64_kernel<8, PBS01_S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                Pbs01Smem<8, PBS01_S>::TOTAL);
 }
-
-size_t pbs01_f64_smem_bytes() { return Pbs01Smem<PBS01_W, PBS01_S>::TOTAL; }
 
 }  // namespace cfdb

@@ -22,12 +22,15 @@
 // slots hold (hi, lo) float pairs in the same 16 KB per TRGSW row.
 #include "fft_f32.cuh"
 #include "pbs_common.cuh"
+#include "ring.cuh"
+
+#include <type_traits>
 
 namespace cfdb {
 
 template <int W, int S>
 struct Pbs01SplitSmem {
-    static constexpr int RING_OFF = 128;
+    static constexpr int RING_OFF = RING_HEADER_BYTES;
     static constexpr int CHUNK_BYTES = 16384;   // 16 slots x 2 outputs x 32 lanes x float4(hi, lo)
     static constexpr int TAB_OFF = RING_OFF + S * CHUNK_BYTES;
     static constexpr int WARP_OFF = TAB_OFF + ((int)sizeof(Fft512TablesF) + 127) / 128 * 128;
@@ -83,55 +86,35 @@ __device__ __forceinline__ void add_inverse_lo(uint32_t *poly, float2 v[16], flo
     }
 }
 
-template <int W, int S>
-__global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_split_kernel(Pbs01Args a)
+// W consumer warps, plus a producer warp when PRODUCER (ring.cuh has both
+// feeds; the launch picks per shape, see launch_pbs01_split)
+template <int W, int S, bool PRODUCER>
+__global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_kernel(Pbs01Args a)
 {
     using L = Pbs01SplitSmem<W, S>;
     extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem);
-    uint64_t *empty = full + S;
-    float4 *ring = reinterpret_cast<float4 *>(smem + L::RING_OFF);
     Fft512TablesF *T = reinterpret_cast<Fft512TablesF *>(smem + L::TAB_OFF);
+    const int ngroups = (a.B + W - 1) / W;
+    constexpr int CHUNKS = N0 * 2 * L1;
+    using Feed = std::conditional_t<PRODUCER, ProducerRing<S, L::CHUNK_BYTES, W>, KeyRing<S, L::CHUNK_BYTES, W>>;
+    Feed ring{reinterpret_cast<RingHeader *>(smem), smem + L::RING_OFF, reinterpret_cast<const unsigned char *>(a.bk),
+              (uint32_t)CHUNKS, (uint32_t)groups_of_block(ngroups, blockIdx.x, gridDim.x) * CHUNKS};
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < S; ++s) {
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], W);
-        }
-        fence_barrier_init();
-    }
+    if (threadIdx.x == 0) ring.init_by_thread0();
     {
         const float4 *src = reinterpret_cast<const float4 *>(a.tables);
         float4 *dst = reinterpret_cast<float4 *>(T);
         for (int i = threadIdx.x; i < (int)(sizeof(Fft512TablesF) / 16); i += blockDim.x) dst[i] = src[i];
     }
     __syncthreads();
-
-    const int ngroups = (a.B + W - 1) / W;
-    constexpr int CHUNKS = N0 * 2 * L1;
-    const float4 *bk = reinterpret_cast<const float4 *>(a.bk);
-
-    if (warp == W) {
-        if (lane == 0) {
-            uint32_t c = 0;
-            bool ok = true;
-            for (int g = blockIdx.x; g < ngroups && ok; g += gridDim.x) {
-                for (int ch = 0; ch < CHUNKS; ++ch, ++c) {
-                    const int slot = c % S;
-                    if (c >= (uint32_t)S && !mbar_wait(&empty[slot], ((c / S) - 1) & 1)) {
-                        report_error(a.err, DEV_TIMEOUT_EMPTY);
-                        ok = false;
-                        break;
-                    }
-                    mbar_arrive_expect_tx(&full[slot], L::CHUNK_BYTES);
-                    bulk_g2s(ring + slot * 1024, bk + (size_t)ch * 1024, L::CHUNK_BYTES, &full[slot]);
-                }
-            }
-            for (uint32_t k = (c > (uint32_t)S ? c - S : 0); k < c; ++k)
-                if (!mbar_wait(&full[k % S], (k / S) & 1)) report_error(a.err, DEV_TIMEOUT_DRAIN);
+    if constexpr (PRODUCER) {
+        if (warp == W) {
+            ring.run_producer(lane, a.err);
+            return;
         }
-        return;
+    } else {
+        if (threadIdx.x == 0) ring.prologue_by_thread0();
     }
 
     unsigned char *wb = smem + L::WARP_OFF + warp * L::PER_WARP;
@@ -161,16 +144,11 @@ __global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_split_kernel(Pbs01Args 
             float2 f0h[16], f0l[16], f1h[16], f1l[16];
 #pragma unroll 1
             for (int r = 0; r < 2 * L1; ++r, ++c) {
-                const int slot = c % S;
-                if (!mbar_wait(&full[slot], (c / S) & 1)) {
-                    report_error(a.err, DEV_TIMEOUT_FULL);
-                    return;
-                }
+                const float4 *bkc = reinterpret_cast<const float4 *>(ring.acquire(c, a.err));
                 if (active) {
                     float2 v[16];
                     load_digit_poly1_f(v, acc + (r / L1) * N1, ab, r % L1, lane, *T);
                     ffft512_fwd(v, xp, *T, lane);
-                    const float4 *bkc = ring + slot * 1024;
                     if (r == 0) {
 #pragma unroll
                         for (int s = 0; s < 16; ++s) {
@@ -191,8 +169,7 @@ __global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_split_kernel(Pbs01Args 
                         }
                     }
                 }
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&empty[slot]);
+                ring.release(c, lane);
             }
             if (active) {
                 add_inverse_hi(acc, f0h, xp, lane, *T);
@@ -209,25 +186,42 @@ __global__ void __launch_bounds__((W + 1) * 32, 1) pbs01_split_kernel(Pbs01Args 
         }
         __syncwarp();
     }
+    if constexpr (!PRODUCER) {
+        __syncthreads();
+        if (threadIdx.x == 0) ring.drain_by_thread0(a.err);
+    }
 }
 
-constexpr int PBS01S_W = 7, PBS01S_S = 6;
+constexpr int PBS01S_S = 6;
 
-cudaError_t launch_pbs01_split(const Pbs01Args &a, int num_sms, cudaStream_t st)
+// 7 ciphertexts per CTA run with a producer warp (8 warps), 8 per CTA without
+// one (8 warps): both keep 2 warps per SM sub-partition (up to 255 registers)
+template <int W>
+static cudaError_t launch_pbs01_split_t(const Pbs01Args &a, int grid, cudaStream_t st)
+{
+    constexpr bool PROD = W == 7;
+    using L = Pbs01SplitSmem<W, PBS01S_S>;
+    static_assert(L::TOTAL <= 227 * 1024, "shared memory budget");
+    pbs01_split_kernel<W, PBS01S_S, PROD><<<grid, (W + (PROD ? 1 : 0)) * 32, L::TOTAL, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pbs01_split(const Pbs01Args &a, int num_sms, int w, cudaStream_t st)
 {
     if (a.B <= 0) return cudaSuccess;
-    using L = Pbs01SplitSmem<PBS01S_W, PBS01S_S>;
-    static_assert(L::TOTAL <= 227 * 1024, "shared memory budget");
-    const int groups = (a.B + PBS01S_W - 1) / PBS01S_W;
-    pbs01_split_kernel<PBS01S_W, PBS01S_S>
-        <<<groups < num_sms ? groups : num_sms, (PBS01S_W + 1) * 32, L::TOTAL, st>>>(a);
-    return cudaGetLastError();
+    const int groups = (a.B + w - 1) / w;
+    const int grid = groups < num_sms ? groups : num_sms;
+    return w == 7 ? launch_pbs01_split_t<7>(a, grid, st) : launch_pbs01_split_t<8>(a, grid, st);
 }
 
 cudaError_t init_pbs01_split()
 {
-    return cudaFuncSetAttribute(pbs01_split_kernel<PBS01S_W, PBS01S_S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                Pbs01SplitSmem<PBS01S_W, PBS01S_S>::TOTAL);
+    cudaError_t e = cudaFuncSetAttribute(pbs01_split_kernel<7, PBS01S_S, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         Pbs01SplitSmem<7, PBS01S_S>::TOTAL);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(pbs01_split_kernel<8, PBS01S_S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                Pbs01SplitSmem<8, PBS01S_S>::TOTAL);
 }
 
 }  // namespace cfdb

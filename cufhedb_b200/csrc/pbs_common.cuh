@@ -68,9 +68,22 @@ struct Pbs01Args {
     int *err;
 };
 
-cudaError_t launch_pbs01_f64(const Pbs01Args &a, int num_sms, cudaStream_t st);
+// w: ciphertexts (warps) per CTA, 7 or 8
+cudaError_t launch_pbs01_f64(const Pbs01Args &a, int num_sms, int w, cudaStream_t st);
 // bk: split-precision key (float4 hi/lo chunk layout), tables: Fft512TablesF
-cudaError_t launch_pbs01_split(const Pbs01Args &a, int num_sms, cudaStream_t st);
+cudaError_t launch_pbs01_split(const Pbs01Args &a, int num_sms, int w, cudaStream_t st);
+
+// Launch shape of the lvl01 PBS: each CTA works through ceil(B / w / SMs)
+// passes of w ciphertexts, one pass taking pass_ms[w - 7]; the choice
+// minimises passes x pass time (ties go to w = 7, the lighter pass).
+inline int pbs01_choose_w(int B, int num_sms, const float pass_ms[2])
+{
+    auto cost = [&](int w) {
+        const int groups = (B + w - 1) / w;
+        return (float)((groups + num_sms - 1) / num_sms) * pass_ms[w - 7];
+    };
+    return cost(8) < cost(7) ? 8 : 7;
+}
 cudaError_t init_pbs01_f64();
 cudaError_t init_pbs01_split();
 

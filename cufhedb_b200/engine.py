@@ -134,6 +134,13 @@ class Engine:
         check(self.lib.cufhedb_encrypt_lvl2(self.ctx, seed, stream_id, idx0, _ptr(msg_dev), _ptr(out_dev), B,
                                             _stream(stream)))
 
+    def autotune_pbs01(self, precision: int = _lib.FP64):
+        """time one full pass of the lvl01 PBS with 7 and 8 ciphertexts per CTA;
+        later launches pick the faster shape for their batch.  Returns (ms7, ms8)."""
+        a, b = C.c_float(0.0), C.c_float(0.0)
+        check(self.lib.cufhedb_autotune_pbs01(self.ctx, precision, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def phase_lvl1(self, ct_dev, phase_dev, key_dev=None, stream=None):
         """decryption phases b - <a, s1> of lvl1 TLWEs (key: device words, or the key set's)"""
         B = ct_dev.numel() // (N1 + 1)

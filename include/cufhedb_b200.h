@@ -267,6 +267,16 @@ CUFHEDB_API int cufhedb_extprod_lvl1_host(cufhedb_ctx *ctx, const uint32_t *trlw
 CUFHEDB_API int cufhedb_gate_lvl1_host(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint32_t *cb, uint32_t *out, int B,
                            int precision);
 
+/* ---- launch-shape autotuner --------------------------------------------------- */
+/* Times one full pass of the lvl01 PBS kernel (uniform random lvl0 inputs,
+ * the loaded key) with 7 and with 8 ciphertexts per CTA for `precision`, and
+ * keeps the two pass times in the context: afterwards every lvl01 bootstrap
+ * launch (PBS, gates, operator chains) picks the shape with the least
+ * (passes x pass time) for its batch size.  Without a run both times count
+ * as equal.  Synchronous; call it outside stream capture.  No counterpart in
+ * the reference, which runs one ciphertext per launch. */
+CUFHEDB_API int cufhedb_autotune_pbs01(cufhedb_ctx *ctx, int precision, float *ms_w7, float *ms_w8);
+
 /* ---- diagnostics ------------------------------------------------------------ */
 /* measured CUDA-core FMA throughput (TFLOP/s) of `device`, FP64 (fp64 != 0) or
  * FP32: the roofline denominator of the bootstrapping kernels */

@@ -270,3 +270,29 @@ def test_split_key_from_tfhepp_fft_layout(oracle, keys, bkfft01, bk01):
     eng.load_bkfft_lvl01(bkfft01)
     assert np.array_equal(eng.export_bk_lvl01(), bk01)
     eng.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split32"])
+def test_autotuned_launch_shapes_decrypt(engine, oracle, keys, precision):
+    """The autotuner times both launch shapes; batches that land on either
+    shape (1,024 -> 7 per CTA, one pass of 8 per CTA on every SM -> 8) still
+    decrypt to the gate's truth table."""
+    import torch
+    from cufhedb_b200 import FP64, SPLIT32
+    prec = FP64 if precision == "fp64" else SPLIT32
+    ms7, ms8 = engine.autotune_pbs01(prec)
+    assert ms7 > 0 and ms8 > 0
+    _, s1, _ = keys
+    for B in (1024, 8 * engine.num_sms):
+        bits = torch.randint(0, 2, (2, B), generator=torch.Generator().manual_seed(B))
+        msg = torch.where(bits == 1, MU, -MU).to(torch.int32).cuda()
+        ca, cb = empty_dev(B * (N1 + 1)), empty_dev(B * (N1 + 1))
+        engine.encrypt_lvl1(SEED, 0x64, 0, msg[0].contiguous(), ca)
+        engine.encrypt_lvl1(SEED, 0x64, B, msg[1].contiguous(), cb)
+        out = empty_dev(B * (N1 + 1))
+        engine.gate_lvl1("AND", ca, cb, out, prec)
+        ph = empty_dev(B)
+        engine.phase_lvl1(out, ph)
+        engine.sync()
+        got = (ph > 0).cpu().numpy().astype(int)
+        assert np.array_equal(got, (bits[0] & bits[1]).numpy().astype(int))

@@ -91,6 +91,23 @@ def test_compare_lvl2_20bit_range_filter(eng_all, oracle, keys, op):
     assert np.array_equal(logic_bits(oracle, out, s1, B), TRUTH[op](x, np.full(B, c)).astype(int))
 
 
+@pytest.mark.parametrize("logic", [True, False])
+def test_compare_lvl2_30bit(eng_all, oracle, keys, logic):
+    """30-bit values (the reference's HomComp width): the longest MSB chain
+    (ImExtractMSB33), LOGIC and ARITHMETIC results."""
+    _, s1, s2 = keys
+    pb, B = 30, 32
+    rng = np.random.default_rng(65)
+    x = rng.integers(0, 2 ** pb, B); y = rng.integers(0, 2 ** pb, B)
+    y[:4] = x[:4]
+    c1, c2 = enc2(oracle, s2, x, pb, 2000), enc2(oracle, s2, y, pb, 3000)
+    out = _empty1(B)
+    eng_all.compare("ge", 2, _dev(c1), _dev(c2), out, pb, logic=logic)
+    eng_all.sync()
+    got = logic_bits(oracle, out, s1, B) if logic else arith_bits(oracle, out, s1, B)
+    assert np.array_equal(got, (x >= y).astype(int))
+
+
 def test_compare_arithmetic_result_and_gates(eng_all, oracle, keys):
     _, s1, _ = keys
     pb, B = 5, 32
