@@ -47,7 +47,7 @@ WORKLOAD = ("1,024 lvl1 HomNAND gate bootstraps (IKS10 + PBS01 each) over unifor
             "TFHEpp 128-bit params (n=672, N=1024, l=3, Bg=2^6, IKS10 basebit 10 t 2)")
 # DRAM bytes (read + write) of one 1,024-ciphertext PBS launch, from the ncu
 # captures summarised under profiles/ (pbs01_*_batch1024.md)
-TRAFFIC = {"split32": 69_178_624 + 3_230_464, "fp64": 69_528_064 + 4_634_880}
+TRAFFIC = {"split32": 69_423_872 + 3_995_392, "fp64": 69_177_856 + 4_107_776}
 
 
 def parse(argv=None):
@@ -72,6 +72,8 @@ def parse(argv=None):
                    help="run only the PBS kernel on `--batch` random lvl0 inputs (bootstrapping key only, "
                         "a few hundred MB on the device): the small case for ncu captures")
     p.add_argument("--level", type=int, choices=[1, 2], default=1, help="PBS level for --profile-pbs")
+    p.add_argument("--profile-iks", type=int, choices=[10, 20, 21], default=0,
+                   help="run only the identity key switch of this kind on `--batch` random inputs (its key only)")
     return p.parse_args(argv)
 
 
@@ -618,9 +620,47 @@ def run_profile_pbs(args):
     eng.close()
 
 
+def run_profile_iks(args):
+    """--steps launches of one identity key switch alone (lvl10: 5.6 GB key,
+    lvl20: 11.3 GB, lvl21: 0.59 GB)."""
+    import torch
+    from cufhedb_b200 import GEN_KSK10, GEN_KSK20, GEN_KSK21, Engine
+    flags = {10: GEN_KSK10, 20: GEN_KSK20, 21: GEN_KSK21}[args.profile_iks]
+    eng = Engine(0)
+    eng.keygen(SEED, flags)
+    g = torch.Generator(device="cuda").manual_seed(98)
+    if args.profile_iks == 10:
+        x = torch.randint(-2 ** 31, 2 ** 31, (args.batch * (N1 + 1),), generator=g, device="cuda",
+                          dtype=torch.int64).to(torch.int32)
+        rows, width = 2 * N1, N0 + 1
+    else:
+        x = torch.randint(-2 ** 62, 2 ** 62, (args.batch * (N2 + 1),), generator=g, device="cuda", dtype=torch.int64)
+        rows, width = (2 * N2, N0 + 1) if args.profile_iks == 20 else (10 * N2, N1 + 1)
+    out = torch.empty(args.batch * width, dtype=torch.int32, device="cuda")
+    fn = lambda: eng.iks(args.profile_iks, x, out)
+    for _ in range(args.warmup):
+        fn()
+    ev = _events(args.steps)
+    for e0, e1 in ev:
+        e0.record()
+        fn()
+        e1.record()
+    eng.sync()
+    ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+    # algorithmic bytes: every selected key row (uniform inputs select a non-zero digit
+    # with probability 1 - 2^-basebit) of `width` words, per ciphertext
+    row_bytes = width * 4
+    print(json.dumps({"profile": f"iks{args.profile_iks}", "batch": args.batch, "ms": ms,
+                      "algorithmic_bytes_per_ct_max": rows * row_bytes,
+                      "gbs_at_max_rows": args.batch * rows * row_bytes / (statistics.median(ms) / 1000.0) / 1e9}))
+    eng.close()
+
+
 def main():
     args = parse()
-    if args.profile_pbs:
+    if args.profile_iks:
+        run_profile_iks(args)
+    elif args.profile_pbs:
         run_profile_pbs(args)
     elif args.filter_only:
         run_filter_only(args)
