@@ -72,6 +72,13 @@ def parse(argv=None):
                    help="run only the PBS kernel on `--batch` random lvl0 inputs (bootstrapping key only, "
                         "a few hundred MB on the device): the small case for ncu captures")
     p.add_argument("--level", type=int, choices=[1, 2], default=1, help="PBS level for --profile-pbs")
+    p.add_argument("--agg-rows", type=int, default=0,
+                   help="run only the filter + grouped aggregate query (3 range predicates, 6 groups) over this "
+                        "many rows, its operator DAG captured as one CUDA graph")
+    p.add_argument("--queue", type=int, default=0,
+                   help="run only a queue of this many filter queries, rows log-uniform in [2^8, --queue-max-rows], "
+                        "widths uniform in {8, 16, 24, 32}")
+    p.add_argument("--queue-max-rows", type=int, default=65536)
     p.add_argument("--profile-iks", type=int, choices=[10, 20, 21], default=0,
                    help="run only the identity key switch of this kind on `--batch` random inputs (its key only)")
     return p.parse_args(argv)
@@ -656,9 +663,49 @@ def run_profile_iks(args):
     eng.close()
 
 
+def _engine_all_keys_tuned():
+    from cufhedb_b200 import FP64, GEN_ALL, SPLIT32, Engine
+    eng = Engine(0)
+    eng.keygen(SEED, GEN_ALL)
+    tune = {name: eng.autotune_pbs01(p) for name, p in (("split32", SPLIT32), ("fp64", FP64))}
+    return eng, tune
+
+
+def run_agg(args):
+    from cufhedb_b200 import FP64, SPLIT32
+    from cufhedb_b200.queries import filter_group_aggregate
+    eng, tune = _engine_all_keys_tuned()
+    prec = FP64 if args.precision == "fp64" else SPLIT32
+    r = filter_group_aggregate(eng, args.agg_rows, prec, steps=max(1, min(args.steps, 3)))
+    print(json.dumps({"workload": "filter (date range at lvl2, discount range, quantity bound) + 3 x 2 groups, "
+                                  "SUM(price * (1 - discount)) and COUNT after decryption; DAG replayed as a CUDA graph",
+                      "precision": args.precision, "autotune_pass_ms": tune, **r}))
+    eng.close()
+
+
+def run_queue_bench(args):
+    import numpy as np
+    from cufhedb_b200 import FP64, SPLIT32
+    from cufhedb_b200.queries import run_queue
+    eng, tune = _engine_all_keys_tuned()
+    prec = FP64 if args.precision == "fp64" else SPLIT32
+    rng = np.random.default_rng(64)
+    lo, hi = np.log(2.0 ** 8), np.log(float(args.queue_max_rows))
+    queries = [(int(round(np.exp(rng.uniform(lo, hi)))), int(rng.choice([8, 16, 24, 32]))) for _ in range(args.queue)]
+    r = run_queue(eng, queries, prec)
+    print(json.dumps({"workload": f"{args.queue} filter queries x <= c, rows log-uniform in [2^8, {args.queue_max_rows}], "
+                                  "widths uniform in {8, 16, 24, 32}, packed by width",
+                      "precision": args.precision, "autotune_pass_ms": tune, **r}))
+    eng.close()
+
+
 def main():
     args = parse()
-    if args.profile_iks:
+    if args.agg_rows:
+        run_agg(args)
+    elif args.queue:
+        run_queue_bench(args)
+    elif args.profile_iks:
         run_profile_iks(args)
     elif args.profile_pbs:
         run_profile_pbs(args)
