@@ -1,6 +1,8 @@
 // C ABI of the engine (include/cufhedb_b200.h): context, key material,
 // batched operations and host-buffer entry points.
+#include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -444,6 +446,94 @@ int cufhedb_load_ksk(cufhedb_ctx *ctx, int kind, const uint32_t *ksk)
     int rc = ensure_alloc((void **)&ctx->ksk[slot], bytes);
     if (rc) return rc;
     CK(cudaMemcpy(ctx->ksk[slot], ksk, bytes, cudaMemcpyHostToDevice));
+    return CUFHEDB_OK;
+}
+
+// ---- key files (the reference's raw layout, test/HE3_Query/fastR.h:6-74) -----
+
+namespace {
+
+// whole-file sizes of the three sections
+constexpr size_t KF_SK_BYTES = (size_t)N1 * 4;
+constexpr size_t KF_BK_BYTES = BK01_WORDS * sizeof(double);
+constexpr size_t KF_KSK_BYTES = (size_t)1024 * 2 * 1023 * (N0 + 1) * 4;
+constexpr size_t KF_CHUNK = (size_t)64 << 20;   // host staging for the key-switching key
+
+struct FileCloser {
+    FILE *f;
+    ~FileCloser()
+    {
+        if (f) fclose(f);
+    }
+};
+
+struct PinnedBuf {
+    void *p = nullptr;
+    ~PinnedBuf() { cudaFreeHost(p); }
+};
+
+}  // namespace
+
+int cufhedb_load_keyfile(cufhedb_ctx *ctx, const char *path, uint32_t *sk_out)
+{
+    NEED(ctx && path, "null argument");
+    FileCloser fc{fopen(path, "rb")};
+    if (!fc.f) return fail(CUFHEDB_ERR_ARG, std::string("cannot open key file ") + path);
+    if (fseeko(fc.f, 0, SEEK_END) != 0) return fail(CUFHEDB_ERR_ARG, "cannot size key file");
+    const off_t size = ftello(fc.f);
+    if (size != (off_t)(KF_SK_BYTES + KF_BK_BYTES + KF_KSK_BYTES))
+        return fail(CUFHEDB_ERR_ARG, "key file size is not secret key + BootstrappingKeyFFT<lvl01> + "
+                                     "KeySwitchingKey<lvl10>");
+    rewind(fc.f);
+    std::vector<uint32_t> sk(N1);
+    if (fread(sk.data(), 1, KF_SK_BYTES, fc.f) != KF_SK_BYTES) return fail(CUFHEDB_ERR_ARG, "short read (sk)");
+    std::vector<double> bk(BK01_WORDS);
+    if (fread(bk.data(), 1, KF_BK_BYTES, fc.f) != KF_BK_BYTES) return fail(CUFHEDB_ERR_ARG, "short read (bkfft)");
+    int rc = cufhedb_load_bkfft_lvl01(ctx, bk.data());
+    if (rc) return rc;
+    DeviceGuard g(ctx->device);
+    rc = ensure_alloc((void **)&ctx->ksk[0], KF_KSK_BYTES);
+    if (rc) return rc;
+    PinnedBuf buf;
+    CK(cudaMallocHost(&buf.p, KF_CHUNK));
+    for (size_t off = 0; off < KF_KSK_BYTES; off += KF_CHUNK) {
+        const size_t n = std::min(KF_CHUNK, KF_KSK_BYTES - off);
+        if (fread(buf.p, 1, n, fc.f) != n) return fail(CUFHEDB_ERR_ARG, "short read (key-switching key)");
+        CK(cudaMemcpy(reinterpret_cast<char *>(ctx->ksk[0]) + off, buf.p, n, cudaMemcpyHostToDevice));
+    }
+    if (sk_out) std::memcpy(sk_out, sk.data(), KF_SK_BYTES);
+    return CUFHEDB_OK;
+}
+
+int cufhedb_save_keyfile(cufhedb_ctx *ctx, const char *path, const uint32_t *sk)
+{
+    NEED(ctx && path, "null argument");
+    if (!ctx->bk01_int) return fail(CUFHEDB_ERR_NOKEY, "lvl01 bootstrapping key not loaded");
+    if (!ctx->ksk[0]) return fail(CUFHEDB_ERR_NOKEY, "lvl10 key-switching key not loaded");
+    DeviceGuard g(ctx->device);
+    std::vector<uint32_t> skw(N1, 0u);
+    if (sk) std::memcpy(skw.data(), sk, KF_SK_BYTES);
+    else if (ctx->have_sk) CK(cudaMemcpy(skw.data(), ctx->s1_d, KF_SK_BYTES, cudaMemcpyDeviceToHost));
+    // TFHEpp's BootstrappingKeyFFT<lvl01param>: TwistIFFT of every key polynomial
+    double *fd = nullptr;
+    CK(cudaMalloc((void **)&fd, KF_BK_BYTES));
+    std::vector<double> bk(BK01_WORDS);
+    cudaError_t e = launch_twist_ifft1(fd, ctx->bk01_int, (int)(BK01_ROWS * 2), ctx->tab512, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(bk.data(), fd, KF_BK_BYTES, cudaMemcpyDeviceToHost);
+    cudaFree(fd);
+    if (e != cudaSuccess) return cuda_fail(e, "save_keyfile (bkfft)");
+    FileCloser fc{fopen(path, "wb")};
+    if (!fc.f) return fail(CUFHEDB_ERR_ARG, std::string("cannot create key file ") + path);
+    if (fwrite(skw.data(), 1, KF_SK_BYTES, fc.f) != KF_SK_BYTES || fwrite(bk.data(), 1, KF_BK_BYTES, fc.f) != KF_BK_BYTES)
+        return fail(CUFHEDB_ERR_ARG, "short write");
+    PinnedBuf buf;
+    CK(cudaMallocHost(&buf.p, KF_CHUNK));
+    for (size_t off = 0; off < KF_KSK_BYTES; off += KF_CHUNK) {
+        const size_t n = std::min(KF_CHUNK, KF_KSK_BYTES - off);
+        CK(cudaMemcpy(buf.p, reinterpret_cast<const char *>(ctx->ksk[0]) + off, n, cudaMemcpyDeviceToHost));
+        if (fwrite(buf.p, 1, n, fc.f) != n) return fail(CUFHEDB_ERR_ARG, "short write (key-switching key)");
+    }
+    if (fflush(fc.f) != 0) return fail(CUFHEDB_ERR_ARG, "flush failed");
     return CUFHEDB_OK;
 }
 

@@ -158,15 +158,41 @@ __device__ __forceinline__ void cx_dft8(C v[8])
     for (int i = 0; i < 8; ++i) v[i] = x[i];
 }
 
+// ---- the negacyclic twist, split in two ------------------------------------------
+// The twist factor of input m = t + T j is w^m = w^t * W_32^j (w = exp(2 pi i
+// / 4M), 4M = 32 T).  W_32^j is a compile-time constant per register j, and
+// w^t is common to the 8 values of thread t, so it commutes with stage A's
+// 8-point DFT and is folded into that stage's twiddle table.  The kernels
+// therefore multiply their inputs by W_32^j (cx_w32) and no twist table is
+// read at all.
+__host__ __device__ constexpr double w32_cos(int j)
+{
+    return j == 0 ? 1.0 : j == 1 ? 0.98078528040323044913 : j == 2 ? 0.92387953251128675613
+         : j == 3 ? 0.83146961230254523708 : j == 4 ? 0.70710678118654752440 : j == 5 ? 0.55557023301960222474
+         : j == 6 ? 0.38268343236508977173 : j == 7 ? 0.19509032201612826785 : 0.0;
+}
+__host__ __device__ constexpr double w32_sin(int j) { return w32_cos(8 - j); }
+
+// a * W_32^j (S = +1) or a * conj(W_32^j) (S = -1); j < 8 known after unrolling
+template <int S, typename C>
+__device__ __forceinline__ C cx_w32(C a, int j)
+{
+    using R = typename cx_real<C>::type;
+    if (j == 0) return a;
+    const R c = (R)w32_cos(j), s = (R)(S > 0 ? w32_sin(j) : -w32_sin(j));
+    C r;
+    r.x = a.x * c - a.y * s;
+    r.y = a.x * s + a.y * c;
+    return r;
+}
+
 // ---- tables ---------------------------------------------------------------------
-//   twist[j T + t] = w^{t + T j}          (M entries)
-//   twA[k T + t]   = W_M^{t k}            (M entries, k < 8)
+//   twA[k T + t]   = w^t W_M^{t k}        (M entries, k < 8: stage A twiddle with the twist's w^t)
 //   twB[q1 L + a]  = W_T^{a q1}           (8 L = T entries)
 //   wC[j]          = W_L^j, j < L / 2
 template <typename C, int T>
 struct Fft8xTables {
     static constexpr int M = 8 * T, L = T / 8;
-    C twist[M];
     C twA[M];
     C twB[T];
     C wC[L / 2];
@@ -182,11 +208,8 @@ inline void build_fft8x_tables(Fft8xTables<double2, T> &tab)
         const long double a = 2.0L * PI * (long double)num / (long double)den;
         return make_double2((double)cosl(a), (double)sinl(a));
     };
-    for (int j = 0; j < 8; ++j)
-        for (int t = 0; t < T; ++t) {
-            tab.twist[j * T + t] = cis(t + T * j, 4 * M);
-            tab.twA[j * T + t] = cis((long long)(t * j) % M, M);
-        }
+    for (int k = 0; k < 8; ++k)
+        for (int t = 0; t < T; ++t) tab.twA[k * T + t] = cis((long long)t * (1 + 4 * k) % (4 * M), 4 * M);
     for (int q1 = 0; q1 < 8; ++q1)
         for (int a = 0; a < L; ++a) tab.twB[q1 * L + a] = cis((long long)(a * q1) % T, T);
     for (int j = 0; j < L / 2; ++j) tab.wC[j] = cis(j, L);
@@ -242,15 +265,16 @@ __device__ __forceinline__ int fft8x_xp(int t, int k)
     else return t * 8 + (k ^ ((t >> 1) & 7));
 }
 
-// forward: v[j] = z_{t + T j} in, v[s] = V(fft8x_freq<T>(t, s)) out.
-// xp: M-entry scratch shared by the group; bar: its named barrier.
+// forward: v[j] = z_{t + T j} / w^t in (the inputs multiplied by W_32^j only),
+// v[s] = V(fft8x_freq<T>(t, s)) out.  xp: M-entry scratch shared by the
+// group; bar: its named barrier.
 template <typename C, int T>
 __device__ __forceinline__ void fft8x_fwd(C v[8], C *xp, const Fft8xTables<C, T> &tab, int t, int bar)
 {
     constexpr int L = T / 8, NST = ilog2c(L);
     cx_dft8<1>(v);
 #pragma unroll
-    for (int k = 1; k < 8; ++k) v[k] = cx_mul(v[k], tab.twA[k * T + t]);
+    for (int k = 0; k < 8; ++k) v[k] = cx_mul(v[k], tab.twA[k * T + t]);
     group_sync<T>(bar);
 #pragma unroll
     for (int k = 0; k < 8; ++k) xp[fft8x_xp<C>(t, k)] = v[k];
@@ -279,7 +303,8 @@ __device__ __forceinline__ void fft8x_fwd(C v[8], C *xp, const Fft8xTables<C, T>
     }
 }
 
-// inverse: v[s] = V(fft8x_freq<T>(t, s)) in, v[j] = M z_{t + T j} out
+// inverse: v[s] = V(fft8x_freq<T>(t, s)) in, v[j] = M z_{t + T j} / w^t out
+// (callers multiply by conj(W_32^j) to finish the untwist)
 template <typename C, int T>
 __device__ __forceinline__ void fft8x_inv(C v[8], C *xp, const Fft8xTables<C, T> &tab, int t, int bar)
 {
@@ -311,7 +336,7 @@ __device__ __forceinline__ void fft8x_inv(C v[8], C *xp, const Fft8xTables<C, T>
 #pragma unroll
     for (int kk = 0; kk < 8; ++kk) v[kk] = xp[fft8x_xp<C>(t, kk)];
 #pragma unroll
-    for (int kk = 1; kk < 8; ++kk) v[kk] = cx_mulc(v[kk], tab.twA[kk * T + t]);
+    for (int kk = 0; kk < 8; ++kk) v[kk] = cx_mulc(v[kk], tab.twA[kk * T + t]);
     cx_dft8<-1>(v);
 }
 

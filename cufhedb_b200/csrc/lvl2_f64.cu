@@ -32,11 +32,12 @@ __device__ __forceinline__ long long digit_field2(uint64_t x, int d)
     return (long long)(x << (BGBIT2 * d)) >> (64 - BGBIT2);
 }
 
-// digit d of (X^a - 1) * poly (or of poly when ROT is false), twisted:
-// v[j] = (dig_d(m) + i dig_d(m+1024)) * w^m, m = t + 128 j
+// digit-extraction words of (X^a - 1) * poly (or of poly when ROT is false)
+// at m = t + 128 j and m + 1024: x = (c + offset + round) ^ DEC2_XOR, from
+// which every digit is two shifts (all four digits of a polynomial from one
+// load of the accumulator)
 template <bool ROT>
-__device__ __forceinline__ void digits2(double2 v[8], const uint64_t *poly, uint32_t abar, int d, int t,
-                                        const Fft1024Tables &T)
+__device__ __forceinline__ void digit_words2(uint64_t x[16], const uint64_t *poly, uint32_t abar, int t)
 {
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
@@ -46,19 +47,27 @@ __device__ __forceinline__ void digits2(double2 v[8], const uint64_t *poly, uint
             c0 = rot_coef<N2>(poly, m, abar) - c0;
             c1 = rot_coef<N2>(poly, m + 1024, abar) - c1;
         }
-        const long long d0 = digit_field2((c0 + DEC2_OFFSET + DEC2_ROUND) ^ DEC2_XOR, d);
-        const long long d1 = digit_field2((c1 + DEC2_OFFSET + DEC2_ROUND) ^ DEC2_XOR, d);
-        v[j] = cx_mul(make_double2((double)d0, (double)d1), T.twist[j * T2 + t]);
+        x[2 * j] = (c0 + DEC2_OFFSET + DEC2_ROUND) ^ DEC2_XOR;
+        x[2 * j + 1] = (c1 + DEC2_OFFSET + DEC2_ROUND) ^ DEC2_XOR;
     }
 }
 
+// digit d, twisted by W_32^j (fft8x folds the rest of the twist):
+// v[j] = (dig_d(m) + i dig_d(m+1024)) * W_32^j, m = t + 128 j
+__device__ __forceinline__ void digits2(double2 v[8], const uint64_t x[16], int d)
+{
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+        v[j] = cx_w32<1>(make_double2((double)digit_field2(x[2 * j], d), (double)digit_field2(x[2 * j + 1], d)), j);
+}
+
 // poly[m] += round-toward-zero of the inverse transform, m = t + 128 j
-__device__ __forceinline__ void add_inverse2(uint64_t *poly, const double2 v[8], int t, const Fft1024Tables &T)
+__device__ __forceinline__ void add_inverse2(uint64_t *poly, const double2 v[8], int t)
 {
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         const int m = t + T2 * j;
-        const double2 y = cx_mulc(v[j], T.twist[j * T2 + t]);
+        const double2 y = cx_w32<-1>(v[j], j);
         poly[m] += f64_to_torus64(y.x * (1.0 / 1024.0));
         poly[m + 1024] += f64_to_torus64(y.y * (1.0 / 1024.0));
     }
@@ -128,11 +137,13 @@ __global__ void __launch_bounds__(4 * P * 32, 1) pbs02_f64_kernel(Pbs02Args a)
             const uint32_t ab = valid ? abar_s[i] : 0u;
             const bool active = ab != 0;
             double2 f0[8], f1[8];
+            uint64_t xw[16];
 #pragma unroll 1
             for (int r = 0; r < 2 * L2; ++r) {
                 double2 v[8];
                 if (active) {
-                    digits2<true>(v, acc + (r / L2) * N2, ab, r % L2, t, *T);
+                    if (r % L2 == 0) digit_words2<true>(xw, acc + (r / L2) * N2, ab, t);
+                    digits2(v, xw, r % L2);
                     fft8x_fwd<double2, T2>(v, xp, *T, t, bar);
                 }
 #pragma unroll
@@ -162,9 +173,9 @@ __global__ void __launch_bounds__(4 * P * 32, 1) pbs02_f64_kernel(Pbs02Args a)
             }
             if (active) {
                 fft8x_inv<double2, T2>(f0, xp, *T, t, bar);
-                add_inverse2(acc, f0, t, *T);
+                add_inverse2(acc, f0, t);
                 fft8x_inv<double2, T2>(f1, xp, *T, t, bar);
-                add_inverse2(acc + N2, f1, t, *T);
+                add_inverse2(acc + N2, f1, t);
             }
             group_sync<T2>(bar);
         }
@@ -191,8 +202,7 @@ __global__ void __launch_bounds__(T2) bk_fft2_kernel(double2 *dst, const uint64_
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         const int m = t + T2 * j;
-        v[j] = cx_mul(make_double2(__ll2double_rn((long long)p[m]), __ll2double_rn((long long)p[m + 1024])),
-                      T->twist[j * T2 + t]);
+        v[j] = cx_w32<1>(make_double2(__ll2double_rn((long long)p[m]), __ll2double_rn((long long)p[m + 1024])), j);
     }
     fft8x_fwd<double2, T2>(v, xp_s, *T, t, 1);
     double2 *d = dst + poly * 1024;
@@ -225,8 +235,7 @@ __global__ void __launch_bounds__(T2) twist_ifft2_kernel(double *out, const uint
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         const int m = t + T2 * j;
-        v[j] = cx_mul(make_double2(__ll2double_rn((long long)x[m]), __ll2double_rn((long long)x[m + 1024])),
-                      T->twist[j * T2 + t]);
+        v[j] = cx_w32<1>(make_double2(__ll2double_rn((long long)x[m]), __ll2double_rn((long long)x[m + 1024])), j);
     }
     fft8x_fwd<double2, T2>(v, xp_s, *T, t, 1);
     double *o = out + p * N2;
@@ -255,7 +264,7 @@ __global__ void __launch_bounds__(T2) twist_fft2_kernel(uint64_t *out, const dou
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         const int m = t + T2 * j;
-        const double2 y = cx_mulc(v[j], T->twist[j * T2 + t]);
+        const double2 y = cx_w32<-1>(v[j], j);
         o[m] = f64_to_torus64(y.x * (1.0 / 1024.0));
         o[m + 1024] = f64_to_torus64(y.y * (1.0 / 1024.0));
     }
@@ -274,7 +283,9 @@ __global__ void __launch_bounds__(T2) extprod2_kernel(ExtProd2Args a)
 #pragma unroll 1
     for (int r = 0; r < 2 * L2; ++r) {
         double2 v[8];
-        digits2<false>(v, in + (r / L2) * N2, 0, r % L2, t, T);
+        uint64_t xw[16];
+        digit_words2<false>(xw, in + (r / L2) * N2, 0, t);
+        digits2(v, xw, r % L2);
         fft8x_fwd<double2, T2>(v, xp_s, T, t, 1);
         const double2 *g0 = g + ((size_t)r * 2) * 1024, *g1 = g0 + 1024;
         if (r == 0) {
@@ -296,7 +307,7 @@ __global__ void __launch_bounds__(T2) extprod2_kernel(ExtProd2Args a)
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         const int m = t + T2 * j;
-        const double2 y = cx_mulc(f0[j], T.twist[j * T2 + t]);
+        const double2 y = cx_w32<-1>(f0[j], j);
         o[m] = f64_to_torus64(y.x * (1.0 / 1024.0));
         o[m + 1024] = f64_to_torus64(y.y * (1.0 / 1024.0));
     }
@@ -304,13 +315,13 @@ __global__ void __launch_bounds__(T2) extprod2_kernel(ExtProd2Args a)
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         const int m = t + T2 * j;
-        const double2 y = cx_mulc(f1[j], T.twist[j * T2 + t]);
+        const double2 y = cx_w32<-1>(f1[j], j);
         o[N2 + m] = f64_to_torus64(y.x * (1.0 / 1024.0));
         o[N2 + m + 1024] = f64_to_torus64(y.y * (1.0 / 1024.0));
     }
 }
 
-constexpr int PBS02_P = 3, PBS02_S = 2;
+constexpr int PBS02_P = 3, PBS02_S = 3;
 
 }  // namespace
 

@@ -105,6 +105,17 @@ class Engine:
         ksk = np.ascontiguousarray(ksk, np.uint32)
         check(self.lib.cufhedb_load_ksk(self.ctx, kind, _ptr(ksk)))
 
+    def load_keyfile(self, path: str) -> np.ndarray:
+        """load the lvl01 bootstrapping key and lvl10 key-switching key from a
+        key file in the reference's raw layout; returns the stored lvl1 secret key"""
+        sk = np.zeros(N1, np.uint32)
+        check(self.lib.cufhedb_load_keyfile(self.ctx, path.encode(), _ptr(sk)))
+        return sk
+
+    def save_keyfile(self, path: str, sk=None):
+        skp = None if sk is None else _ptr(np.ascontiguousarray(sk, np.uint32))
+        check(self.lib.cufhedb_save_keyfile(self.ctx, path.encode(), skp))
+
     def export_bk_lvl01(self) -> np.ndarray:
         out = np.zeros(BK01_SHAPE, np.uint32)
         check(self.lib.cufhedb_export_bk_lvl01(self.ctx, _ptr(out)))

@@ -141,6 +141,16 @@ CUFHEDB_API int cufhedb_export_bk_lvl02(cufhedb_ctx *ctx, uint64_t *bk);
 CUFHEDB_API int cufhedb_export_ksk_rows(cufhedb_ctx *ctx, int kind, const uint64_t *rows, int n, uint32_t *out);
 /* the secret keys of the deterministic key set (host-only computation) */
 CUFHEDB_API int cufhedb_secret_keys(uint64_t seed, uint32_t *s0, uint32_t *s1, uint64_t *s2);
+/* Key files in the raw layout of the reference's query programs
+ * (test/HE3_Query/fastR.h:6-74): the lvl1 secret key (1024 x uint32), TFHEpp's
+ * BootstrappingKeyFFT<lvl01param> (672 x 6 x 2 x 1024 doubles) and
+ * KeySwitchingKey<lvl10param> (1024 x 2 x 1023 x 673 uint32), in that order,
+ * 5.71 GB.  load: uploads both keys (the key-switching key in 64 MB pieces)
+ * and copies the secret key to sk_out when it is not NULL; save: writes this
+ * context's lvl01 and lvl10 keys, with `sk` (1024 words), or the
+ * deterministic key set's lvl1 key when sk is NULL, or zeros. */
+CUFHEDB_API int cufhedb_load_keyfile(cufhedb_ctx *ctx, const char *path, uint32_t *sk_out);
+CUFHEDB_API int cufhedb_save_keyfile(cufhedb_ctx *ctx, const char *path, const uint32_t *sk);
 /* deterministic lvl1 TLWE encryptions of B messages (device arrays), counter
  * blocks idx0.. of generator stream `stream_id` (test/benchmark inputs) */
 CUFHEDB_API int cufhedb_encrypt_lvl1(cufhedb_ctx *ctx, uint64_t seed, uint64_t stream_id, uint64_t idx0, const uint32_t *msg,
