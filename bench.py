@@ -79,6 +79,9 @@ def parse(argv=None):
                    help="run only a queue of this many filter queries, rows log-uniform in [2^8, --queue-max-rows], "
                         "widths uniform in {8, 16, 24, 32}")
     p.add_argument("--queue-max-rows", type=int, default=65536)
+    p.add_argument("--arc-rows", type=int, default=0,
+                   help="run only the ArcEDB comparison measurement over this many rows")
+    p.add_argument("--arc-digits", type=int, default=2, help="radix-1024 digits per value for --arc-rows")
     p.add_argument("--profile-iks", type=int, choices=[10, 20, 21], default=0,
                    help="run only the identity key switch of this kind on `--batch` random inputs (its key only)")
     return p.parse_args(argv)
@@ -699,9 +702,105 @@ def run_queue_bench(args):
     eng.close()
 
 
+def _arc_model(op, xd, yd):
+    """plaintext result of the ArcEDB digit combination (the same rule the
+    GPU path and the reference compute): +mu iff true"""
+    def single(x, y):
+        return {"gt": x > y, "lt": x <= y, "eq": x == y}[op]
+    r = single(xd[0], yd[0])
+    for x, y in zip(xd[1:], yd[1:]):
+        if op == "eq":
+            r = r and x == y
+        else:
+            units = (2 if x == y else 0) + (4 if single(x, y) else -4) + (2 if r else -2) + 1
+            r = 1 <= units % 16 <= 7
+    return r
+
+
+def run_arc(args):
+    """ArcEDB comparisons (greater_than / less_than / equality over radix-1024
+    digits: TRLWE of mu X^x_d against TRGSW of X^-y_d) of --arc-rows rows,
+    FP64 and split; every output decrypted on the GPU and checked against the
+    plaintext model; the reference's TFHEpp composition (oracle/_ref) timed on
+    the host threads over a bounded sample."""
+    import numpy as np
+    import torch
+    from cufhedb_b200 import FP64, GEN_BK01, GEN_KSK10, SPLIT32, Engine
+    from oracle.oracle import Oracle, RefTFHEpp
+    rows, D = args.arc_rows, args.arc_digits
+    eng = Engine(0)
+    eng.keygen(SEED, GEN_BK01 | GEN_KSK10)
+    tune = {name: eng.autotune_pbs01(p) for name, p in (("split32", SPLIT32), ("fp64", FP64))}
+    o = Oracle()
+    s0, s1, s2 = o.secret_keys(SEED)
+    # 256 distinct encrypted rows (a quarter equal values, a quarter equal top
+    # digits), tiled to `rows`
+    nsamp = min(256, rows)
+    rng = np.random.default_rng(99)
+    xs = rng.integers(0, 1024 ** D, nsamp)
+    ys = rng.integers(0, 1024 ** D, nsamp)
+    ys[::4] = xs[::4]
+    top = 1024 ** (D - 1)
+    ys[1::4] = (xs[1::4] // top) * top + rng.integers(0, top, len(ys[1::4]))
+    dig = lambda v, d: (int(v) >> (10 * d)) & 1023
+    trl = np.stack([np.stack([o.arc_trlwe(dig(xs[i], d), s1, SEED, 0xB1, d * nsamp + i) for i in range(nsamp)])
+                    for d in range(D)])
+    g = np.stack([np.stack([o.arc_trgsw(dig(ys[i], d), s1, SEED, 0xB2, d * nsamp + i) for i in range(nsamp)])
+                  for d in range(D)])
+    idx = np.arange(rows) % nsamp
+    trl_d = torch.from_numpy(np.ascontiguousarray(trl[:, idx]).view(np.int32)).cuda()
+    g_d = torch.from_numpy(np.ascontiguousarray(g[:, idx]).view(np.int32)).cuda()
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")
+    out = torch.empty(rows * (N1 + 1), dtype=torch.int32, device="cuda")
+    ph = torch.empty(rows, dtype=torch.int32, device="cuda")
+    res = {}
+    for name, prec in (("split32", SPLIT32), ("fp64", FP64)):
+        prep = torch.empty(D * rows * 98304 // 8, dtype=torch.float64, device="cuda")
+        eng.trgsw_prepare_lvl1(g_d, prep, prec)
+        for op in ("gt", "lt", "eq"):
+            fn = lambda: eng.arc_compare(op, trl_d, prep, out, D, precision=prec, stream=stream)
+            for _ in range(max(3, args.warmup)):
+                fn()
+            ms = statistics.median(_timed(fn, max(3, min(args.steps, 10)), flush, stream))
+            eng.phase_lvl1(out, ph, stream=stream)
+            got = (ph > 0).cpu().numpy()
+            want = np.array([_arc_model(op, [dig(xs[i], d) for d in range(D)], [dig(ys[i], d) for d in range(D)])
+                             for i in range(nsamp)])[idx]
+            res[f"{op}_{name}"] = {"ms": ms, "rows_per_s": rows / (ms / 1000.0),
+                                   "decrypt_errors": int((got != want).sum())}
+        del prep
+    eng.close()
+    # the reference's composition on the host (TFHEpp from oracle/_ref)
+    nthreads = os.cpu_count() or 1
+    r = RefTFHEpp()
+    r.set_secret(s0, s1, s2)
+    r.set_bk01(o.bk01(SEED, s0, s1, nthreads))
+    ptr, _ = r.ksk_view(10)
+    o.ksk_full_into(10, SEED, (s0, s1, s2), ptr, nthreads)
+    ncpu = min(nsamp, max(2 * nthreads, 64))
+    gf = np.stack([np.stack([o.trgsw32_fft(g[d, i]) for i in range(ncpu)]) for d in range(D)])
+    t0 = time.perf_counter()
+    cout = r.arc_compare_batch("gt", np.ascontiguousarray(trl[:, :ncpu]), gf, nthreads)
+    cpu_rate = ncpu / (time.perf_counter() - t0)
+    cpu_sign = [(int(o.phase32(c, s1)) + 2 ** 31) % 2 ** 32 - 2 ** 31 > 0 for c in cout]
+    cpu_err = sum(int(sg != _arc_model("gt", [dig(xs[i], d) for d in range(D)], [dig(ys[i], d) for d in range(D)]))
+                  for i, sg in enumerate(cpu_sign))
+    r.close()
+    print(json.dumps({"workload": f"ArcEDB comparisons, {rows} rows x {D} radix-1024 digits "
+                                  f"({nsamp} distinct encrypted rows tiled), lvl1 TRLWE vs TRGSW",
+                      "per_row": {"external_products": D, "lvl01_bootstraps": D - 1, "iks10": D - 1},
+                      "autotune_pass_ms": tune, **res,
+                      "cpu_baseline": {"value": cpu_rate, "unit": "rows/s", "cores": nthreads, "kind": "reference",
+                                       "sample": f"{ncpu} greater_than rows, TFHEpp composition of "
+                                                 "comparable.cpp from oracle/_ref", "decrypt_errors": cpu_err}}))
+
+
 def main():
     args = parse()
-    if args.agg_rows:
+    if args.arc_rows:
+        run_arc(args)
+    elif args.agg_rows:
         run_agg(args)
     elif args.queue:
         run_queue_bench(args)

@@ -294,6 +294,15 @@ class Engine:
         check(self.lib.cufhedb_compare(self.ctx, _lib.COMPARE[op], level, _ptr(c1), _ptr(c2), _ptr(out),
                                        self._rows(c1, level), plain_bits, int(logic), precision, _stream(stream)))
 
+    ARC_OPS = {"gt": 0, "lt": 1, "eq": 2, "lt_strict": 3}
+
+    def arc_compare(self, op: str, trlwe_dev, trgsw_prepared, out_dev, digits: int, precision=_lib.FP64,
+                    stream=None):
+        """ArcEDB comparison of B rows of `digits` radix-1024 digits (digit-major layouts)"""
+        B = trlwe_dev.numel() // (digits * 2 * N1)
+        check(self.lib.cufhedb_arc_compare(self.ctx, self.ARC_OPS[op], _ptr(trlwe_dev), _ptr(trgsw_prepared),
+                                           _ptr(out_dev), B, digits, precision, _stream(stream)))
+
     def graph_begin(self, stream):
         check(self.lib.cufhedb_graph_begin(self.ctx, _stream(stream)))
 

@@ -259,6 +259,21 @@ CUFHEDB_API int cufhedb_compare(cufhedb_ctx *ctx, int op, int level, const void 
                                 uint32_t *out_lvl1, int B, uint32_t plain_bits, int logic, int precision,
                                 cufhedb_stream_t stream);
 
+/* ArcEDB comparisons (cuARCEDB::greater_than_tfhepp / less_than_tfhepp /
+ * equality_tfhepp, src/cuHEDB/comparable_gpu.cuh:52-168; CPU twins
+ * src/ARCEDB/comparison/comparable.cpp:506-729) of B rows of D radix-1024
+ * digits.  trlwe: D x B x [2][1024] uint32, the TRLWE of mu X^{x_d}
+ * (exponent_encrypt); trgsw: D x B prepared TRGSWs (98,304 bytes each, from
+ * cufhedb_trgsw_prepare_lvl1 / cufhedb_trgswfft_prepare_lvl1) of X^{-y_d}
+ * (exponent_encrypt_rgsw with is_negative); digit 0 least significant.
+ * op 0: greater_than (+mu iff x > y), 1: less_than exactly as the reference
+ * computes it (x_d <= y_d per digit; over several digits the lower digits'
+ * result is complemented when the top digits are equal), 2: equality,
+ * 3: strict less_than (x < y, combining like greater_than; no counterpart in
+ * the reference).  out: B lvl1 TLWEs (+-mu); D > 1 needs the lvl10 and lvl01 keys. */
+CUFHEDB_API int cufhedb_arc_compare(cufhedb_ctx *ctx, int op, const uint32_t *trlwe, const void *trgsw,
+                                    uint32_t *out, int B, int D, int precision, cufhedb_stream_t stream);
+
 /* ---- CUDA-graph capture of an operator DAG: everything enqueued on `stream`
  *      between begin and end (which must be a non-default stream) becomes one
  *      graph, replayed by cufhedb_graph_launch. */

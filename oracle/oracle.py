@@ -57,6 +57,7 @@ class Oracle:
         self._bk02 = _sig(L, "orc_bk02", [u64, _u32p, _u64p, _u64p, i32])
         self._trgsw32 = _sig(L, "orc_trgsw32", [_u32p, u32, _u32p, u64, u64, u64])
         self._trgsw64 = _sig(L, "orc_trgsw64", [_u64p, u64, _u64p, u64, u64, u64])
+        self._trlwe32 = _sig(L, "orc_trlwe32_encrypt", [_u32p, _u32p, _u32p, u64, u64, u64])
         self._k10row = _sig(L, "orc_ksk10_row", [u64, _u32p, _u32p, i32, i32, i32, _u32p])
         self._k20row = _sig(L, "orc_ksk20_row", [u64, _u64p, _u32p, i32, i32, i32, _u32p])
         self._k21row = _sig(L, "orc_ksk21_row", [u64, _u64p, _u32p, i32, i32, i32, _u32p])
@@ -112,6 +113,47 @@ class Oracle:
         g = np.zeros((2 * L2, 2, N2), np.uint64)
         self._trgsw64(g, m0, s2, seed, stream, idx)
         return g
+
+    def trlwe32(self, plain, s1, seed, stream, idx):
+        out = np.zeros((2, N1), np.uint32)
+        self._trlwe32(out, np.ascontiguousarray(plain, np.uint32), s1, seed, stream, idx)
+        return out
+
+    # ---- ArcEDB encodings and single-digit comparisons -----------------------
+    def arc_trlwe(self, v, s1, seed, stream, idx):
+        """exponent_encrypt<Lvl1> (src/ARCEDB/comparison/comparable.h:169-179):
+        the TRLWE of mu X^v, v in [0, N)"""
+        plain = np.zeros(N1, np.uint32)
+        plain[v] = MU1
+        return self.trlwe32(plain, s1, seed, stream, idx)
+
+    def arc_trgsw(self, v, s1, seed, stream, idx):
+        """exponent_encrypt_rgsw<Lvl1>(is_negative = true) (comparable.h:228-274):
+        the TRGSW of X^{-v}; -h_i at coefficient N - v, or +h_i at 0 when v = 0"""
+        g = self.trgsw32(0, s1, seed, stream, idx)
+        for i in range(L1):
+            h = np.uint32(1 << (32 - (i + 1) * BG1))
+            for k in range(2):
+                if v:
+                    g[i + k * L1, k, N1 - v] -= h
+                else:
+                    g[i + k * L1, k, 0] += h
+        return g
+
+    def arc_single(self, op, trlwe, g):
+        """greater_than_tfhepp / less_than_tfhepp / equality_tfhepp of one digit
+        (comparable.cpp:506-523, 652-666, 623-633) with the exact external
+        product; op "lt_strict" uses the test polynomial -1 + X + ... + X^{N-1}."""
+        t = self.extprod32_exact(trlwe, g)
+        if op == "eq":
+            out = sample_extract32(t) * np.uint32(2)
+            out[N1] -= np.uint32(MU1)
+            return out
+        p = np.ones(N1, np.uint32)
+        if op == "lt_strict":
+            p[0] = np.uint32(0xFFFFFFFF)
+        out = sample_extract32(np.stack([polymul32(t[0], p), polymul32(t[1], p)]))
+        return (np.uint32(0) - out) if op == "gt" else out
 
     def ksk_row(self, kind, seed, keys, i, j, k):
         s0, s1, s2 = keys
@@ -236,6 +278,26 @@ class Oracle:
         return out
 
 
+def sample_extract32(trlwe):
+    """SampleExtractIndex(index 0) (TFHEpp src/trlwe.cpp:108-118)"""
+    a, b = np.asarray(trlwe, np.uint32)
+    out = np.empty(N1 + 1, np.uint32)
+    out[0] = a[0]
+    out[1:N1] = np.uint32(0) - a[:0:-1]
+    out[N1] = b[0]
+    return out
+
+
+def polymul32(a, p):
+    """negacyclic a * p mod 2^32, exact (TFHEpp PolyMul, include/mulfft.hpp:124-153)"""
+    a = np.asarray(a, np.uint64)
+    full = np.zeros(2 * len(a), np.uint64)
+    for j, pj in enumerate(np.asarray(p, np.uint64)):
+        if pj:
+            full[j:j + len(a)] += a * pj
+    return (full[:len(a)] - full[len(a):]).astype(np.uint32)
+
+
 def ref_available() -> bool:
     return os.path.exists(os.path.join(HERE, "_ref", "libtfheref.so"))
 
@@ -277,6 +339,8 @@ class RefTFHEpp:
         _sig(L, "tref_compare_lvl1", [vp, _u32p, _u32p, _u32p, i32, u32, i32])
         _sig(L, "tref_compare_lvl2", [vp, _u32p, _u64p, _u64p, i32, u32, i32])
         _sig(L, "tref_homand", [vp, _u32p, _u32p, _u32p, i32])
+        _sig(L, "tref_arc_digit_lvl1", [_u32p, i32, _u32p, _f64p])
+        _sig(L, "tref_arc_compare_batch", [vp, _u32p, i32, _u32p, _f64p, i32, i32, i32])
         self.L = L
         self.ctx = L.tref_new()
 
@@ -351,6 +415,25 @@ class RefTFHEpp:
             out = np.zeros(N0 + 1, np.uint32); self.L.tref_iks20(self.ctx, out, np.ascontiguousarray(x, np.uint64))
         else:
             out = np.zeros(N1 + 1, np.uint32); self.L.tref_iks21(self.ctx, out, np.ascontiguousarray(x, np.uint64))
+        return out
+
+    ARC_DIGIT = {"gt": 0, "lt": 1, "eq": 2, "equal_term": 3}
+
+    def arc_digit(self, op, trlwe, gfft):
+        """one digit of the reference's ArcEDB comparison (TFHEpp steps of
+        comparable.cpp:506-523 / 652-666 / 623-633)"""
+        out = np.zeros(N1 + 1, np.uint32)
+        self.L.tref_arc_digit_lvl1(out, self.ARC_DIGIT[op], np.ascontiguousarray(trlwe, np.uint32),
+                                   np.ascontiguousarray(gfft, np.float64))
+        return out
+
+    def arc_compare_batch(self, op, trlwe, gfft, nthreads=1):
+        """the reference's multi-digit ArcEDB comparison of n rows (trlwe
+        D x n x 2 x N, gfft D x n TRGSWFFT); needs the lvl01 key and lvl10 key"""
+        D, n = trlwe.shape[:2]
+        out = np.zeros((n, N1 + 1), np.uint32)
+        self.L.tref_arc_compare_batch(self.ctx, out, self.ARC_DIGIT[op], np.ascontiguousarray(trlwe, np.uint32),
+                                      np.ascontiguousarray(gfft, np.float64), n, D, nthreads)
         return out
 
     def homnand(self, ca, cb):

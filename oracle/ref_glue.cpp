@@ -218,6 +218,40 @@ void tref_extprod_lvl2(uint64_t *res, const uint64_t *trlwe, const double *trgsw
     delete g;
 }
 
+// One digit of the ArcEDB comparisons exactly as src/ARCEDB/comparison/
+// comparable.cpp runs it with TFHEpp (that file itself needs SEAL, so its
+// TFHEpp steps are repeated here): op 0 greater_than_tfhepp (506-523),
+// 1 less_than_tfhepp (652-666), 2 equality_tfhepp (623-633), 3 the equal
+// term of the multi-digit order comparisons (537-538).
+void tref_arc_digit_lvl1(uint32_t *res, int op, const uint32_t *trlwe, const double *trgswfft)
+{
+    using P = lvl1param;
+    TRLWE<P> in, prod, mul;
+    TLWE<P> r;
+    auto *g = new TRGSWFFT<P>;
+    std::memcpy(in.data(), trlwe, sizeof(in));
+    std::memcpy(g->data(), trgswfft, sizeof(*g));
+    trgswfftExternalProduct<P>(prod, in, *g);
+    delete g;
+    if (op == 2 || op == 3) {
+        SampleExtractIndex<P>(r, prod, 0);
+        if (op == 2) {
+            for (size_t i = 0; i <= P::n; i++) r[i] = 2 * r[i];
+            r[P::n] -= P::μ;
+        }
+    } else {
+        Polynomial<P> test_plaintext;
+        for (size_t i = 0; i < P::n; i++) test_plaintext[i] = 1;
+        if (op == 1) test_plaintext[0] = P::plain_modulus - 1;
+        PolyMul<P>(mul[0], prod[0], test_plaintext);
+        PolyMul<P>(mul[1], prod[1], test_plaintext);
+        SampleExtractIndex<P>(r, mul, 0);
+        if (op == 0)
+            for (size_t i = 0; i <= P::n; i++) r[i] = -r[i];
+    }
+    std::memcpy(res, r.data(), sizeof(r));
+}
+
 // ---- PBS / IKS / gates ------------------------------------------------------
 void tref_pbs01(void *p, uint32_t *out, const uint32_t *in0, const uint32_t *tv)
 {
@@ -371,6 +405,51 @@ void tref_homand(void *p, uint32_t *res, const uint32_t *ca, const uint32_t *cb,
     std::memcpy(b.data(), cb, sizeof(b));
     HEDB::HomAND(r, a, b, c->ek, logic != 0);
     std::memcpy(res, r.data(), sizeof(r));
+}
+
+// Whole ArcEDB comparisons of n rows of D digits on `nthreads` host threads,
+// as comparable.cpp composes them from the single-digit functions (order
+// comparisons 525-557 / 668-698: equal term, doubled high digit, lower
+// result, mu/2, IdentityKeySwitch<lvl10>, GateBootstrappingTLWE2TLWEFFT<lvl01>
+// with mu; equality 635-650: TFHEpp::HomAND).  The top digit's external
+// product runs twice per digit, as there.  trlwe: D x n x [2][1024];
+// trgswfft: D x n TRGSWFFT<lvl1param>; op 0 gt, 1 lt, 2 eq.
+void tref_arc_compare_batch(void *p, uint32_t *res, int op, const uint32_t *trlwe, const double *trgswfft,
+                            int n, int D, int nthreads)
+{
+    using P = lvl1param;
+    RefCtx *c = static_cast<RefCtx *>(p);
+    const size_t tw = 2 * P::n, gw = sizeof(TRGSWFFT<P>) / sizeof(double), w = P::n + 1;
+    std::atomic<int> next(0);
+    auto work = [&]() {
+        for (;;) {
+            const int i = next.fetch_add(1);
+            if (i >= n) break;
+            auto x = [&](int d) { return trlwe + ((size_t)d * n + i) * tw; };
+            auto g = [&](int d) { return trgswfft + ((size_t)d * n + i) * gw; };
+            TLWE<P> r, hi, eq, sum;
+            TLWE<lvl0param> l0;
+            tref_arc_digit_lvl1(r.data(), op, x(0), g(0));
+            for (int d = 1; d < D; ++d) {
+                tref_arc_digit_lvl1(hi.data(), op, x(d), g(d));
+                if (op == 2) {
+                    HomAND<P>(sum, r, hi, c->ek);
+                    r = sum;
+                    continue;
+                }
+                tref_arc_digit_lvl1(eq.data(), 3, x(d), g(d));
+                for (size_t k = 0; k <= P::n; k++) sum[k] = eq[k] + 2 * hi[k] + r[k];
+                sum[P::n] += P::μ >> 1;
+                IdentityKeySwitch<lvl10param>(l0, sum, *c->ek.iksklvl10);
+                GateBootstrappingTLWE2TLWEFFT<lvl01param>(r, l0, *c->ek.bkfftlvl01, μpolygen<P, P::μ>());
+            }
+            std::memcpy(res + (size_t)i * w, r.data(), sizeof(r));
+        }
+    };
+    if (nthreads <= 1) { work(); return; }
+    std::vector<std::thread> th;
+    for (int t = 0; t < nthreads; t++) th.emplace_back(work);
+    for (auto &t : th) t.join();
 }
 
 }  // extern "C"

@@ -145,6 +145,15 @@ static void trlwe64_zero(uint64_t *c, int N, const uint64_t *key, int64_t ns,
     }
 }
 
+/* trlwe.cpp:30-37 (trlweSymEncrypt<lvl1param>): a TRLWE of zero with the
+ * plaintext polynomial added to b. */
+void orc_trlwe32_encrypt(uint32_t *out, const uint32_t *plain, const uint32_t *s1, uint64_t seed,
+                         uint64_t stream, uint64_t idx)
+{
+    trlwe32_zero(out, ORC_N1, s1, NS_LVL1, seed, stream, idx);
+    for (int j = 0; j < ORC_N1; j++) out[ORC_N1 + j] += plain[j];
+}
+
 /* trgsw.cpp:206-222 (trgswSymEncrypt) with plainpoly = {m0} as bkgen uses
  * (cloudkey.cpp:11-20): row r = i + k*l gets m0*h_i on poly k, coeff 0. */
 void orc_trgsw32(uint32_t *out, uint32_t m0, const uint32_t *s1, uint64_t seed,

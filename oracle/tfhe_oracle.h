@@ -56,6 +56,9 @@ uint64_t orc_tlwe64_phase(const uint64_t *c, int n, const uint64_t *key);
 /* bootstrapping keys (integer TRGSW form, [672][(k+1)l][2][N]) */
 void orc_bk01(uint64_t seed, const uint32_t *s0, const uint32_t *s1, uint32_t *bk, int nthreads);
 void orc_bk02(uint64_t seed, const uint32_t *s0, const uint64_t *s2, uint64_t *bk, int nthreads);
+/* a lvl1 TRLWE of the plaintext polynomial `plain` (trlwe.cpp:30-37) */
+void orc_trlwe32_encrypt(uint32_t *out, const uint32_t *plain, const uint32_t *s1, uint64_t seed,
+                         uint64_t stream, uint64_t idx);
 /* one TRGSW of the monomial-0 message m0 (cloudkey.cpp:11-20, trgsw.cpp:206-222) */
 void orc_trgsw32(uint32_t *out, uint32_t m0, const uint32_t *s1, uint64_t seed,
                  uint64_t stream, uint64_t idx);

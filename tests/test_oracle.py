@@ -142,3 +142,26 @@ def test_golden_vectors(oracle, keys):
     for x0, out in zip(g["pbs_in"][:2], g["pbs_out"][:2]):
         mine = oracle.pbs01(x0, bkf, tv)
         assert (signed_diff(oracle.phase32(mine, s1), 0) > 0) == (signed_diff(oracle.phase32(out, s1), 0) > 0)
+
+
+def test_arcedb_digit_matches_reference(oracle, ref, keys):
+    """The oracle's ArcEDB encodings and single-digit comparisons against the
+    reference's own TFHEpp steps (FFT external product and FFT PolyMul, so a
+    few torus units of rounding apart from the exact oracle)."""
+    _, s1, _ = keys
+    rng = np.random.default_rng(77)
+    pairs = [(0, 0), (0, 1), (1, 0), (5, 5), (1023, 0), (0, 1023), (512, 511), (1023, 1023)]
+    pairs += [tuple(int(v) for v in rng.integers(0, 1024, 2)) for _ in range(4)]
+    for i, (x, y) in enumerate(pairs):
+        trl = oracle.arc_trlwe(x, s1, SEED, 0xA1, i)
+        g = oracle.arc_trgsw(y, s1, SEED, 0xA2, i)
+        gfft = oracle.trgsw32_fft(g)
+        for op, truth in (("gt", x > y), ("lt", x <= y), ("eq", x == y)):
+            mine = oracle.arc_single(op, trl, g)
+            theirs = ref.arc_digit(op, trl, gfft)
+            assert np.max(np.abs(signed_diff(mine, theirs))) <= 256, (op, x, y)
+            assert (signed_diff(oracle.phase32(mine, s1), 0) > 0) == truth, (op, x, y)
+        strict = oracle.arc_single("lt_strict", trl, g)
+        assert (signed_diff(oracle.phase32(strict, s1), 0) > 0) == (x < y)
+        eq_term = signed_diff(oracle.phase32(ref.arc_digit("equal_term", trl, gfft), s1), 0)
+        assert abs(eq_term - (1 << 29 if x == y else 0)) < 1 << 26
