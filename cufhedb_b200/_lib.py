@@ -64,6 +64,8 @@ SIGNATURES = {
     "cufhedb_autotune_pbs01": [_vp, _i32, _vp, _vp],
     "cufhedb_load_keyfile": [_vp, C.c_char_p, _vp],
     "cufhedb_arc_compare": [_vp, _i32, _vp, _vp, _vp, _i32, _i32, _i32, _vp],
+    "cufhedb_polymul_lvl1": [_vp, _vp, _vp, _vp, _i32, _i32, _vp],
+    "cufhedb_polymul_lvl2": [_vp, _vp, _vp, _vp, _i32, _i32, _vp],
     "cufhedb_save_keyfile": [_vp, C.c_char_p, _vp],
     "cufhedb_phase_lvl2": [_vp, _vp, _vp, _vp, _i32, _vp],
     "cufhedb_pbs_lvl01": [_vp, _vp, _vp, _i32, C.POINTER(TestVec), _i32, _vp],

@@ -24,6 +24,8 @@
 // exactly like greater_than.
 #include "ctx.cuh"
 #include "extprod.cuh"
+#include "fftops.cuh"
+#include "lvl2.cuh"
 
 namespace cfdb {
 
@@ -102,6 +104,29 @@ __global__ void arc_combine_kernel(uint32_t *out, const uint32_t *eq, const uint
         if (e % (N1 + 1) == N1) v += MU >> 1;
         out[e] = v;
     }
+}
+
+// x_i <- x_i * m (pointwise, TFHEpp's frequency-domain layout: re in
+// [0, N/2), im in [N/2, N); MulInFD, utils.hpp:83-93); m shared or per row
+__global__ void fd_mul_kernel(double *x, const double *m, int half, size_t rows, int shared)
+{
+    const size_t total = rows * (size_t)half;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = e / half, k = e % half;
+        double *xr = x + r * 2 * half;
+        const double *mr = m + (shared ? 0 : r * 2 * half);
+        const double ar = xr[k], ai = xr[k + half], br = mr[k], bi = mr[k + half];
+        xr[k] = fma(ar, br, -(ai * bi));
+        xr[k + half] = fma(ai, br, ar * bi);
+    }
+}
+
+cudaError_t launch_fd_mul(double *x, const double *m, int half, int rows, int shared, cudaStream_t st)
+{
+    const size_t total = (size_t)rows * half;
+    const unsigned grid = (unsigned)std::min<size_t>((total + 255) / 256, 4096);
+    fd_mul_kernel<<<grid, 256, 0, st>>>(x, m, half, (size_t)rows, shared);
+    return cudaGetLastError();
 }
 
 struct Arc {
@@ -195,4 +220,39 @@ int cufhedb_arc_compare(cufhedb_ctx *ctx, int op, const uint32_t *trlwe, const v
     for (uint32_t *p : {t, eq, hi, sum})
         if (p) cudaFreeAsync(p, A.st);
     return rc;
+}
+
+// PolyMul_st (cufft_gpu.cuh:214-226): TwistFFT(TwistIFFT(a_i) * m) per row
+int cufhedb_polymul_lvl1(cufhedb_ctx *ctx, const uint32_t *a, const double *m_fd, uint32_t *out, int B, int shared,
+                         cufhedb_stream_t stream)
+{
+    if (!ctx || B < 0) return set_error(CUFHEDB_ERR_ARG, "bad argument");
+    if (B == 0) return CUFHEDB_OK;
+    if (!a || !m_fd || !out) return set_error(CUFHEDB_ERR_ARG, "null buffer");
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    double *fd = nullptr;
+    cudaError_t e = cudaMallocAsync((void **)&fd, (size_t)B * N1 * sizeof(double), st);
+    if (e == cudaSuccess) e = launch_twist_ifft1(fd, a, B, ctx->tab512, st);
+    if (e == cudaSuccess) e = launch_fd_mul(fd, m_fd, N1 / 2, B, shared, st);
+    if (e == cudaSuccess) e = launch_twist_fft1(out, fd, B, ctx->tab512, st);
+    if (fd) cudaFreeAsync(fd, st);
+    return e == cudaSuccess ? CUFHEDB_OK : cuda_error(e, "polynomial product (lvl1)");
+}
+
+int cufhedb_polymul_lvl2(cufhedb_ctx *ctx, const uint64_t *a, const double *m_fd, uint64_t *out, int B, int shared,
+                         cufhedb_stream_t stream)
+{
+    if (!ctx || B < 0) return set_error(CUFHEDB_ERR_ARG, "bad argument");
+    if (B == 0) return CUFHEDB_OK;
+    if (!a || !m_fd || !out) return set_error(CUFHEDB_ERR_ARG, "null buffer");
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    double *fd = nullptr;
+    cudaError_t e = cudaMallocAsync((void **)&fd, (size_t)B * N2 * sizeof(double), st);
+    if (e == cudaSuccess) e = launch_twist_ifft2(fd, a, B, ctx->tab1024, st);
+    if (e == cudaSuccess) e = launch_fd_mul(fd, m_fd, N2 / 2, B, shared, st);
+    if (e == cudaSuccess) e = launch_twist_fft2(out, fd, B, ctx->tab1024, st);
+    if (fd) cudaFreeAsync(fd, st);
+    return e == cudaSuccess ? CUFHEDB_OK : cuda_error(e, "polynomial product (lvl2)");
 }

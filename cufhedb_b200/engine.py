@@ -294,6 +294,17 @@ class Engine:
         check(self.lib.cufhedb_compare(self.ctx, _lib.COMPARE[op], level, _ptr(c1), _ptr(c2), _ptr(out),
                                        self._rows(c1, level), plain_bits, int(logic), precision, _stream(stream)))
 
+    def polymul_lvl1(self, a_dev, m_fd_dev, out_dev, shared: bool = True, stream=None):
+        """negacyclic products a_i * m, m in TFHEpp's frequency-domain layout"""
+        B = a_dev.numel() // N1
+        check(self.lib.cufhedb_polymul_lvl1(self.ctx, _ptr(a_dev), _ptr(m_fd_dev), _ptr(out_dev), B, int(shared),
+                                            _stream(stream)))
+
+    def polymul_lvl2(self, a_dev, m_fd_dev, out_dev, shared: bool = True, stream=None):
+        B = a_dev.numel() // N2
+        check(self.lib.cufhedb_polymul_lvl2(self.ctx, _ptr(a_dev), _ptr(m_fd_dev), _ptr(out_dev), B, int(shared),
+                                            _stream(stream)))
+
     ARC_OPS = {"gt": 0, "lt": 1, "eq": 2, "lt_strict": 3}
 
     def arc_compare(self, op: str, trlwe_dev, trgsw_prepared, out_dev, digits: int, precision=_lib.FP64,

@@ -259,6 +259,17 @@ CUFHEDB_API int cufhedb_compare(cufhedb_ctx *ctx, int op, int level, const void 
                                 uint32_t *out_lvl1, int B, uint32_t plain_bits, int logic, int precision,
                                 cufhedb_stream_t stream);
 
+/* B negacyclic products out_i = a_i * m (the reference's PolyMul_st,
+ * src/cuHEDB/fft_gpu/cufft_gpu.cuh:214-226, which multiplies by the
+ * polynomial its engine last transformed): TwistFFT(TwistIFFT(a_i) x m) in
+ * FP64.  a / out: B polynomials (1024 uint32 or 2048 uint64); m_fd: the
+ * multiplier in TFHEpp's frequency-domain layout (TwistIFFT output, N doubles),
+ * one for all rows when `shared` != 0, else B of them.  Device memory. */
+CUFHEDB_API int cufhedb_polymul_lvl1(cufhedb_ctx *ctx, const uint32_t *a, const double *m_fd, uint32_t *out, int B,
+                                     int shared, cufhedb_stream_t stream);
+CUFHEDB_API int cufhedb_polymul_lvl2(cufhedb_ctx *ctx, const uint64_t *a, const double *m_fd, uint64_t *out, int B,
+                                     int shared, cufhedb_stream_t stream);
+
 /* ArcEDB comparisons (cuARCEDB::greater_than_tfhepp / less_than_tfhepp /
  * equality_tfhepp, src/cuHEDB/comparable_gpu.cuh:52-168; CPU twins
  * src/ARCEDB/comparison/comparable.cpp:506-729) of B rows of D radix-1024

@@ -4,8 +4,10 @@
 // msb_gpu,HomCompare_gpu}.cuh and fft_gpu/cufft_gpu.cuh.  It re-provides, with
 // the same names, signatures and TFHEpp types:
 //   * cufft::CuFFT_Torus<P> (cufft_gpu.cuh:10-451): the constructor, LoadBK,
-//     ifft_st, fft_st, ExternalProduct_st, GateBootstrappingTLWE2TLWEFFT_st,
-//     IdeGateBootstrappingTLWE2TLWEFFT_st and the *_test timing loops;
+//     ifft_st, fft_st, PolyMul_st, ExternalProduct_st,
+//     GateBootstrappingTLWE2TLWEFFT_st, IdeGateBootstrappingTLWE2TLWEFFT_st
+//     and the *_test timing loops (MoveBuf, a debug copy of the reference's
+//     per-stream product buffer, has no counterpart: no such buffer exists);
 //   * the globals cufftlvl1 / cufftlvl2 (gatebootstrap_gpu.cuh:24-25) and
 //     warmupGPU() (cufft_gpu.cuh:462-470);
 //   * cuHEDB::MSBGateBootstrapping x3, IdeGateBootstrapping x3, HomNOT, HomAND,
@@ -188,6 +190,7 @@ class CuFFT_Torus {
                                                           (double *)s.g, 1, s.st));
         cufhedb_dropin::d2h(res, s.g, s.st);
         cufhedb_dropin::finish(s.st);
+        set_multiplier(res);
     }
 
     void fft_st(std::array<typename P::T, P::n> &res, std::array<double, P::n> &a, const uint32_t stream_id)
@@ -201,6 +204,34 @@ class CuFFT_Torus {
             cufhedb_dropin::check(cufhedb_twist_fft_lvl2(cufhedb_dropin::engine(), (const double *)s.g,
                                                          (uint64_t *)s.a, 1, s.st));
         cufhedb_dropin::d2h(res, s.a, s.st);
+        cufhedb_dropin::finish(s.st);
+        set_multiplier(a);
+    }
+
+    // PolyMul_st (cufft_gpu.cuh:214-226): both polynomials of `trlwe` times the
+    // engine's multiplier.  As in the reference that is the all-ones
+    // polynomial its constructor transforms (cufft_gpu.cuh:116-127), replaced
+    // by the result of the last ifft_st or the input of the last fft_st (both
+    // write the buffer PolyMul reads there).
+    void PolyMul_st(std::array<std::array<typename P::T, P::n>, 2> &res,
+                    std::array<std::array<typename P::T, P::n>, 2> &trlwe, const uint32_t stream_id)
+    {
+        std::array<double, P::n> m;
+        if (!get_multiplier(m)) {
+            std::array<typename P::T, P::n> ones;
+            ones.fill(1);
+            ifft_st(m, ones, stream_id);
+        }
+        auto &s = slots_.get(stream_id);
+        cufhedb_dropin::h2d(s.a, trlwe, s.st);
+        cufhedb_dropin::h2d(s.g, m, s.st);
+        if constexpr (P::n == 1024)
+            cufhedb_dropin::check(cufhedb_polymul_lvl1(cufhedb_dropin::engine(), (const uint32_t *)s.a,
+                                                       (const double *)s.g, (uint32_t *)s.b, 2, 1, s.st));
+        else
+            cufhedb_dropin::check(cufhedb_polymul_lvl2(cufhedb_dropin::engine(), (const uint64_t *)s.a,
+                                                       (const double *)s.g, (uint64_t *)s.b, 2, 1, s.st));
+        cufhedb_dropin::d2h(res, s.b, s.st);
         cufhedb_dropin::finish(s.st);
     }
 
@@ -292,6 +323,22 @@ class CuFFT_Torus {
 
   private:
     cufhedb_dropin::Slots slots_;
+    std::mutex mul_mu_;
+    bool mul_set_ = false;
+    std::array<double, P::n> mul_{};
+
+    void set_multiplier(const std::array<double, P::n> &m)
+    {
+        std::lock_guard<std::mutex> lk(mul_mu_);
+        mul_ = m;
+        mul_set_ = true;
+    }
+    bool get_multiplier(std::array<double, P::n> &m)
+    {
+        std::lock_guard<std::mutex> lk(mul_mu_);
+        m = mul_;
+        return mul_set_;
+    }
 
     void pbs(std::array<typename P::T, P::n + 1> &tlwe, std::array<uint32_t, 673> &poly, const cufhedb_testvec &tv,
              uint32_t stream_id)

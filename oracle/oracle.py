@@ -132,12 +132,10 @@ class Oracle:
         the TRGSW of X^{-v}; -h_i at coefficient N - v, or +h_i at 0 when v = 0"""
         g = self.trgsw32(0, s1, seed, stream, idx)
         for i in range(L1):
-            h = np.uint32(1 << (32 - (i + 1) * BG1))
+            h = 1 << (32 - (i + 1) * BG1)
             for k in range(2):
-                if v:
-                    g[i + k * L1, k, N1 - v] -= h
-                else:
-                    g[i + k * L1, k, 0] += h
+                j = N1 - v if v else 0
+                g[i + k * L1, k, j] = (int(g[i + k * L1, k, j]) + (-h if v else h)) % 2 ** 32
         return g
 
     def arc_single(self, op, trlwe, g):
@@ -147,7 +145,7 @@ class Oracle:
         t = self.extprod32_exact(trlwe, g)
         if op == "eq":
             out = sample_extract32(t) * np.uint32(2)
-            out[N1] -= np.uint32(MU1)
+            out[N1] = (int(out[N1]) - MU1) % 2 ** 32
             return out
         p = np.ones(N1, np.uint32)
         if op == "lt_strict":

@@ -1,0 +1,307 @@
+// Drop-in check of include/cufhedb_b200/comparable_gpu.hpp.
+//
+// The flow of the reference's ArcEDB GPU program (test/Arc_Query/comparable.cu):
+// TFHEpp generates the keys, cufftplvl1.LoadBK uploads the bootstrapping key,
+// values are split into radix-1024 digits and encrypted as TRLWEs of mu X^x_d
+// and TRGSWs of X^-y_d, and the cuARCEDB:: comparisons run on them with a
+// stream id.  Only the include differs.  Every GPU result is decrypted and
+// checked against the plaintext and against the reference's TFHEpp steps run
+// on the CPU on the same ciphertexts (the composition of
+// src/ARCEDB/comparison/comparable.cpp, which itself needs SEAL to build).
+//
+// Exit status 0 means every check passed.
+#include "cufhedb_b200/comparable_gpu.hpp"
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <random>
+#include <string>
+#include <vector>
+
+namespace {
+
+using P1 = TFHEpp::lvl1param;
+
+int g_failed = 0;
+
+void report(const char *what, bool ok, const std::string &detail = "")
+{
+    std::printf("%-58s %s %s\n", what, ok ? "PASS" : "FAIL", detail.c_str());
+    if (!ok) ++g_failed;
+}
+
+int32_t phase(const TFHEpp::TLWE<P1> &c, const TFHESecretKey &sk)
+{
+    const auto &s = sk.key.get<P1>();
+    uint32_t p = c[P1::n];
+    for (int i = 0; i < P1::n; i++) p -= c[i] * s[i];
+    return (int32_t)p;
+}
+
+// exponent_encrypt<Lvl1> (comparable.h:169-179): the TRLWE of mu X^v
+TFHEpp::TRLWE<P1> enc_exp(uint32_t v, const TFHESecretKey &sk)
+{
+    std::array<uint32_t, P1::n> plain{};
+    plain[v] = P1::μ;
+    return TFHEpp::trlweSymEncrypt<P1>(plain, P1::α, sk.key.get<P1>());
+}
+
+// exponent_encrypt_rgsw<Lvl1>(is_negative) (comparable.h:228-274): X^-v
+TFHEpp::TRGSWFFT<P1> enc_exp_rgsw(uint32_t v, const TFHESecretKey &sk)
+{
+    constexpr std::array<uint32_t, P1::l> h = TFHEpp::hgen<P1>();
+    TFHEpp::TRGSW<P1> g;
+    for (auto &row : g) row = TFHEpp::trlweSymEncryptZero<P1>(P1::α, sk.key.get<P1>());
+    for (int i = 0; i < P1::l; i++)
+        for (int k = 0; k < 2; k++) {
+            if (v)
+                g[i + k * P1::l][k][P1::n - v] -= h[i];
+            else
+                g[i + k * P1::l][k][0] += h[i];
+        }
+    return TFHEpp::ApplyFFT2trgsw<P1>(g);
+}
+
+std::vector<uint32_t> digits_of(uint64_t v, int D)
+{
+    std::vector<uint32_t> d(D);
+    for (int i = 0; i < D; i++) d[i] = (v >> (10 * i)) & 1023;
+    return d;
+}
+
+// the reference's single-digit steps with TFHEpp on the CPU (comparable.cpp
+// 506-523 greater, 652-666 less, 623-633 equality; op 3 the equal term)
+TFHEpp::TLWE<P1> cpu_digit(int op, const TFHEpp::TRLWE<P1> &x, const TFHEpp::TRGSWFFT<P1> &y)
+{
+    TFHEpp::TRLWE<P1> prod, mul;
+    TFHEpp::TLWE<P1> r;
+    TFHEpp::trgswfftExternalProduct<P1>(prod, x, y);
+    if (op == 2 || op == 3) {
+        TFHEpp::SampleExtractIndex<P1>(r, prod, 0);
+        if (op == 2) {
+            for (int i = 0; i <= P1::n; i++) r[i] = 2 * r[i];
+            r[P1::n] -= P1::μ;
+        }
+        return r;
+    }
+    TFHEpp::Polynomial<P1> t;
+    for (int i = 0; i < P1::n; i++) t[i] = 1;
+    if (op == 1) t[0] = P1::plain_modulus - 1;
+    TFHEpp::PolyMul<P1>(mul[0], prod[0], t);
+    TFHEpp::PolyMul<P1>(mul[1], prod[1], t);
+    TFHEpp::SampleExtractIndex<P1>(r, mul, 0);
+    if (op == 0)
+        for (int i = 0; i <= P1::n; i++) r[i] = -r[i];
+    return r;
+}
+
+TFHEpp::TLWE<P1> cpu_boot(const TFHEpp::TLWE<P1> &x, const TFHEEvalKey &ek)
+{
+    TFHEpp::TLWE<TFHEpp::lvl0param> l0;
+    TFHEpp::TLWE<P1> r;
+    TFHEpp::IdentityKeySwitch<TFHEpp::lvl10param>(l0, x, *ek.iksklvl10);
+    TFHEpp::Polynomial<P1> tv;
+    tv.fill(P1::μ);
+    TFHEpp::GateBootstrappingTLWE2TLWEFFT<TFHEpp::lvl01param>(r, l0, *ek.bkfftlvl01, tv);
+    return r;
+}
+
+// the multi-digit composition (comparable.cpp:525-557, 635-650, 668-698)
+TFHEpp::TLWE<P1> cpu_compare(int op, const std::vector<TRLWELvl1> &x, const std::vector<TRGSWLvl1> &y, int D,
+                             const TFHEEvalKey &ek)
+{
+    TFHEpp::TLWE<P1> r = cpu_digit(op, x[0], y[0]);
+    for (int d = 1; d < D; d++) {
+        TFHEpp::TLWE<P1> hi = cpu_digit(op, x[d], y[d]), sum;
+        if (op == 2) {
+            for (int i = 0; i <= P1::n; i++) sum[i] = r[i] + hi[i];
+            sum[P1::n] -= P1::μ;
+        } else {
+            TFHEpp::TLWE<P1> eq = cpu_digit(3, x[d], y[d]);
+            for (int i = 0; i <= P1::n; i++) sum[i] = eq[i] + 2 * hi[i] + r[i];
+            sum[P1::n] += P1::μ >> 1;
+        }
+        r = cpu_boot(sum, ek);
+    }
+    return r;
+}
+
+// the reference's digit combination on plaintext digits
+bool model(int op, const std::vector<uint32_t> &x, const std::vector<uint32_t> &y)
+{
+    auto single = [&](uint32_t a, uint32_t b) { return op == 0 ? a > b : op == 1 ? a <= b : a == b; };
+    bool r = single(x[0], y[0]);
+    for (size_t d = 1; d < x.size(); d++) {
+        if (op == 2) {
+            r = r && x[d] == y[d];
+        } else {
+            int units = (x[d] == y[d] ? 2 : 0) + (single(x[d], y[d]) ? 4 : -4) + (r ? 2 : -2) + 1;
+            units = ((units % 16) + 16) % 16;
+            r = units >= 1 && units <= 7;
+        }
+    }
+    return r;
+}
+
+}  // namespace
+
+int main()
+{
+    warmupGPU();
+    auto t0 = std::chrono::steady_clock::now();
+    TFHESecretKey sk;
+    TFHEEvalKey ek;
+    ek.emplacebkfft<Lvl01>(sk);
+    ek.emplaceiksk<Lvl10>(sk);
+    std::printf("TFHEpp keys: %.1f s\n",
+                std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
+    cufftplvl1.LoadBK(*ek.bkfftlvl01);
+
+    std::mt19937_64 rng(2024);
+    const char *names[3] = {"greater_than_tfhepp", "less_than_tfhepp", "equality_tfhepp"};
+
+    // PolyMul_st against TFHEpp::PolyMul with the all-ones polynomial
+    {
+        TRLWELvl1 a, got;
+        for (auto &p : a)
+            for (auto &v : p) v = (uint32_t)rng();
+        cufftplvl1.PolyMul_st(got, a, 0);
+        TFHEpp::Polynomial<P1> ones;
+        ones.fill(1);
+        int64_t worst = 0;
+        for (int k = 0; k < 2; k++) {
+            TFHEpp::Polynomial<P1> want;
+            TFHEpp::PolyMul<P1>(want, a[k], ones);
+            for (int i = 0; i < P1::n; i++) worst = std::max<int64_t>(worst, std::llabs((int32_t)(got[k][i] - want[i])));
+        }
+        report("cufftplvl1.PolyMul_st (all-ones) vs TFHEpp::PolyMul", worst <= 64,
+               "max |diff| " + std::to_string(worst));
+    }
+
+    // single digits, every operator, against TFHEpp's steps and the plaintext
+    {
+        int bad = 0;
+        int64_t worst = 0;
+        const uint32_t pairs[][2] = {{0, 0}, {0, 1}, {1, 0}, {511, 511}, {1023, 0}, {0, 1023}, {700, 699}, {5, 900}};
+        for (auto &pr : pairs) {
+            TRLWELvl1 x = enc_exp(pr[0], sk);
+            TRGSWLvl1 y = enc_exp_rgsw(pr[1], sk);
+            for (int op = 0; op < 3; op++) {
+                TLWELvl1 got;
+                if (op == 0) cuARCEDB::greater_than_tfhepp(x, y, got, sk, 1);
+                if (op == 1) cuARCEDB::less_than_tfhepp(x, y, got, sk, 1);
+                if (op == 2) cuARCEDB::equality_tfhepp(x, y, got, sk, 1);
+                TLWELvl1 want = cpu_digit(op, x, y);
+                for (int i = 0; i <= P1::n; i++)
+                    worst = std::max<int64_t>(worst, std::llabs((int32_t)(got[i] - want[i])));
+                const bool truth = op == 0 ? pr[0] > pr[1] : op == 1 ? pr[0] <= pr[1] : pr[0] == pr[1];
+                bad += (phase(got, sk) > 0) != truth;
+            }
+        }
+        report("cuARCEDB single digit (gt / lt / eq), 8 pairs", bad == 0 && worst <= 256,
+               "wrong " + std::to_string(bad) + ", max |diff| vs TFHEpp " + std::to_string(worst));
+    }
+
+    // several digits (20- and 30-bit values), one call per comparison
+    for (int D : {2, 3}) {
+        const int n = 12;
+        int bad_model = 0, bad_cpu = 0, bad_plain = 0;
+        double gpu_s = 0, cpu_s = 0;
+        for (int r = 0; r < n; r++) {
+            const uint64_t top = 1ull << (10 * D);
+            uint64_t a = rng() % top, b = rng() % top;
+            if (r % 3 == 0) b = a;
+            if (r % 3 == 1) b = (a >> 10 * (D - 1) << 10 * (D - 1)) | (rng() % (1ull << 10 * (D - 1)));
+            std::vector<TRLWELvl1> xs(D);
+            std::vector<TRGSWLvl1> ys(D);
+            auto da = digits_of(a, D), db = digits_of(b, D);
+            for (int d = 0; d < D; d++) {
+                xs[d] = enc_exp(da[d], sk);
+                ys[d] = enc_exp_rgsw(db[d], sk);
+            }
+            for (int op = 0; op < 3; op++) {
+                TLWELvl1 got;
+                auto g0 = std::chrono::steady_clock::now();
+                if (op == 0) cuARCEDB::greater_than_tfhepp(xs, ys, D, got, ek, sk, 2);
+                if (op == 1) cuARCEDB::less_than_tfhepp(xs, ys, D, got, ek, sk, 2);
+                if (op == 2) cuARCEDB::equality_tfhepp(xs, ys, D, got, ek, sk, 2);
+                auto g1 = std::chrono::steady_clock::now();
+                TLWELvl1 want = cpu_compare(op, xs, ys, D, ek);
+                auto g2 = std::chrono::steady_clock::now();
+                gpu_s += std::chrono::duration<double>(g1 - g0).count();
+                cpu_s += std::chrono::duration<double>(g2 - g1).count();
+                const bool sg = phase(got, sk) > 0;
+                bad_model += sg != model(op, da, db);
+                bad_cpu += sg != (phase(want, sk) > 0);
+                if (op != 1) bad_plain += sg != (op == 0 ? a > b : a == b);
+            }
+        }
+        char buf[160];
+        std::snprintf(buf, sizeof buf, "wrong vs model %d, vs TFHEpp %d, vs plaintext %d; %.2f ms (GPU) / %.2f ms (CPU)",
+                      bad_model, bad_cpu, bad_plain, 1e3 * gpu_s / (3 * n), 1e3 * cpu_s / (3 * n));
+        std::string what = "cuARCEDB " + std::to_string(D) + " digits (gt / lt / eq), 12 rows";
+        report(what.c_str(), bad_model == 0 && bad_cpu == 0 && bad_plain == 0, buf);
+    }
+
+    // HomAND / HomOR and lift_and_and against TFHEpp on the CPU
+    {
+        int bad = 0;
+        int64_t worst_lift = 0;
+        for (int t = 0; t < 8; t++) {
+            const bool ba = t & 1, bb = (t >> 1) & 1;
+            auto enc = [&](bool bit) {
+                return TFHEpp::tlweSymEncrypt<P1>(bit ? P1::μ : -P1::μ, P1::α, sk.key.get<P1>());
+            };
+            TLWELvl1 ca = enc(ba), cb = enc(bb), r_and, r_or, lift;
+            cuARCEDB::HomAND(r_and, ca, cb, ek, 3);
+            cuARCEDB::HomOR(r_or, ca, cb, ek, 3);
+            bad += (phase(r_and, sk) > 0) != (ba && bb);
+            bad += (phase(r_or, sk) > 0) != (ba || bb);
+            const uint32_t scale_bits = 20;
+            cuARCEDB::lift_and_and(ca, cb, lift, scale_bits, ek, sk, 3);
+            // the reference's steps (comparable.cpp lift_and_and, TFHEpp on the CPU)
+            TLWELvl1 temp;
+            for (int i = 0; i <= P1::n; i++) temp[i] = ca[i] + cb[i];
+            temp[P1::n] -= P1::μ;
+            TFHEpp::TLWE<TFHEpp::lvl0param> l0;
+            TFHEpp::IdentityKeySwitch<TFHEpp::lvl10param>(l0, temp, *ek.iksklvl10);
+            const uint32_t c = 1u << (scale_bits - 1);
+            TFHEpp::Polynomial<P1> tv;
+            tv.fill(0u - c);
+            TLWELvl1 want;
+            TFHEpp::GateBootstrappingTLWE2TLWEFFT<TFHEpp::lvl01param>(want, l0, *ek.bkfftlvl01, tv);
+            want[P1::n] += c;
+            worst_lift = std::max<int64_t>(worst_lift, std::llabs((int64_t)phase(lift, sk) - phase(want, sk)));
+        }
+        report("cuARCEDB HomAND / HomOR / lift_and_and, 8 inputs", bad == 0 && worst_lift < (1 << 24),
+               "wrong " + std::to_string(bad) + ", lift phase |diff| vs TFHEpp " + std::to_string(worst_lift));
+    }
+
+    // a whole column in one call
+    {
+        const int rows = 64, D = 2;
+        std::vector<std::vector<TRLWELvl1>> xs(rows);
+        std::vector<std::vector<TRGSWLvl1>> ys(rows);
+        std::vector<uint64_t> a(rows), b(rows);
+        for (int r = 0; r < rows; r++) {
+            a[r] = rng() % (1u << 20);
+            b[r] = r % 4 == 0 ? a[r] : rng() % (1u << 20);
+            auto da = digits_of(a[r], D), db = digits_of(b[r], D);
+            for (int d = 0; d < D; d++) {
+                xs[r].push_back(enc_exp(da[d], sk));
+                ys[r].push_back(enc_exp_rgsw(db[d], sk));
+            }
+        }
+        int bad = 0;
+        for (int op : {0, 2}) {
+            std::vector<TLWELvl1> res;
+            cuARCEDB::batch::compare(op, xs, ys, D, res, ek);
+            for (int r = 0; r < rows; r++) bad += (phase(res[r], sk) > 0) != (op == 0 ? a[r] > b[r] : a[r] == b[r]);
+        }
+        report("cuARCEDB::batch::compare, 64 rows x 2 digits (gt, eq)", bad == 0, "wrong " + std::to_string(bad));
+    }
+
+    std::printf("%s\n", g_failed ? "SOME CHECKS FAILED" : "all checks passed");
+    return g_failed ? 1 : 0;
+}

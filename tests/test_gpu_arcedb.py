@@ -162,3 +162,43 @@ def test_arc_multi_digit_against_reference(engine, oracle, ref_keyed, keys, bkff
                 x[N1] = np.uint32((int(x[N1]) + (MU >> 1)) % 2 ** 32)
             r = boot(x)
             assert got[i] == (signed_diff(oracle.phase32(r, s1), 0) > 0), (op, i)
+
+
+def test_polymul_lvl1_and_lvl2(engine, oracle):
+    """cufhedb_polymul_lvl1/2 (the reference's PolyMul_st) against the exact
+    negacyclic product: the all-ones multiplier (the reference's default)
+    shared by the batch, and one small multiplier per row."""
+    import torch
+    from oracle.oracle import N2, polymul32
+    rng = np.random.default_rng(8)
+    B = 6
+    a = rng.integers(0, 2 ** 32, (B, N1), dtype=np.uint64).astype(np.uint32)
+    ones = np.ones(N1, np.uint32)
+    m = torch.from_numpy(oracle.twist_ifft32(ones)).cuda()
+    out = torch.zeros(B * N1, dtype=torch.int32, device="cuda")
+    engine.polymul_lvl1(_dev(a), m, out, shared=True)
+    engine.sync()
+    got = out.cpu().numpy().view(np.uint32).reshape(B, N1)
+    for i in range(B):
+        assert np.max(np.abs(signed_diff(got[i], polymul32(a[i], ones)))) <= 4
+    p = rng.integers(-2, 3, (B, N1)).astype(np.int64).astype(np.uint32)
+    mp = torch.from_numpy(np.stack([oracle.twist_ifft32(x) for x in p])).cuda()
+    engine.polymul_lvl1(_dev(a), mp, out, shared=False)
+    engine.sync()
+    got = out.cpu().numpy().view(np.uint32).reshape(B, N1)
+    for i in range(B):
+        assert np.max(np.abs(signed_diff(got[i], polymul32(a[i], p[i])))) <= 4
+    # lvl2: 64-bit torus through the FP64 transform keeps the top ~2^-45 of
+    # the product, as the reference's GPU kernel does
+    a2 = rng.integers(0, 2 ** 64, (2, N2), dtype=np.uint64)
+    m2 = torch.from_numpy(oracle.twist_ifft64(np.ones(N2, np.uint64))).cuda()
+    out2 = torch.zeros(2 * N2, dtype=torch.int64, device="cuda")
+    engine.polymul_lvl2(torch.from_numpy(a2.view(np.int64).copy()).cuda(), m2, out2, shared=True)
+    engine.sync()
+    got2 = out2.cpu().numpy().view(np.uint64).reshape(2, N2)
+    for i in range(2):
+        s = np.cumsum(a2[i].astype(object)) % 2 ** 64
+        want = np.array([(2 * int(s[k]) - int(s[-1])) % 2 ** 64 for k in range(N2)], dtype=object)
+        d = (got2[i].astype(object) - want) % 2 ** 64
+        d = np.array([int(x) - 2 ** 64 if x >= 2 ** 63 else int(x) for x in d])
+        assert np.max(np.abs(d)) < 2 ** 30
