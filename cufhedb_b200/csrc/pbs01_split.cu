@@ -41,48 +41,51 @@ struct Pbs01SplitSmem {
     static constexpr int TOTAL = WARP_OFF + W * PER_WARP;
 };
 
-// digit d of (X^a - 1) * poly at coefficients m and m+512, twisted:
-// v[m2] = (dig_d(m) + i dig_d(m+512)) * w^m,  m = lane + 32 m2.  The signed
-// digit is the sign-extended field d of (t + offset + round) ^ DEC1_XOR.
-__device__ __forceinline__ void load_digit_poly1_f(float2 v[16], const uint32_t *poly, uint32_t abar, int d, int lane,
-                                        const Fft512TablesF &T)
+// the decomposition words of (X^a - 1) * poly, once per polynomial:
+// w[2 m2 + h] = (((X^a - 1) poly)[m + 512 h] + offset + round) ^ DEC1_XOR,
+// m = lane + 32 m2; each of the l = 3 digits is then a field of these words
+__device__ __forceinline__ void digit_words1(uint32_t w[32], const uint32_t *poly, uint32_t abar, int lane)
 {
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int m = lane + 32 * m2;
-        const uint32_t x0 = ((rot_coef<N1>(poly, m, abar) - poly[m]) + DEC1_OFFSET + DEC1_ROUND) ^ DEC1_XOR;
-        const uint32_t x1 = ((rot_coef<N1>(poly, m + 512, abar) - poly[m + 512]) + DEC1_OFFSET + DEC1_ROUND) ^ DEC1_XOR;
-        const int d0 = digit_field1(x0, d), d1 = digit_field1(x1, d);
+        w[2 * m2] = ((rot_coef<N1>(poly, m, abar) - poly[m]) + DEC1_OFFSET + DEC1_ROUND) ^ DEC1_XOR;
+        w[2 * m2 + 1] = ((rot_coef<N1>(poly, m + 512, abar) - poly[m + 512]) + DEC1_OFFSET + DEC1_ROUND) ^ DEC1_XOR;
+    }
+}
+
+// v[m2] = (dig_d(m) + i dig_d(m+512)) * w^m from the cached words
+__device__ __forceinline__ void digits_from_words_f(float2 v[16], const uint32_t w[32], int d, int lane,
+                                                    const Fft512TablesF &T)
+{
+#pragma unroll
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int d0 = digit_field1(w[2 * m2], d), d1 = digit_field1(w[2 * m2 + 1], d);
         v[m2] = fcmul(make_float2((float)d0, (float)d1), T.twist[m2 * 32 + lane]);
     }
 }
 
-// poly[m] += round(hi_m) * 2^24 (mod 2^32): the hi limb's products round exactly
-__device__ __forceinline__ void add_inverse_hi(uint32_t *poly, float2 v[16], float2 *xp, int lane,
-                                               const Fft512TablesF &T)
+// poly[m] += round(hi_m) * 2^24 + round(lo_m) (mod 2^32), one read-modify-write
+// of the accumulator per polynomial.  The hi limb's products round exactly;
+// the lo limb's FP32 error stays far below the bootstrapping noise.
+__device__ __forceinline__ void add_inverse_split(uint32_t *poly, float2 hi[16], float2 lo[16], float2 *xp, int lane,
+                                                  const Fft512TablesF &T)
 {
-    ffft512_inv(v, xp, T, lane);
+    uint32_t t[32];
+    ffft512_inv(hi, xp, T, lane);
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
-        const int m = lane + 32 * m2;
-        const float2 y = fcmul(v[m2], T.untwist[m2 * 32 + lane]);
-        poly[m] += (uint32_t)__float2int_rn(y.x) << 24;
-        poly[m + 512] += (uint32_t)__float2int_rn(y.y) << 24;
+        const float2 y = fcmul(hi[m2], T.untwist[m2 * 32 + lane]);
+        t[2 * m2] = (uint32_t)__float2int_rn(y.x) << 24;
+        t[2 * m2 + 1] = (uint32_t)__float2int_rn(y.y) << 24;
     }
-}
-
-// poly[m] += round(lo_m) (mod 2^32); the lo limb's FP32 error stays far below
-// the bootstrapping noise
-__device__ __forceinline__ void add_inverse_lo(uint32_t *poly, float2 v[16], float2 *xp, int lane,
-                                               const Fft512TablesF &T)
-{
-    ffft512_inv(v, xp, T, lane);
+    ffft512_inv(lo, xp, T, lane);
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int m = lane + 32 * m2;
-        const float2 y = fcmul(v[m2], T.untwist[m2 * 32 + lane]);
-        poly[m] += (uint32_t)__float2ll_rn(y.x);
-        poly[m + 512] += (uint32_t)__float2ll_rn(y.y);
+        const float2 y = fcmul(lo[m2], T.untwist[m2 * 32 + lane]);
+        poly[m] += t[2 * m2] + (uint32_t)__float2ll_rn(y.x);
+        poly[m + 512] += t[2 * m2 + 1] + (uint32_t)__float2ll_rn(y.y);
     }
 }
 
@@ -142,12 +145,14 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
             const uint32_t ab = valid ? abar_s[i] : 0u;
             const bool active = ab != 0;
             float2 f0h[16], f0l[16], f1h[16], f1l[16];
+            uint32_t w[32];
 #pragma unroll 1
             for (int r = 0; r < 2 * L1; ++r, ++c) {
+                if (active && r % L1 == 0) digit_words1(w, acc + (r / L1) * N1, ab, lane);
                 const float4 *bkc = reinterpret_cast<const float4 *>(ring.acquire(c, a.err));
                 if (active) {
                     float2 v[16];
-                    load_digit_poly1_f(v, acc + (r / L1) * N1, ab, r % L1, lane, *T);
+                    digits_from_words_f(v, w, r % L1, lane, *T);
                     ffft512_fwd(v, xp, *T, lane);
                     if (r == 0) {
 #pragma unroll
@@ -172,10 +177,8 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
                 ring.release(c, lane);
             }
             if (active) {
-                add_inverse_hi(acc, f0h, xp, lane, *T);
-                add_inverse_lo(acc, f0l, xp, lane, *T);
-                add_inverse_hi(acc + N1, f1h, xp, lane, *T);
-                add_inverse_lo(acc + N1, f1l, xp, lane, *T);
+                add_inverse_split(acc, f0h, f0l, xp, lane, *T);
+                add_inverse_split(acc + N1, f1h, f1l, xp, lane, *T);
                 __syncwarp();
             }
         }
