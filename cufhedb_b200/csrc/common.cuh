@@ -11,6 +11,9 @@ namespace cfdb {
 // lvl0 LWE, lvl1 / lvl2 TRLWE + gadget, key-switching parameters
 constexpr int N0 = 672;
 constexpr int N1 = 1024, L1 = 3, BGBIT1 = 6;
+// per-warp transpose scratch of the 512-point transforms: 32 rows of 16
+// values padded to 17 (fft_f64.cuh, fft_f32.cuh)
+constexpr int FFT512_XP = 32 * 17;
 constexpr int N2 = 2048, L2 = 4, BGBIT2 = 9;
 constexpr int KS10_BASEBIT = 10, KS10_T = 2;
 constexpr int KS20_BASEBIT = 10, KS20_T = 2;

@@ -41,7 +41,7 @@ __device__ __forceinline__ void digits_f32(float2 v[16], const uint32_t *poly, i
 
 __global__ void __launch_bounds__(128) extprod1_f64_kernel(ExtProdArgs a)
 {
-    __shared__ double2 xp_s[4][512];
+    __shared__ double2 xp_s[4][FFT512_XP];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int p = blockIdx.x * 4 + w;
     if (p >= a.B) return;
@@ -107,7 +107,7 @@ __device__ __forceinline__ void store_split(uint32_t *o, float2 hi[16], float2 l
 
 __global__ void __launch_bounds__(128) extprod1_split_kernel(ExtProdArgs a)
 {
-    __shared__ float2 xp_s[4][512];
+    __shared__ float2 xp_s[4][FFT512_XP];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int p = blockIdx.x * 4 + w;
     if (p >= a.B) return;

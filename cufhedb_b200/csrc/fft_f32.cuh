@@ -114,9 +114,10 @@ __device__ __forceinline__ void fdft16(float2 v[16])
     for (int i = 0; i < 16; ++i) v[i] = t[i];
 }
 
-// 8-byte elements: swizzle over 16 columns so each half-warp hits 16 distinct
-// 8-byte bank pairs on both the row-wise write and the column-wise read
-__device__ __forceinline__ int xpf_index(int m1, int q2) { return m1 * 16 + (q2 ^ (m1 & 15)); }
+// 8-byte elements in rows padded to 17 (FFT512_XP entries per warp): each
+// half-warp hits 16 distinct 8-byte bank pairs on both the row-wise write and
+// the column-wise read, with compile-time offsets from a per-lane base
+__device__ __forceinline__ int xpf_index(int m1, int q2) { return m1 * 17 + q2; }
 
 __device__ __forceinline__ void ffft512_fwd(float2 v[16], float2 *xp, const Fft512TablesF &T, int lane)
 {

@@ -10,7 +10,7 @@
 // Factorisation 512 = 16 x 32 with m = m1 + 32 m2, q = q2 + 16 q1:
 //   1. lane m1 holds z_{m1+32 m2}, m2 = 0..15: 16-point DFT over m2 in
 //      registers, then twiddle W^{m1 q2};
-//   2. one shared-memory transpose (per-warp 8 KB, XOR-swizzled so both the
+//   2. one shared-memory transpose (per-warp 8.5 KB, rows padded so both the
 //      write and the read are bank-conflict free);
 //   3. lane (q2 = lane & 15, h = lane >> 4) holds the 16 values with m1 of
 //      parity h: 16-point DFT in registers, then one radix-2 step with the
@@ -108,10 +108,14 @@ __device__ __forceinline__ void dft16(double2 v[16])
     for (int i = 0; i < 16; ++i) v[i] = t[i];
 }
 
-__device__ __forceinline__ int xp_index(int m1, int q2) { return m1 * 16 + (q2 ^ (m1 & 7)); }
+// transpose scratch (FFT512_XP entries per warp): 32 rows of 16 values
+// padded to 17, so that both the row-wise write and the column-wise read are
+// free of bank conflicts and every address is a per-lane base plus a
+// compile-time offset
+__device__ __forceinline__ int xp_index(int m1, int q2) { return m1 * 17 + q2; }
 
 // forward transform of the 16 values z_{lane+32 m2} held in v[m2]; on return
-// v[s] = V(fft512_freq(lane, s)).  xp: this warp's 512-entry scratch.
+// v[s] = V(fft512_freq(lane, s)).  xp: this warp's FFT512_XP-entry scratch.
 __device__ __forceinline__ void fft512_fwd(double2 v[16], double2 *xp, const Fft512Tables &T, int lane)
 {
     dft16<1>(v);

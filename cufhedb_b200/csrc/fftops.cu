@@ -12,7 +12,7 @@ __device__ __forceinline__ int bitrev9(int x) { return (int)(__brev((unsigned)x)
 
 __global__ void twist_ifft1_kernel(double *out, const uint32_t *in, int B, const Fft512Tables *T)
 {
-    __shared__ double2 xp_s[4][512];
+    __shared__ double2 xp_s[4][FFT512_XP];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int p = blockIdx.x * 4 + w;
     if (p >= B) return;
@@ -35,7 +35,7 @@ __global__ void twist_ifft1_kernel(double *out, const uint32_t *in, int B, const
 
 __global__ void twist_fft1_kernel(uint32_t *out, const double *in, int B, const Fft512Tables *T)
 {
-    __shared__ double2 xp_s[4][512];
+    __shared__ double2 xp_s[4][FFT512_XP];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int p = blockIdx.x * 4 + w;
     if (p >= B) return;

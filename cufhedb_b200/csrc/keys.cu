@@ -173,7 +173,7 @@ __global__ void tlwe_phase_kernel(T *phase, const T *ct, int B, int n, const T *
 // src: [rows][2][1024] 32-bit torus; dst: [rows][16 s][2 o][32 lane] complex
 __global__ void bk_fft1_kernel(double2 *dst, const uint32_t *src, int rows, const Fft512Tables *T)
 {
-    __shared__ double2 xp_s[4][512];
+    __shared__ double2 xp_s[4][FFT512_XP];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int poly = blockIdx.x * 4 + w;   // = row * 2 + o
     if (poly >= rows * 2) return;
@@ -211,7 +211,7 @@ __global__ void bk_permute1_kernel(double2 *dst, const double *src, int rows)
 // split-precision chunk layout [rows][16 s][2 o][32 lane] float4(hi, lo)
 __global__ void bk_split1_kernel(float4 *dst, const uint32_t *src, int rows, const Fft512Tables *T)
 {
-    __shared__ double2 xp_s[4][512];
+    __shared__ double2 xp_s[4][FFT512_XP];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int poly = blockIdx.x * 4 + w;
     if (poly >= rows * 2) return;
@@ -240,7 +240,7 @@ __global__ void bk_split1_kernel(float4 *dst, const uint32_t *src, int rows, con
 // transform, rounded: exact for keys that are transforms of 32-bit integers)
 __global__ void bk_fft1_to_int_kernel(uint32_t *dst, const double2 *src, int rows, const Fft512Tables *T)
 {
-    __shared__ double2 xp_s[4][512];
+    __shared__ double2 xp_s[4][FFT512_XP];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int poly = blockIdx.x * 4 + w;
     if (poly >= rows * 2) return;

@@ -25,7 +25,7 @@ struct Pbs01Smem {
     static constexpr int CHUNK_BYTES = 16384;  // one TRGSW row: 2 outputs x 512 complex x 16 B
     static constexpr int TAB_OFF = RING_OFF + S * CHUNK_BYTES;
     static constexpr int WARP_OFF = TAB_OFF + ((int)sizeof(Fft512Tables) + 127) / 128 * 128;
-    static constexpr int XP_BYTES = 512 * 16;
+    static constexpr int XP_BYTES = FFT512_XP * 16;
     static constexpr int ACC_BYTES = 2 * N1 * 4;
     static constexpr int ABAR_BYTES = ((N0 * 2) + 127) / 128 * 128;
     static constexpr int PER_WARP = XP_BYTES + ACC_BYTES + ABAR_BYTES;

@@ -34,7 +34,7 @@ struct Pbs01SplitSmem {
     static constexpr int CHUNK_BYTES = 16384;   // 16 slots x 2 outputs x 32 lanes x float4(hi, lo)
     static constexpr int TAB_OFF = RING_OFF + S * CHUNK_BYTES;
     static constexpr int WARP_OFF = TAB_OFF + ((int)sizeof(Fft512TablesF) + 127) / 128 * 128;
-    static constexpr int XP_BYTES = 512 * 8;
+    static constexpr int XP_BYTES = FFT512_XP * 8;
     static constexpr int ACC_BYTES = 2 * N1 * 4;
     static constexpr int ABAR_BYTES = ((N0 * 2) + 127) / 128 * 128;
     static constexpr int PER_WARP = XP_BYTES + ACC_BYTES + ABAR_BYTES;
