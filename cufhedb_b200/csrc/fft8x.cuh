@@ -256,18 +256,22 @@ __device__ __forceinline__ void group_sync(int id)
     else asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(T) : "memory");
 }
 
-// transpose scratch index: row t (the thread of stage A), column k; the XOR
-// swizzle keeps both the row-wise write and the column-wise read conflict-free
+// transpose scratch: row t (the thread of stage A) holds its 8 values in a
+// row padded to 9 entries (FFT8X_XP<T> entries in all), which keeps both the
+// row-wise write and the column-wise read free of bank conflicts for 8- and
+// 16-byte elements, with every address a per-thread base plus a compile-time
+// offset
+template <int T>
+constexpr int FFT8X_XP = 9 * T;
 template <typename C>
 __device__ __forceinline__ int fft8x_xp(int t, int k)
 {
-    if constexpr (sizeof(C) == 16) return t * 8 + (k ^ (t & 7));
-    else return t * 8 + (k ^ ((t >> 1) & 7));
+    return t * 9 + k;
 }
 
 // forward: v[j] = z_{t + T j} / w^t in (the inputs multiplied by W_32^j only),
-// v[s] = V(fft8x_freq<T>(t, s)) out.  xp: M-entry scratch shared by the
-// group; bar: its named barrier.
+// v[s] = V(fft8x_freq<T>(t, s)) out.  xp: FFT8X_XP<T>-entry scratch shared
+// by the group; bar: its named barrier.
 template <typename C, int T>
 __device__ __forceinline__ void fft8x_fwd(C v[8], C *xp, const Fft8xTables<C, T> &tab, int t, int bar)
 {

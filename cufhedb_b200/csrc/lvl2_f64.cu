@@ -79,7 +79,7 @@ struct Pbs02Smem {
     static constexpr int RING_OFF = RING_HEADER_BYTES;
     static constexpr int TAB_OFF = RING_OFF + S * CHUNK_BYTES;
     static constexpr int GROUP_OFF = TAB_OFF + ((int)sizeof(Fft1024Tables) + 127) / 128 * 128;
-    static constexpr int XP_BYTES = 1024 * 16;
+    static constexpr int XP_BYTES = FFT8X_XP<T2> * 16;
     static constexpr int ACC_BYTES = 2 * N2 * 8;
     static constexpr int ABAR_BYTES = ((N0 * 2) + 127) / 128 * 128;
     static constexpr int PER_GROUP = XP_BYTES + ACC_BYTES + ABAR_BYTES;
@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(4 * P * 32, 1) pbs02_f64_kernel(Pbs02Args a)
 // [rows][2 o][8 s][128 u] complex (one 1024-complex chunk per (row, o))
 __global__ void __launch_bounds__(T2) bk_fft2_kernel(double2 *dst, const uint64_t *src, const Fft1024Tables *T)
 {
-    __shared__ double2 xp_s[1024];
+    __shared__ double2 xp_s[FFT8X_XP<T2>];
     const int t = threadIdx.x;
     const size_t poly = blockIdx.x;
     const uint64_t *p = src + poly * N2;
@@ -227,7 +227,7 @@ __global__ void bk_permute2_kernel(double2 *dst, const double *src, int rows)
 
 __global__ void __launch_bounds__(T2) twist_ifft2_kernel(double *out, const uint64_t *in, const Fft1024Tables *T)
 {
-    __shared__ double2 xp_s[1024];
+    __shared__ double2 xp_s[FFT8X_XP<T2>];
     const int t = threadIdx.x;
     const size_t p = blockIdx.x;
     const uint64_t *x = in + p * N2;
@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(T2) twist_ifft2_kernel(double *out, const uint
 
 __global__ void __launch_bounds__(T2) twist_fft2_kernel(uint64_t *out, const double *in, const Fft1024Tables *T)
 {
-    __shared__ double2 xp_s[1024];
+    __shared__ double2 xp_s[FFT8X_XP<T2>];
     const int t = threadIdx.x;
     const size_t p = blockIdx.x;
     const double *x = in + p * N2;
@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(T2) twist_fft2_kernel(uint64_t *out, const dou
 // one product per 128-thread block; trgsw prepared: [8 rows][2 o][1024] complex
 __global__ void __launch_bounds__(T2) extprod2_kernel(ExtProd2Args a)
 {
-    __shared__ double2 xp_s[1024];
+    __shared__ double2 xp_s[FFT8X_XP<T2>];
     const int t = threadIdx.x;
     const size_t p = blockIdx.x;
     const Fft1024Tables &T = *a.tables;
