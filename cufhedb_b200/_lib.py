@@ -65,6 +65,7 @@ SIGNATURES = {
     "cufhedb_load_keyfile": [_vp, C.c_char_p, _vp],
     "cufhedb_arc_compare": [_vp, _i32, _vp, _vp, _vp, _i32, _i32, _i32, _vp],
     "cufhedb_polymul_lvl1": [_vp, _vp, _vp, _vp, _i32, _i32, _vp],
+    "cufhedb_selftest_wait_timeout": [_vp, C.c_uint32],
     "cufhedb_polymul_lvl2": [_vp, _vp, _vp, _vp, _i32, _i32, _vp],
     "cufhedb_save_keyfile": [_vp, C.c_char_p, _vp],
     "cufhedb_phase_lvl2": [_vp, _vp, _vp, _vp, _i32, _vp],

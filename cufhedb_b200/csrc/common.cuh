@@ -80,10 +80,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// returns false if the phase did not complete within WAIT_LIMIT polls
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+// returns false if the phase did not complete within `limit` polls
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit = WAIT_LIMIT)
 {
-    for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
+    for (uint32_t it = 0; it < limit; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }

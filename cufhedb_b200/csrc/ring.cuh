@@ -34,6 +34,7 @@ struct KeyRing {
     const unsigned char *src;   // the key: `per_pass` chunks, CHUNK bytes each
     uint32_t per_pass;          // chunks in one pass over the key
     uint32_t total;             // chunks this block consumes (passes x per_pass)
+    uint32_t limit = WAIT_LIMIT;   // polls per bounded wait
 
     __device__ __forceinline__ void init_by_thread0()
     {
@@ -66,7 +67,7 @@ struct KeyRing {
     __device__ __forceinline__ const unsigned char *acquire(uint32_t c, int *err)
     {
         const int s = c % S;
-        if (!aborted() && !mbar_wait(&h->full[s], (c / S) & 1)) {
+        if (!aborted() && !mbar_wait(&h->full[s], (c / S) & 1, limit)) {
             report_error(err, DEV_TIMEOUT_FULL);
             *(volatile int *)&h->abort = 1;
         }
@@ -94,7 +95,7 @@ struct KeyRing {
     {
         if (!aborted()) return;
         for (int s = 0; s < S; ++s)
-            if (h->issued[s] > 0 && !mbar_wait(&h->full[s], (uint32_t)(h->issued[s] - 1) & 1))
+            if (h->issued[s] > 0 && !mbar_wait(&h->full[s], (uint32_t)(h->issued[s] - 1) & 1, limit))
                 report_error(err, DEV_TIMEOUT_DRAIN);
     }
 };

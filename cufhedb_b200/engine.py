@@ -305,6 +305,11 @@ class Engine:
         check(self.lib.cufhedb_polymul_lvl2(self.ctx, _ptr(a_dev), _ptr(m_fd_dev), _ptr(out_dev), B, int(shared),
                                             _stream(stream)))
 
+    def selftest_wait_timeout(self, polls: int = 4096) -> int:
+        """run the bounded-wait self-test; returns the raw status (ERR_DEVICE
+        when the expired wait was recorded and reported, as it should be)"""
+        return self.lib.cufhedb_selftest_wait_timeout(self.ctx, polls)
+
     ARC_OPS = {"gt": 0, "lt": 1, "eq": 2, "lt_strict": 3}
 
     def arc_compare(self, op: str, trlwe_dev, trgsw_prepared, out_dev, digits: int, precision=_lib.FP64,

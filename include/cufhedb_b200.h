@@ -303,6 +303,13 @@ CUFHEDB_API int cufhedb_extprod_lvl1_host(cufhedb_ctx *ctx, const uint32_t *trlw
 CUFHEDB_API int cufhedb_gate_lvl1_host(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint32_t *cb, uint32_t *out, int B,
                            int precision);
 
+/* Self-test of the kernels' bounded waits (no counterpart in the reference,
+ * which has none): one block waits `polls` times (1 .. 2^20) for a key-ring
+ * chunk that is never issued, gives up, records the failure and returns.
+ * Returns what cufhedb_sync then reports: CUFHEDB_ERR_DEVICE with the wait's
+ * code when the path works; the context stays usable afterwards. */
+CUFHEDB_API int cufhedb_selftest_wait_timeout(cufhedb_ctx *ctx, uint32_t polls);
+
 /* ---- launch-shape autotuner --------------------------------------------------- */
 /* Times one full pass of the lvl01 PBS kernel (uniform random lvl0 inputs,
  * the loaded key) with 7 and with 8 ciphertexts per CTA for `precision`, and

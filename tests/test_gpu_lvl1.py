@@ -296,3 +296,26 @@ def test_autotuned_launch_shapes_decrypt(engine, oracle, keys, precision):
         engine.sync()
         got = (ph > 0).cpu().numpy().astype(int)
         assert np.array_equal(got, (bits[0] & bits[1]).numpy().astype(int))
+
+
+def test_bounded_wait_expires_reports_and_context_survives(engine, oracle, keys):
+    """A key-ring wait that can never complete (no chunk is issued) gives up
+    after its poll limit, the failure is reported by cufhedb_sync, and the
+    same context then bootstraps correctly."""
+    from cufhedb_b200 import _lib
+    rc = engine.selftest_wait_timeout(4096)
+    assert rc == _lib.ERR_DEVICE
+    assert b"bounded wait" in _lib.load().cufhedb_last_error()
+    # reported once, then cleared
+    engine.sync()
+    _, s1, _ = keys
+    B = 16
+    bits = np.arange(B) % 2
+    ca = np.stack([oracle.tlwe32(MU if b else (-MU) & 0xFFFFFFFF, s1, NS_LVL1, SEED, 0x45, i) for i, b in enumerate(bits)])
+    cb = np.stack([oracle.tlwe32(MU, s1, NS_LVL1, SEED, 0x46, i) for i in range(B)])
+    out = empty_dev(B * (N1 + 1))
+    engine.gate_lvl1("NAND", dev(ca), dev(cb), out)
+    engine.sync()
+    got = host(out).reshape(B, N1 + 1)
+    for i in range(B):
+        assert (phase(oracle, got[i], s1) > 0) == (not (bits[i] and 1))
