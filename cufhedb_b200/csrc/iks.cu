@@ -8,7 +8,8 @@
 // The reference runs this on the host for every GPU bootstrap
 // (src/cuHEDB/gatebootstrap_gpu.cuh:42,133).  Here it is an HBM-bound gather:
 // one CTA per ciphertext walks the input coefficients in chunks of NT; each
-// chunk's digits are decoded into a shared list of selected key rows, then
+// chunk's digits are decoded into a shared list of selected key rows (in key
+// order), then
 // every thread accumulates a fixed set of output words over those rows with
 // several rows' loads in flight.  All CTAs of a batch walk the key in the same
 // order, so concurrently running CTAs that select the same row share it in L2.
@@ -71,8 +72,10 @@ __device__ __forceinline__ uint64_t iks_input(const IksArgs &a, size_t base, int
 template <int NT, bool WIDE, int NIN, int BASEBIT, int TT, int NOUT>
 __global__ void __launch_bounds__(NT) iks_kernel(IksArgs a)
 {
+    static_assert(NT % 32 == 0, "whole warps");
+    constexpr int NW = NT / 32;
     __shared__ uint32_t rowid[NT * TT];
-    __shared__ int cnt;
+    __shared__ int wsum[NW];
     constexpr int W = WIDE ? 64 : 32;
     constexpr uint64_t prec = 1ull << (W - (1 + BASEBIT * TT));
     constexpr uint32_t mask = (1u << BASEBIT) - 1;
@@ -83,20 +86,42 @@ __global__ void __launch_bounds__(NT) iks_kernel(IksArgs a)
 #pragma unroll
     for (int p = 0; p < PER; ++p) acc[p] = 0;
 
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int i0 = 0; i0 < NIN; i0 += NT) {
-        if (threadIdx.x == 0) cnt = 0;
-        __syncthreads();
+        // the chunk's selected rows, compacted in key order (ascending i, j)
+        // so that every CTA of the batch walks the key the same way and rows
+        // that several ciphertexts select are fetched close together in time
         const int i = i0 + threadIdx.x;
+        uint32_t ids[TT];
+        int n = 0;
         if (i < NIN) {
             const uint64_t abar = iks_input<WIDE>(a, base, i) + prec;
 #pragma unroll
             for (int j = 0; j < TT; ++j) {
                 const uint32_t d = (uint32_t)((WIDE ? abar : (uint32_t)abar) >> (W - (j + 1) * BASEBIT)) & mask;
-                if (d) rowid[atomicAdd(&cnt, 1)] = ((uint32_t)i * TT + j) * mask + d - 1;
+                if (d) ids[n++] = ((uint32_t)i * TT + j) * mask + d - 1;
             }
         }
+        int incl = n;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl += y;
+        }
+        if (lane == 31) wsum[wid] = incl;
         __syncthreads();
-        gather_rows<NOUT, NT>(a.ksk, rowid, cnt, acc);
+        int pos = incl - n, total = 0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+            const int c = wsum[w];
+            if (w < wid) pos += c;
+            total += c;
+        }
+#pragma unroll
+        for (int j = 0; j < TT; ++j)
+            if (j < n) rowid[pos + j] = ids[j];
+        __syncthreads();
+        gather_rows<NOUT, NT>(a.ksk, rowid, total, acc);
         __syncthreads();
     }
 
