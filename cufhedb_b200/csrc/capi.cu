@@ -86,12 +86,17 @@ void build_tables2(Fft1024Tables &T) { build_fft8x_tables<T2>(T); }
 
 void build_tables_f(const Fft512Tables &D, Fft512TablesF &F)
 {
+    auto dup = [](double c, double s) { return make_float4((float)c, (float)c, (float)s, (float)s); };
     for (int i = 0; i < 512; ++i) {
         F.tw512[i] = make_float2((float)D.tw512[i].x, (float)D.tw512[i].y);
         F.twist[i] = make_float2((float)D.twist[i].x, (float)D.twist[i].y);
-        F.untwist[i] = make_float2((float)(D.twist[i].x / 512.0), (float)(-D.twist[i].y / 512.0));
+        F.tw512p[i] = dup(D.tw512[i].x, D.tw512[i].y);
+        F.untwistp[i] = dup(D.twist[i].x / 512.0, -D.twist[i].y / 512.0);
     }
-    for (int j = 0; j < 16; ++j) F.w32[j] = make_float2((float)D.w32[j].x, (float)D.w32[j].y);
+    for (int j = 0; j < 16; ++j) {
+        F.w32[j] = make_float2((float)D.w32[j].x, (float)D.w32[j].y);
+        F.w32p[j] = dup(D.w32[j].x, D.w32[j].y);
+    }
 }
 
 struct GateSpec {

@@ -88,62 +88,61 @@ __global__ void __launch_bounds__(128) extprod1_f64_kernel(ExtProdArgs a)
     }
 }
 
-__device__ __forceinline__ void store_split(uint32_t *o, float2 hi[16], float2 lo[16], float2 *xp, int lane,
+// o = the torus32 polynomial of the paired (hi, lo) frequency accumulator f:
+// round(hi) * 2^24 + round(lo) (mod 2^32)
+__device__ __forceinline__ void store_split(uint32_t *o, CP f[16], unsigned long long *xp, int lane,
                                             const Fft512TablesF &T)
 {
-    ffft512_inv(hi, xp, T, lane);
-    ffft512_inv(lo, xp, T, lane);
+    pfft512_inv(f, xp, T, lane);
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int m = lane + 32 * m2;
-        const float2 yh = fcmulc(hi[m2], T.twist[m2 * 32 + lane]);
-        const float2 yl = fcmulc(lo[m2], T.twist[m2 * 32 + lane]);
-        o[m] = ((uint32_t)__float2int_rn(yh.x * (1.0f / 512.0f)) << 24) +
-               (uint32_t)__float2ll_rn(yl.x * (1.0f / 512.0f));
-        o[m + 512] = ((uint32_t)__float2int_rn(yh.y * (1.0f / 512.0f)) << 24) +
-                     (uint32_t)__float2ll_rn(yl.y * (1.0f / 512.0f));
+        const CP y = pmul_t(f[m2], T.untwistp[m2 * 32 + lane]);
+        const float2 re = unpk2(y.re), im = unpk2(y.im);
+        o[m] = ((uint32_t)__float2int_rn(re.x) << 24) + (uint32_t)__float2ll_rn(re.y);
+        o[m + 512] = ((uint32_t)__float2int_rn(im.x) << 24) + (uint32_t)__float2ll_rn(im.y);
+    }
+}
+
+// both limbs of one output: f (+)= v * k, k = (hi.re, lo.re, hi.im, lo.im)
+__device__ __forceinline__ void pmac_limbs(CP &f, float2 v, float4 k, bool first)
+{
+    const unsigned long long vr = pk2(v.x, v.x), vi = pk2(v.y, v.y), nvi = pk2(-v.y, -v.y);
+    const unsigned long long kr = pk2(k.x, k.y), ki = pk2(k.z, k.w);
+    if (first) {
+        f.re = f2(nvi, ki, m2(vr, kr));
+        f.im = f2(vi, kr, m2(vr, ki));
+    } else {
+        f.re = f2(nvi, ki, f2(vr, kr, f.re));
+        f.im = f2(vi, kr, f2(vr, ki, f.im));
     }
 }
 
 __global__ void __launch_bounds__(128) extprod1_split_kernel(ExtProdArgs a)
 {
-    __shared__ float2 xp_s[4][FFT512_XP];
+    __shared__ unsigned long long xp_s[4][FFT512_XP];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int p = blockIdx.x * 4 + w;
     if (p >= a.B) return;
     const Fft512TablesF &T = *reinterpret_cast<const Fft512TablesF *>(a.tables);
     const uint32_t *in = a.trlwe + (size_t)p * 2 * N1;
     const float4 *g = reinterpret_cast<const float4 *>(a.trgsw) + (a.shared ? 0 : (size_t)p * 6 * 1024);
-    float2 f0h[16], f0l[16], f1h[16], f1l[16];
+    CP f0[16], f1[16];
 #pragma unroll 1
     for (int r = 0; r < 2 * L1; ++r) {
         float2 v[16];
         digits_f32(v, in + (r / L1) * N1, r % L1, lane, T);
-        ffft512_fwd(v, xp_s[w], T, lane);
+        ffft512_fwd(v, reinterpret_cast<float2 *>(xp_s[w]), T, lane);
         const float4 *gc = g + (size_t)r * 1024;
-        if (r == 0) {
 #pragma unroll
-            for (int s = 0; s < 16; ++s) {
-                const float4 k0 = gc[(2 * s) * 32 + lane], k1 = gc[(2 * s + 1) * 32 + lane];
-                f0h[s] = fcmul(v[s], make_float2(k0.x, k0.y));
-                f0l[s] = fcmul(v[s], make_float2(k0.z, k0.w));
-                f1h[s] = fcmul(v[s], make_float2(k1.x, k1.y));
-                f1l[s] = fcmul(v[s], make_float2(k1.z, k1.w));
-            }
-        } else {
-#pragma unroll
-            for (int s = 0; s < 16; ++s) {
-                const float4 k0 = gc[(2 * s) * 32 + lane], k1 = gc[(2 * s + 1) * 32 + lane];
-                fcfma(f0h[s], v[s], make_float2(k0.x, k0.y));
-                fcfma(f0l[s], v[s], make_float2(k0.z, k0.w));
-                fcfma(f1h[s], v[s], make_float2(k1.x, k1.y));
-                fcfma(f1l[s], v[s], make_float2(k1.z, k1.w));
-            }
+        for (int s = 0; s < 16; ++s) {
+            pmac_limbs(f0[s], v[s], gc[(2 * s) * 32 + lane], r == 0);
+            pmac_limbs(f1[s], v[s], gc[(2 * s + 1) * 32 + lane], r == 0);
         }
     }
     uint32_t *o = a.out + (size_t)p * 2 * N1;
-    store_split(o, f0h, f0l, xp_s[w], lane, T);
-    store_split(o + N1, f1h, f1l, xp_s[w], lane, T);
+    store_split(o, f0, xp_s[w], lane, T);
+    store_split(o + N1, f1, xp_s[w], lane, T);
 }
 
 }  // namespace

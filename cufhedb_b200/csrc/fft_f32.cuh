@@ -9,11 +9,15 @@
 
 namespace cfdb {
 
+// scalar tables for the forward transform, and the inverse transform's tables
+// with each cosine and sine duplicated (c, c, s, s) for the paired form below
 struct Fft512TablesF {
     float2 tw512[512];
     float2 twist[512];
-    float2 untwist[512];   // conj(twist) / 512: inverse untwist and scaling in one product
     float2 w32[16];
+    float4 tw512p[512];
+    float4 untwistp[512];   // conj(twist) / 512: inverse untwist and scaling in one product
+    float4 w32p[16];
 };
 
 __device__ __forceinline__ unsigned long long f2_bits(float2 a)
@@ -142,6 +146,175 @@ __device__ __forceinline__ void ffft512_fwd(float2 v[16], float2 *xp, const Fft5
         v[j] = fadd2(a, t);
         v[8 + j] = fsub2(a, t);
     }
+}
+
+// ---- paired form: two polynomials transformed in lock step ----------------------
+// A CP holds one complex value of each of two polynomials as (re_0, re_1),
+// (im_0, im_1): every operation is one packed f32x2 instruction per
+// component, the same for both.  Used for the hi and lo limb of one output.
+struct CP {
+    unsigned long long re, im;
+};
+
+__device__ __forceinline__ unsigned long long pk2(float a, float b)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ float2 unpk2(unsigned long long v)
+{
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+    return r;
+}
+__device__ __forceinline__ unsigned long long a2(unsigned long long a, unsigned long long b)
+{
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned long long s2(unsigned long long a, unsigned long long b)
+{
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned long long m2(unsigned long long a, unsigned long long b)
+{
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned long long f2(unsigned long long a, unsigned long long b, unsigned long long c)
+{
+    unsigned long long r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+
+__device__ __forceinline__ CP padd(CP a, CP b) { return CP{a2(a.re, b.re), a2(a.im, b.im)}; }
+__device__ __forceinline__ CP psub(CP a, CP b) { return CP{s2(a.re, b.re), s2(a.im, b.im)}; }
+// a * (c + i s) for a twiddle stored (c, c, s, s)
+__device__ __forceinline__ CP pmul_t(CP a, float4 w)
+{
+    const unsigned long long C = pk2(w.x, w.y), S = pk2(w.z, w.w);
+    return CP{s2(m2(a.re, C), m2(a.im, S)), f2(a.re, S, m2(a.im, C))};
+}
+// a * conj(c + i s)
+__device__ __forceinline__ CP pmulc_t(CP a, float4 w)
+{
+    const unsigned long long C = pk2(w.x, w.y), S = pk2(w.z, w.w);
+    return CP{f2(a.re, C, m2(a.im, S)), s2(m2(a.im, C), m2(a.re, S))};
+}
+__device__ __forceinline__ CP pshfl_xor(CP v, int m)
+{
+    const float2 r = unpk2(v.re), i = unpk2(v.im);
+    return CP{pk2(__shfl_xor_sync(0xffffffffu, r.x, m), __shfl_xor_sync(0xffffffffu, r.y, m)),
+              pk2(__shfl_xor_sync(0xffffffffu, i.x, m), __shfl_xor_sync(0xffffffffu, i.y, m))};
+}
+__device__ __forceinline__ CP psel(bool c, CP a, CP b) { return c ? a : b; }
+
+template <int S>
+__device__ __forceinline__ void pdft4(CP &a0, CP &a1, CP &a2_, CP &a3)
+{
+    const CP s02 = padd(a0, a2_), d02 = psub(a0, a2_);
+    const CP s13 = padd(a1, a3), d13 = psub(a1, a3);
+    a0 = padd(s02, s13);
+    a2_ = psub(s02, s13);
+    // a1 = d02 + i^S d13, a3 = d02 - i^S d13 (i d = (-d.im, d.re))
+    if constexpr (S > 0) {
+        a1 = CP{s2(d02.re, d13.im), a2(d02.im, d13.re)};
+        a3 = CP{a2(d02.re, d13.im), s2(d02.im, d13.re)};
+    } else {
+        a1 = CP{a2(d02.re, d13.im), s2(d02.im, d13.re)};
+        a3 = CP{s2(d02.re, d13.im), a2(d02.im, d13.re)};
+    }
+}
+
+template <int S, int E>
+__device__ __forceinline__ CP pw16(CP a)
+{
+    constexpr float C1 = 0.92387953251128673848f;
+    constexpr float S1 = 0.38268343236508978178f;
+    constexpr float R2 = 0.70710678118654752440f;
+    if constexpr (E == 0) return a;
+    else if constexpr (E == 4) {
+        const unsigned long long zero = pk2(0.0f, 0.0f);
+        return (S > 0) ? CP{s2(zero, a.im), a.re} : CP{a.im, s2(zero, a.re)};
+    } else if constexpr (E == 2) {
+        const unsigned long long r = pk2(R2, R2);
+        return (S > 0) ? CP{m2(s2(a.re, a.im), r), m2(a2(a.re, a.im), r)}
+                       : CP{m2(a2(a.re, a.im), r), m2(s2(a.im, a.re), r)};
+    } else if constexpr (E == 6) {
+        const unsigned long long r = pk2(R2, R2), nr = pk2(-R2, -R2);
+        return (S > 0) ? CP{m2(a2(a.re, a.im), nr), m2(s2(a.re, a.im), r)}
+                       : CP{m2(s2(a.im, a.re), r), m2(a2(a.re, a.im), nr)};
+    } else {
+        constexpr float c = (E == 1) ? C1 : (E == 3) ? S1 : -C1;
+        constexpr float s0 = (E == 1) ? S1 : (E == 3) ? C1 : -S1;
+        constexpr float sn = (S > 0) ? s0 : -s0;
+        const unsigned long long Cp = pk2(c, c), Sp = pk2(sn, sn), NSp = pk2(-sn, -sn);
+        return CP{f2(a.re, Cp, m2(a.im, NSp)), f2(a.re, Sp, m2(a.im, Cp))};
+    }
+}
+
+template <int S>
+__device__ __forceinline__ void pdft16(CP v[16])
+{
+#pragma unroll
+    for (int n1 = 0; n1 < 4; ++n1) pdft4<S>(v[n1], v[n1 + 4], v[n1 + 8], v[n1 + 12]);
+    v[5] = pw16<S, 1>(v[5]);
+    v[6] = pw16<S, 2>(v[6]);
+    v[7] = pw16<S, 3>(v[7]);
+    v[9] = pw16<S, 2>(v[9]);
+    v[10] = pw16<S, 4>(v[10]);
+    v[11] = pw16<S, 6>(v[11]);
+    v[13] = pw16<S, 3>(v[13]);
+    v[14] = pw16<S, 6>(v[14]);
+    v[15] = pw16<S, 9>(v[15]);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) pdft4<S>(v[4 * k2], v[4 * k2 + 1], v[4 * k2 + 2], v[4 * k2 + 3]);
+    CP t[16];
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2)
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) t[k2 + 4 * k1] = v[4 * k2 + k1];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = t[i];
+}
+
+// inverse transform of two polynomials at once (the sequence of ffft512_inv);
+// xp: this warp's FFT512_XP 8-byte entries, through which the real and the
+// imaginary parts are transposed one after the other
+__device__ __forceinline__ void pfft512_inv(CP v[16], unsigned long long *xp, const Fft512TablesF &T, int lane)
+{
+    const int h = lane >> 4, q2 = lane & 15;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const CP a = v[j], b = v[8 + j];
+        const CP g0 = padd(a, b);
+        const CP g1 = pmulc_t(psub(a, b), T.w32p[j + 8 * h]);
+        const CP recv = pshfl_xor(psel(h, g0, g1), 16);
+        v[j] = psel(h, recv, g0);
+        v[8 + j] = psel(h, g1, recv);
+    }
+    pdft16<-1>(v);
+    __syncwarp();
+#pragma unroll
+    for (int m1p = 0; m1p < 16; ++m1p) xp[xpf_index(2 * m1p + h, q2)] = v[m1p].re;
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k].re = xp[xpf_index(lane, k)];
+    __syncwarp();
+#pragma unroll
+    for (int m1p = 0; m1p < 16; ++m1p) xp[xpf_index(2 * m1p + h, q2)] = v[m1p].im;
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k].im = xp[xpf_index(lane, k)];
+#pragma unroll
+    for (int k = 1; k < 16; ++k) v[k] = pmulc_t(v[k], T.tw512p[k * 32 + lane]);
+    pdft16<-1>(v);
 }
 
 __device__ __forceinline__ void ffft512_inv(float2 v[16], float2 *xp, const Fft512TablesF &T, int lane)

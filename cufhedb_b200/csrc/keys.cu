@@ -208,7 +208,8 @@ __global__ void bk_permute1_kernel(double2 *dst, const double *src, int rows)
 
 // integer key polynomials [rows][2][1024] -> two limbs hi = round(b / 2^24),
 // lo = b - hi * 2^24, each transformed in FP64 and stored as FP32 in the
-// split-precision chunk layout [rows][16 s][2 o][32 lane] float4(hi, lo)
+// split-precision chunk layout [rows][16 s][2 o][32 lane]
+// float4(hi.re, lo.re, hi.im, lo.im), the pairs the paired products read
 __global__ void bk_split1_kernel(float4 *dst, const uint32_t *src, int rows, const Fft512Tables *T)
 {
     __shared__ double2 xp_s[4][FFT512_XP];
@@ -233,7 +234,7 @@ __global__ void bk_split1_kernel(float4 *dst, const uint32_t *src, int rows, con
     float4 *d = dst + (size_t)row * 1024;
 #pragma unroll
     for (int s = 0; s < 16; ++s)
-        d[(2 * s + o) * 32 + lane] = make_float4((float)vh[s].x, (float)vh[s].y, (float)vl[s].x, (float)vl[s].y);
+        d[(2 * s + o) * 32 + lane] = make_float4((float)vh[s].x, (float)vl[s].x, (float)vh[s].y, (float)vl[s].y);
 }
 
 // FFT-domain key in the FP64 chunk layout -> integer polynomials (the inverse

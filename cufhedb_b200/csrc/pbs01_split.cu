@@ -66,27 +66,37 @@ __device__ __forceinline__ void digits_from_words_f(float2 v[16], const uint32_t
 }
 
 // poly[m] += round(hi_m) * 2^24 + round(lo_m) (mod 2^32), one read-modify-write
-// of the accumulator per polynomial.  The hi limb's products round exactly;
-// the lo limb's FP32 error stays far below the bootstrapping noise.
-__device__ __forceinline__ void add_inverse_split(uint32_t *poly, float2 hi[16], float2 lo[16], float2 *xp, int lane,
+// of the accumulator per polynomial.  f holds the hi and lo limbs of one
+// output as pairs, inverse-transformed together.  The hi limb's products
+// round exactly; the lo limb's FP32 error stays far below the bootstrapping
+// noise.
+__device__ __forceinline__ void add_inverse_split(uint32_t *poly, CP f[16], unsigned long long *xp, int lane,
                                                   const Fft512TablesF &T)
 {
-    uint32_t t[32];
-    ffft512_inv(hi, xp, T, lane);
-#pragma unroll
-    for (int m2 = 0; m2 < 16; ++m2) {
-        const float2 y = fcmul(hi[m2], T.untwist[m2 * 32 + lane]);
-        t[2 * m2] = (uint32_t)__float2int_rn(y.x) << 24;
-        t[2 * m2 + 1] = (uint32_t)__float2int_rn(y.y) << 24;
-    }
-    ffft512_inv(lo, xp, T, lane);
+    pfft512_inv(f, xp, T, lane);
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int m = lane + 32 * m2;
-        const float2 y = fcmul(lo[m2], T.untwist[m2 * 32 + lane]);
-        poly[m] += t[2 * m2] + (uint32_t)__float2ll_rn(y.x);
-        poly[m + 512] += t[2 * m2 + 1] + (uint32_t)__float2ll_rn(y.y);
+        const CP y = pmul_t(f[m2], T.untwistp[m2 * 32 + lane]);
+        const float2 re = unpk2(y.re), im = unpk2(y.im);   // (hi, lo) of coefficients m and m + 512
+        poly[m] += ((uint32_t)__float2int_rn(re.x) << 24) + (uint32_t)__float2ll_rn(re.y);
+        poly[m + 512] += ((uint32_t)__float2int_rn(im.x) << 24) + (uint32_t)__float2ll_rn(im.y);
     }
+}
+
+// f += v * k for both limbs of one output: k = (hi.re, lo.re, hi.im, lo.im),
+// vr = (v.re, v.re), vi = (v.im, v.im), nvi = (-v.im, -v.im)
+__device__ __forceinline__ void pmac(CP &f, unsigned long long vr, unsigned long long vi, unsigned long long nvi,
+                                     float4 k)
+{
+    const unsigned long long kr = pk2(k.x, k.y), ki = pk2(k.z, k.w);
+    f.re = f2(nvi, ki, f2(vr, kr, f.re));
+    f.im = f2(vi, kr, f2(vr, ki, f.im));
+}
+__device__ __forceinline__ CP pmul_first(unsigned long long vr, unsigned long long vi, unsigned long long nvi, float4 k)
+{
+    const unsigned long long kr = pk2(k.x, k.y), ki = pk2(k.z, k.w);
+    return CP{f2(nvi, ki, m2(vr, kr)), f2(vi, kr, m2(vr, ki))};
 }
 
 // W consumer warps, plus a producer warp when PRODUCER (ring.cuh has both
@@ -121,7 +131,7 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
     }
 
     unsigned char *wb = smem + L::WARP_OFF + warp * L::PER_WARP;
-    float2 *xp = reinterpret_cast<float2 *>(wb);
+    unsigned long long *xp = reinterpret_cast<unsigned long long *>(wb);
     uint32_t *acc = reinterpret_cast<uint32_t *>(wb + L::XP_BYTES);
     uint16_t *abar_s = reinterpret_cast<uint16_t *>(wb + L::XP_BYTES + L::ACC_BYTES);
 
@@ -144,7 +154,7 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
         for (int i = 0; i < N0; ++i) {
             const uint32_t ab = valid ? abar_s[i] : 0u;
             const bool active = ab != 0;
-            float2 f0h[16], f0l[16], f1h[16], f1l[16];
+            CP f0[16], f1[16];
             uint32_t w[32];
 #pragma unroll 1
             for (int r = 0; r < 2 * L1; ++r, ++c) {
@@ -153,32 +163,32 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
                 if (active) {
                     float2 v[16];
                     digits_from_words_f(v, w, r % L1, lane, *T);
-                    ffft512_fwd(v, xp, *T, lane);
+                    ffft512_fwd(v, reinterpret_cast<float2 *>(xp), *T, lane);
                     if (r == 0) {
 #pragma unroll
                         for (int s = 0; s < 16; ++s) {
                             const float4 k0 = bkc[(2 * s) * 32 + lane], k1 = bkc[(2 * s + 1) * 32 + lane];
-                            f0h[s] = fcmul(v[s], make_float2(k0.x, k0.y));
-                            f0l[s] = fcmul(v[s], make_float2(k0.z, k0.w));
-                            f1h[s] = fcmul(v[s], make_float2(k1.x, k1.y));
-                            f1l[s] = fcmul(v[s], make_float2(k1.z, k1.w));
+                            const unsigned long long vr = pk2(v[s].x, v[s].x), vi = pk2(v[s].y, v[s].y),
+                                                     nvi = pk2(-v[s].y, -v[s].y);
+                            f0[s] = pmul_first(vr, vi, nvi, k0);
+                            f1[s] = pmul_first(vr, vi, nvi, k1);
                         }
                     } else {
 #pragma unroll
                         for (int s = 0; s < 16; ++s) {
                             const float4 k0 = bkc[(2 * s) * 32 + lane], k1 = bkc[(2 * s + 1) * 32 + lane];
-                            fcfma(f0h[s], v[s], make_float2(k0.x, k0.y));
-                            fcfma(f0l[s], v[s], make_float2(k0.z, k0.w));
-                            fcfma(f1h[s], v[s], make_float2(k1.x, k1.y));
-                            fcfma(f1l[s], v[s], make_float2(k1.z, k1.w));
+                            const unsigned long long vr = pk2(v[s].x, v[s].x), vi = pk2(v[s].y, v[s].y),
+                                                     nvi = pk2(-v[s].y, -v[s].y);
+                            pmac(f0[s], vr, vi, nvi, k0);
+                            pmac(f1[s], vr, vi, nvi, k1);
                         }
                     }
                 }
                 ring.release(c, lane);
             }
             if (active) {
-                add_inverse_split(acc, f0h, f0l, xp, lane, *T);
-                add_inverse_split(acc + N1, f1h, f1l, xp, lane, *T);
+                add_inverse_split(acc, f0, xp, lane, *T);
+                add_inverse_split(acc + N1, f1, xp, lane, *T);
                 __syncwarp();
             }
         }
@@ -195,7 +205,9 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
     }
 }
 
-constexpr int PBS01S_S = 6;
+// key-ring depth: 6 slots with 7 ciphertexts per CTA, 5 with 8 (shared memory)
+template <int W>
+constexpr int PBS01S_S = W == 7 ? 6 : 5;
 
 // 7 ciphertexts per CTA run with a producer warp (8 warps), 8 per CTA without
 // one (8 warps): both keep 2 warps per SM sub-partition (up to 255 registers)
@@ -203,9 +215,9 @@ template <int W>
 static cudaError_t launch_pbs01_split_t(const Pbs01Args &a, int grid, cudaStream_t st)
 {
     constexpr bool PROD = W == 7;
-    using L = Pbs01SplitSmem<W, PBS01S_S>;
+    using L = Pbs01SplitSmem<W, PBS01S_S<W>>;
     static_assert(L::TOTAL <= 227 * 1024, "shared memory budget");
-    pbs01_split_kernel<W, PBS01S_S, PROD><<<grid, (W + (PROD ? 1 : 0)) * 32, L::TOTAL, st>>>(a);
+    pbs01_split_kernel<W, PBS01S_S<W>, PROD><<<grid, (W + (PROD ? 1 : 0)) * 32, L::TOTAL, st>>>(a);
     return cudaGetLastError();
 }
 
@@ -219,12 +231,12 @@ cudaError_t launch_pbs01_split(const Pbs01Args &a, int num_sms, int w, cudaStrea
 
 cudaError_t init_pbs01_split()
 {
-    cudaError_t e = cudaFuncSetAttribute(pbs01_split_kernel<7, PBS01S_S, true>,
+    cudaError_t e = cudaFuncSetAttribute(pbs01_split_kernel<7, PBS01S_S<7>, true>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         Pbs01SplitSmem<7, PBS01S_S>::TOTAL);
+                                         Pbs01SplitSmem<7, PBS01S_S<7>>::TOTAL);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(pbs01_split_kernel<8, PBS01S_S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                Pbs01SplitSmem<8, PBS01S_S>::TOTAL);
+    return cudaFuncSetAttribute(pbs01_split_kernel<8, PBS01S_S<8>, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                Pbs01SplitSmem<8, PBS01S_S<8>>::TOTAL);
 }
 
 }  // namespace cfdb
