@@ -18,6 +18,7 @@
 #include "HEDB/utils/types.h"
 #include "cufhedb_b200/cuhedb_gpu.hpp"
 
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -25,6 +26,7 @@
 #include <memory>
 #include <random>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace {
@@ -307,6 +309,42 @@ void check_pbs02(std::mt19937_64 &rng, const TFHESecretKey &sk)
 
 }  // namespace
 
+// The reference's query programs call the per-row operators from an OpenMP
+// row loop, each thread with its own stream id (test/HE3_Query/TPCH_Q6.cu:
+// 179-181).  Here: 8 host threads, each running a mix of operators on its own
+// stream id at the same time, every result decrypted against the plaintext.
+void check_threads(const TFHESecretKey &sk, TFHEEvalKey &ek)
+{
+    constexpr int NT = 8, ROWS = 12;
+    std::atomic<int> bad{0};
+    std::vector<std::thread> th;
+    for (int t = 0; t < NT; t++)
+        th.emplace_back([&, t] {
+            std::mt19937_64 r(1000 + t);
+            const uint32_t sid = 4 + (uint32_t)t;
+            for (int i = 0; i < ROWS; i++) {
+                const bool a = r() & 1, b = r() & 1;
+                auto ca = TFHEpp::tlweSymEncrypt<Lvl1>(a ? Lvl1::μ : -Lvl1::μ, Lvl1::α, sk.key.get<Lvl1>());
+                auto cb = TFHEpp::tlweSymEncrypt<Lvl1>(b ? Lvl1::μ : -Lvl1::μ, Lvl1::α, sk.key.get<Lvl1>());
+                TLWELvl1 res;
+                cuHEDB::HomAND(res, ca, cb, ek, LOGIC, sid);
+                bad += dec_logic(res, sk) != (a && b);
+                const uint32_t x = r() % 64, y = r() % 64;
+                auto cx = enc_int<Lvl1>(x, 6, sk), cy = enc_int<Lvl1>(y, 6, sk);
+                cuHEDB::less_than_equal<Lvl1>(cx, cy, res, 6, ek, LOGIC, sid);
+                bad += dec_logic(res, sk) != (x <= y);
+                auto in = TFHEpp::tlweSymEncrypt<TFHEpp::lvl0param>(a ? TFHEpp::lvl0param::μ : -TFHEpp::lvl0param::μ,
+                                                                    TFHEpp::lvl0param::α,
+                                                                    sk.key.get<TFHEpp::lvl0param>());
+                cufftlvl1.GateBootstrappingTLWE2TLWEFFT_st(res, in, Lvl1::μ, sid);
+                bad += dec_logic(res, sk) != a;
+            }
+        });
+    for (auto &x : th) x.join();
+    report("8 host threads x 12 rows, own stream ids (AND, <=, PBS)", bad == 0,
+           "wrong " + std::to_string(bad.load()));
+}
+
 int main(int argc, char **argv)
 {
     const bool lvl2 = argc > 1 && std::strcmp(argv[1], "--lvl2") == 0;
@@ -339,6 +377,7 @@ int main(int argc, char **argv)
         check_compare<Lvl1>(rng, *sk, *ek, 6, 8, 2);
         check_batch_compare<Lvl1>(rng, *sk, *ek, 6, 512, CUFHEDB_FP64);
         check_batch_compare<Lvl1>(rng, *sk, *ek, 6, 512, CUFHEDB_SPLIT32);
+        check_threads(*sk, *ek);
         if (lvl2) {
             check_pbs02(rng, *sk);
             check_compare<Lvl2>(rng, *sk, *ek, 20, 3, 1);
