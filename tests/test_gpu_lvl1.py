@@ -319,3 +319,26 @@ def test_bounded_wait_expires_reports_and_context_survives(engine, oracle, keys)
     got = host(out).reshape(B, N1 + 1)
     for i in range(B):
         assert (phase(oracle, got[i], s1) > 0) == (not (bits[i] and 1))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split32"])
+def test_ragged_and_multi_pass_batches(engine, precision):
+    """One ciphertext, and a batch of two full passes over every SM plus a
+    ragged remainder (the persistent grid loops over groups, the last group
+    partly empty): every gate output decrypts to NAND."""
+    import torch
+    from cufhedb_b200 import FP64, SPLIT32
+    prec = FP64 if precision == "fp64" else SPLIT32
+    for B in (1, 2 * 7 * engine.num_sms + 5):
+        bits = torch.randint(0, 2, (2, B), generator=torch.Generator().manual_seed(B + 7))
+        msg = torch.where(bits == 1, MU, -MU).to(torch.int32).cuda()
+        ca, cb = empty_dev(B * (N1 + 1)), empty_dev(B * (N1 + 1))
+        engine.encrypt_lvl1(SEED, 0x66, 0, msg[0].contiguous(), ca)
+        engine.encrypt_lvl1(SEED, 0x66, B, msg[1].contiguous(), cb)
+        out = empty_dev(B * (N1 + 1))
+        engine.gate_lvl1("NAND", ca, cb, out, prec)
+        ph = empty_dev(B)
+        engine.phase_lvl1(out, ph)
+        engine.sync()
+        got = (ph > 0).cpu().numpy().astype(int)
+        assert np.array_equal(got, 1 - (bits[0] & bits[1]).numpy().astype(int)), B

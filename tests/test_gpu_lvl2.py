@@ -147,3 +147,24 @@ def test_iks_from_lvl2_bit_exact(engine2, oracle, keys, kind):
     got = out.cpu().numpy().view(np.uint32).reshape(B, width)
     for x, o in zip(xs, got):
         assert np.array_equal(oracle.iks(kind, x, SEED, keys), o)
+
+
+def test_pbs02_ragged_multi_pass_batch(engine2, oracle, keys):
+    """Two full passes of three ciphertexts per SM plus a ragged remainder of
+    two: every output decrypts to its input bit at +-mu."""
+    from cufhedb_b200 import testvec_const
+    import torch
+    s0, _, _ = keys
+    B = 2 * 3 * engine2.num_sms + 2
+    bits = np.random.default_rng(54).integers(0, 2, B)
+    mu0 = 1 << 29
+    x = np.stack([oracle.tlwe32(mu0 if b else (-mu0) & 0xFFFFFFFF, s0, NS_LVL0, SEED, 0x54, i)
+                  for i, b in enumerate(bits)])
+    out = torch.empty(B * (N2 + 1), dtype=torch.int64, device="cuda")
+    engine2.pbs_lvl02(_dev(x), out, testvec_const(MU2))
+    ph = torch.empty(B, dtype=torch.int64, device="cuda")
+    engine2.phase_lvl2(out, ph)
+    engine2.sync()
+    p = ph.cpu().numpy()
+    assert np.array_equal((p > 0).astype(int), bits)
+    assert np.max(np.abs(np.abs(p.astype(np.float64)) - MU2)) < 2.0 ** 56
