@@ -1,4 +1,5 @@
-"""Generates tests/golden/tfhepp_lvl1.npz from the reference's own TFHEpp.
+"""Generates tests/golden/tfhepp_lvl1.npz and tests/golden/arcedb_lvl1.npz from
+the reference's own TFHEpp.
 
 Run in a container that has the reference sources, after `make -C oracle ref`:
 
@@ -68,6 +69,30 @@ def main():
         pbs_in=pbs_in, pbs_bit=bits.astype(np.uint8), pbs_out=pbs_out)
     r.close()
     print("wrote", os.path.join(HERE, "tfhepp_lvl1.npz"))
+    arcedb(o, s1)
+
+
+# ArcEDB single-digit comparisons (src/ARCEDB/comparison/comparable.cpp
+# 506-523, 652-666, 623-633 and the equal term 537-538), run with the
+# reference's TFHEpp steps on encryptions the oracle makes deterministically
+# (comparable.h:169-179 and 228-274): inputs are stored as (x, y) and
+# regenerated, outputs as the reference computed them.
+ARC_OPS = ("gt", "lt", "eq", "equal_term")
+ARC_PAIRS = ((0, 0), (0, 1), (1, 0), (700, 699), (1023, 0), (5, 900))
+
+
+def arcedb(o, s1):
+    r = RefTFHEpp()
+    out = np.zeros((len(ARC_PAIRS), len(ARC_OPS), N1 + 1), np.uint32)
+    for i, (x, y) in enumerate(ARC_PAIRS):
+        trl = o.arc_trlwe(x, s1, SEED, 0xA5, i)
+        gfft = o.trgsw32_fft(o.arc_trgsw(y, s1, SEED, 0xA6, i))
+        for k, op in enumerate(ARC_OPS):
+            out[i, k] = r.arc_digit(op, trl, gfft)
+    r.close()
+    np.savez_compressed(os.path.join(HERE, "arcedb_lvl1.npz"), seed=np.uint64(SEED),
+                        pairs=np.array(ARC_PAIRS, np.uint32), out=out)
+    print("wrote", os.path.join(HERE, "arcedb_lvl1.npz"))
 
 
 if __name__ == "__main__":

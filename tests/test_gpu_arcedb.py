@@ -202,3 +202,23 @@ def test_polymul_lvl1_and_lvl2(engine, oracle):
         d = (got2[i].astype(object) - want) % 2 ** 64
         d = np.array([int(x) - 2 ** 64 if x >= 2 ** 63 else int(x) for x in d])
         assert np.max(np.abs(d)) < 2 ** 30
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split32"])
+def test_arc_single_digit_golden(engine, oracle, keys, precision):
+    """The GPU comparison against the reference's own outputs stored in
+    tests/golden/arcedb_lvl1.npz (inputs regenerated by the oracle)."""
+    import os
+    from cufhedb_b200 import FP64, SPLIT32
+    prec = FP64 if precision == "fp64" else SPLIT32
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "arcedb_lvl1.npz"))
+    _, s1, _ = keys
+    pairs = g["pairs"]
+    B = len(pairs)
+    trl = np.stack([oracle.arc_trlwe(int(x), s1, SEED, 0xA5, i) for i, (x, _) in enumerate(pairs)])[None]
+    gg = np.stack([oracle.arc_trgsw(int(y), s1, SEED, 0xA6, i) for i, (_, y) in enumerate(pairs)])[None]
+    tol = 1 << 12 if prec == FP64 else 1 << 23
+    for k, op in enumerate(("gt", "lt", "eq")):
+        got = _run(engine, op, trl, gg, 1, B, prec)
+        for i in range(B):
+            assert np.max(np.abs(signed_diff(got[i], g["out"][i, k]))) <= tol, (op, i)

@@ -165,3 +165,22 @@ def test_arcedb_digit_matches_reference(oracle, ref, keys):
         assert (signed_diff(oracle.phase32(strict, s1), 0) > 0) == (x < y)
         eq_term = signed_diff(oracle.phase32(ref.arc_digit("equal_term", trl, gfft), s1), 0)
         assert abs(eq_term - (1 << 29 if x == y else 0)) < 1 << 26
+
+
+def test_arcedb_golden_vectors(oracle, keys):
+    """tests/golden/arcedb_lvl1.npz: the reference's own single-digit ArcEDB
+    outputs (tests/golden/make_golden.py) on encryptions the oracle
+    regenerates deterministically; no compiled reference needed."""
+    g = np.load(os.path.join(GOLD, "arcedb_lvl1.npz"))
+    assert int(g["seed"]) == SEED
+    _, s1, _ = keys
+    ops = ("gt", "lt", "eq")
+    for i, (x, y) in enumerate(g["pairs"]):
+        trl = oracle.arc_trlwe(int(x), s1, SEED, 0xA5, i)
+        gi = oracle.arc_trgsw(int(y), s1, SEED, 0xA6, i)
+        for k, op in enumerate(ops):
+            mine = oracle.arc_single(op, trl, gi)
+            assert np.max(np.abs(signed_diff(mine, g["out"][i, k]))) <= 256, (op, x, y)
+        truth = (x > y, x <= y, x == y)
+        for k in range(3):
+            assert (signed_diff(oracle.phase32(g["out"][i, k], s1), 0) > 0) == truth[k]
