@@ -92,6 +92,8 @@ void build_tables_f(const Fft512Tables &D, Fft512TablesF &F)
         F.twist[i] = make_float2((float)D.twist[i].x, (float)D.twist[i].y);
         F.tw512p[i] = dup(D.tw512[i].x, D.tw512[i].y);
         F.untwistp[i] = dup(D.twist[i].x / 512.0, -D.twist[i].y / 512.0);
+        const double2 a = D.tw512[i], b = D.twist[i % 32];   // W^{m1 k} and w^{m1}
+        F.tw512u[i] = dup((a.x * b.x - a.y * b.y) / 512.0, (a.x * b.y + a.y * b.x) / 512.0);
     }
     for (int j = 0; j < 16; ++j) {
         F.w32[j] = make_float2((float)D.w32[j].x, (float)D.w32[j].y);

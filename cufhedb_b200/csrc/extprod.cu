@@ -93,11 +93,11 @@ __global__ void __launch_bounds__(128) extprod1_f64_kernel(ExtProdArgs a)
 __device__ __forceinline__ void store_split(uint32_t *o, CP f[16], unsigned long long *xp, int lane,
                                             const Fft512TablesF &T)
 {
-    pfft512_inv(f, xp, T, lane);
+    pfft512_inv<true>(f, xp, T, lane);
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int m = lane + 32 * m2;
-        const CP y = pmul_t(f[m2], T.untwistp[m2 * 32 + lane]);
+        const CP y = untwist_m2(f[m2], m2);
         const float2 re = unpk2(y.re), im = unpk2(y.im);
         o[m] = ((uint32_t)__float2int_rn(re.x) << 24) + (uint32_t)__float2ll_rn(re.y);
         o[m + 512] = ((uint32_t)__float2int_rn(im.x) << 24) + (uint32_t)__float2ll_rn(im.y);

@@ -17,6 +17,9 @@ struct Fft512TablesF {
     float2 w32[16];
     float4 tw512p[512];
     float4 untwistp[512];   // conj(twist) / 512: inverse untwist and scaling in one product
+    // tw512u[k * 32 + m1] = W^{m1 k} w^{m1} / 512: the inverse stage-1 twiddle
+    // (used conjugated) with the lane's part of the untwist and the 1/512 scale
+    float4 tw512u[512];
     float4 w32p[16];
 };
 
@@ -286,7 +289,12 @@ __device__ __forceinline__ void pdft16(CP v[16])
 
 // inverse transform of two polynomials at once (the sequence of ffft512_inv);
 // xp: this warp's FFT512_XP 8-byte entries, through which the real and the
-// imaginary parts are transposed one after the other
+// imaginary parts are transposed one after the other.  Output v[m2] =
+// 512 z_{lane + 32 m2} (multiply by untwistp to finish); with FOLD the stage-1
+// twiddles (tw512u) also carry conj(w^{lane}) / 512, so the output is
+// z_{lane + 32 m2} w^{32 m2}... times the rest of the twist only, which
+// untwist_m2 removes with compile-time constants instead of a table read.
+template <bool FOLD>
 __device__ __forceinline__ void pfft512_inv(CP v[16], unsigned long long *xp, const Fft512TablesF &T, int lane)
 {
     const int h = lane >> 4, q2 = lane & 15;
@@ -312,9 +320,36 @@ __device__ __forceinline__ void pfft512_inv(CP v[16], unsigned long long *xp, co
     __syncwarp();
 #pragma unroll
     for (int k = 0; k < 16; ++k) v[k].im = xp[xpf_index(lane, k)];
+    if constexpr (FOLD) {
 #pragma unroll
-    for (int k = 1; k < 16; ++k) v[k] = pmulc_t(v[k], T.tw512p[k * 32 + lane]);
+        for (int k = 0; k < 16; ++k) v[k] = pmulc_t(v[k], T.tw512u[k * 32 + lane]);
+    } else {
+#pragma unroll
+        for (int k = 1; k < 16; ++k) v[k] = pmulc_t(v[k], T.tw512p[k * 32 + lane]);
+    }
     pdft16<-1>(v);
+}
+
+// a * conj(e^{2 pi i m2 / 64}) = a * conj(w^{32 m2}): the per-register part of
+// the untwist left after pfft512_inv (compile-time constants once unrolled)
+__device__ __forceinline__ float2 untwist_m2(float2 a, int m2)
+{
+    constexpr float C[16] = {1.000000000e+00f, 9.951847267e-01f, 9.807852804e-01f, 9.569403357e-01f,
+                             9.238795325e-01f, 8.819212643e-01f, 8.314696123e-01f, 7.730104534e-01f,
+                             7.071067812e-01f, 6.343932842e-01f, 5.555702330e-01f, 4.713967368e-01f,
+                             3.826834324e-01f, 2.902846773e-01f, 1.950903220e-01f, 9.801714033e-02f};
+    if (m2 == 0) return a;
+    const float c = C[m2], sn = C[16 - m2];
+    return make_float2(fmaf(a.x, c, a.y * sn), fmaf(a.y, c, -a.x * sn));
+}
+__device__ __forceinline__ CP untwist_m2(CP a, int m2)
+{
+    constexpr float C[16] = {1.000000000e+00f, 9.951847267e-01f, 9.807852804e-01f, 9.569403357e-01f,
+                             9.238795325e-01f, 8.819212643e-01f, 8.314696123e-01f, 7.730104534e-01f,
+                             7.071067812e-01f, 6.343932842e-01f, 5.555702330e-01f, 4.713967368e-01f,
+                             3.826834324e-01f, 2.902846773e-01f, 1.950903220e-01f, 9.801714033e-02f};
+    if (m2 == 0) return a;
+    return pmulc_t(a, make_float4(C[m2], C[m2], C[16 - m2], C[16 - m2]));
 }
 
 __device__ __forceinline__ void ffft512_inv(float2 v[16], float2 *xp, const Fft512TablesF &T, int lane)
