@@ -126,6 +126,17 @@ __device__ __forceinline__ void fdft16(float2 v[16])
 // the column-wise read, with compile-time offsets from a per-lane base
 __device__ __forceinline__ int xpf_index(int m1, int q2) { return m1 * 17 + q2; }
 
+// e^{2 pi i j / 32} for j < 8 as compile-time constants once unrolled
+__device__ __forceinline__ float2 w32_const(int j)
+{
+    constexpr float C[9] = {1.000000000e+00f, 9.807852804e-01f, 9.238795325e-01f, 8.314696123e-01f,
+                            7.071067812e-01f, 5.555702330e-01f, 3.826834324e-01f, 1.950903220e-01f, 0.0f};
+    return make_float2(C[j], C[8 - j]);
+}
+
+// CONST_W32: the radix-2 step's twiddle W_32^{j + 8h} = W_32^j i^h taken from
+// compile-time constants and a select instead of a table read
+template <bool CONST_W32 = false>
 __device__ __forceinline__ void ffft512_fwd(float2 v[16], float2 *xp, const Fft512TablesF &T, int lane)
 {
     fdft16<1>(v);
@@ -145,7 +156,13 @@ __device__ __forceinline__ void ffft512_fwd(float2 v[16], float2 *xp, const Fft5
         float2 recv = shfl_xor_f2(send, 16);
         float2 a = h ? recv : v[j];
         float2 b = h ? v[8 + j] : recv;
-        float2 t = fcmul(b, T.w32[j + 8 * h]);
+        float2 t;
+        if constexpr (CONST_W32) {
+            t = j == 0 ? b : fcmul(b, w32_const(j));
+            if (h) t = make_float2(-t.y, t.x);
+        } else {
+            t = fcmul(b, T.w32[j + 8 * h]);
+        }
         v[j] = fadd2(a, t);
         v[8 + j] = fsub2(a, t);
     }

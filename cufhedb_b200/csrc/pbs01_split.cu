@@ -164,7 +164,7 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
                 if (active) {
                     float2 v[16];
                     digits_from_words_f(v, w, r % L1, lane, *T);
-                    ffft512_fwd(v, reinterpret_cast<float2 *>(xp), *T, lane);
+                    ffft512_fwd<PRODUCER>(v, reinterpret_cast<float2 *>(xp), *T, lane);
                     if (r == 0) {
 #pragma unroll
                         for (int s = 0; s < 16; ++s) {
