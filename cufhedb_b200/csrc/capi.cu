@@ -87,17 +87,21 @@ void build_tables2(Fft1024Tables &T) { build_fft8x_tables<T2>(T); }
 void build_tables_f(const Fft512Tables &D, Fft512TablesF &F)
 {
     auto dup = [](double c, double s) { return make_float4((float)c, (float)c, (float)s, (float)s); };
+    auto cx = [](double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); };
+    Fft512TablesPlain &P = F.plain;
+    Fft512TablesFold &Q = F.fold;
     for (int i = 0; i < 512; ++i) {
-        F.tw512[i] = make_float2((float)D.tw512[i].x, (float)D.tw512[i].y);
-        F.twist[i] = make_float2((float)D.twist[i].x, (float)D.twist[i].y);
-        F.tw512p[i] = dup(D.tw512[i].x, D.tw512[i].y);
-        F.untwistp[i] = dup(D.twist[i].x / 512.0, -D.twist[i].y / 512.0);
-        const double2 a = D.tw512[i], b = D.twist[i % 32];   // W^{m1 k} and w^{m1}
-        F.tw512u[i] = dup((a.x * b.x - a.y * b.y) / 512.0, (a.x * b.y + a.y * b.x) / 512.0);
+        P.tw512[i] = make_float2((float)D.tw512[i].x, (float)D.tw512[i].y);
+        P.twist[i] = make_float2((float)D.twist[i].x, (float)D.twist[i].y);
+        P.tw512p[i] = dup(D.tw512[i].x, D.tw512[i].y);
+        P.untwistp[i] = dup(D.twist[i].x / 512.0, -D.twist[i].y / 512.0);
+        const double2 t = cx(D.tw512[i], D.twist[i % 32]);   // W^{m1 q2} w^{m1}, m1 = i % 32
+        Q.tw512w[i] = make_float2((float)t.x, (float)t.y);
+        Q.tw512u[i] = dup(t.x / 512.0, t.y / 512.0);
     }
     for (int j = 0; j < 16; ++j) {
-        F.w32[j] = make_float2((float)D.w32[j].x, (float)D.w32[j].y);
-        F.w32p[j] = dup(D.w32[j].x, D.w32[j].y);
+        P.w32[j] = make_float2((float)D.w32[j].x, (float)D.w32[j].y);
+        P.w32p[j] = Q.w32p[j] = dup(D.w32[j].x, D.w32[j].y);
     }
 }
 

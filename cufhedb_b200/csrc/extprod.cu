@@ -27,7 +27,8 @@ __device__ __forceinline__ void digits_f64(double2 v[16], const uint32_t *poly, 
     }
 }
 
-__device__ __forceinline__ void digits_f32(float2 v[16], const uint32_t *poly, int d, int lane, const Fft512TablesF &T)
+__device__ __forceinline__ void digits_f32(float2 v[16], const uint32_t *poly, int d, int lane,
+                                           const Fft512TablesPlain &T)
 {
     const int sh = 32 - BGBIT1 * (d + 1);
 #pragma unroll
@@ -91,13 +92,13 @@ __global__ void __launch_bounds__(128) extprod1_f64_kernel(ExtProdArgs a)
 // o = the torus32 polynomial of the paired (hi, lo) frequency accumulator f:
 // round(hi) * 2^24 + round(lo) (mod 2^32)
 __device__ __forceinline__ void store_split(uint32_t *o, CP f[16], unsigned long long *xp, int lane,
-                                            const Fft512TablesF &T)
+                                            const Fft512TablesPlain &T)
 {
-    pfft512_inv<true>(f, xp, T, lane);
+    pfft512_inv<false>(f, xp, T, lane);
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int m = lane + 32 * m2;
-        const CP y = untwist_m2(f[m2], m2);
+        const CP y = pmul_t(f[m2], T.untwistp[m2 * 32 + lane]);
         const float2 re = unpk2(y.re), im = unpk2(y.im);
         o[m] = ((uint32_t)__float2int_rn(re.x) << 24) + (uint32_t)__float2ll_rn(re.y);
         o[m + 512] = ((uint32_t)__float2int_rn(im.x) << 24) + (uint32_t)__float2ll_rn(im.y);
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(128) extprod1_split_kernel(ExtProdArgs a)
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int p = blockIdx.x * 4 + w;
     if (p >= a.B) return;
-    const Fft512TablesF &T = *reinterpret_cast<const Fft512TablesF *>(a.tables);
+    const Fft512TablesPlain &T = reinterpret_cast<const Fft512TablesF *>(a.tables)->plain;
     const uint32_t *in = a.trlwe + (size_t)p * 2 * N1;
     const float4 *g = reinterpret_cast<const float4 *>(a.trgsw) + (a.shared ? 0 : (size_t)p * 6 * 1024);
     CP f0[16], f1[16];

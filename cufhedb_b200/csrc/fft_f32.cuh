@@ -9,19 +9,33 @@
 
 namespace cfdb {
 
-// scalar tables for the forward transform, and the inverse transform's tables
-// with each cosine and sine duplicated (c, c, s, s) for the paired form below
-struct Fft512TablesF {
+// Tables of the FP32 transforms.  The plain set: the twist, the stage-1 and
+// radix-2 twiddles as (c, s), and for the paired inverse the same with each
+// cosine and sine duplicated (c, c, s, s) plus the untwist (conj(twist) / 512).
+struct Fft512TablesPlain {
     float2 tw512[512];
     float2 twist[512];
     float2 w32[16];
     float4 tw512p[512];
     float4 untwistp[512];   // conj(twist) / 512: inverse untwist and scaling in one product
-    // tw512u[k * 32 + m1] = W^{m1 k} w^{m1} / 512: the inverse stage-1 twiddle
-    // (used conjugated) with the lane's part of the untwist and the 1/512 scale
-    float4 tw512u[512];
     float4 w32p[16];
 };
+// The folded set: the lane's part of the twist rides on the forward stage-1
+// twiddles and the lane's part of the untwist (with the 1/512 scale) on the
+// inverse stage-1 twiddles; the per-register parts are compile-time constants
+// (cw64, untwist_m2), and so are the forward radix-2 twiddles.
+struct Fft512TablesFold {
+    float2 tw512w[512];   // tw512w[q2 * 32 + m1] = W^{m1 q2} w^{m1}
+    float4 tw512u[512];   // tw512u[k * 32 + m1] = W^{m1 k} w^{m1} / 512 (used conjugated)
+    float4 w32p[16];
+};
+// both sets, as the context keeps them in global memory; a kernel copies the
+// set it uses into shared memory
+struct Fft512TablesF {
+    Fft512TablesPlain plain;
+    Fft512TablesFold fold;
+};
+static_assert(sizeof(Fft512TablesPlain) % 16 == 0 && sizeof(Fft512TablesFold) % 16 == 0, "16-byte copies");
 
 __device__ __forceinline__ unsigned long long f2_bits(float2 a)
 {
@@ -134,10 +148,8 @@ __device__ __forceinline__ float2 w32_const(int j)
     return make_float2(C[j], C[8 - j]);
 }
 
-// CONST_W32: the radix-2 step's twiddle W_32^{j + 8h} = W_32^j i^h taken from
-// compile-time constants and a select instead of a table read
-template <bool CONST_W32 = false>
-__device__ __forceinline__ void ffft512_fwd(float2 v[16], float2 *xp, const Fft512TablesF &T, int lane)
+template <class TT>
+__device__ __forceinline__ void ffft512_fwd(float2 v[16], float2 *xp, const TT &T, int lane)
 {
     fdft16<1>(v);
 #pragma unroll
@@ -156,13 +168,50 @@ __device__ __forceinline__ void ffft512_fwd(float2 v[16], float2 *xp, const Fft5
         float2 recv = shfl_xor_f2(send, 16);
         float2 a = h ? recv : v[j];
         float2 b = h ? v[8 + j] : recv;
-        float2 t;
-        if constexpr (CONST_W32) {
-            t = j == 0 ? b : fcmul(b, w32_const(j));
-            if (h) t = make_float2(-t.y, t.x);
-        } else {
-            t = fcmul(b, T.w32[j + 8 * h]);
-        }
+        float2 t = fcmul(b, T.w32[j + 8 * h]);
+        v[j] = fadd2(a, t);
+        v[8 + j] = fsub2(a, t);
+    }
+}
+
+// a * e^{2 pi i m2 / 64} = a * w^{32 m2} (compile-time constants once unrolled)
+__device__ __forceinline__ float2 cw64(float2 a, int m2)
+{
+    constexpr float C[17] = {1.000000000e+00f, 9.951847267e-01f, 9.807852804e-01f, 9.569403357e-01f,
+                             9.238795325e-01f, 8.819212643e-01f, 8.314696123e-01f, 7.730104534e-01f,
+                             7.071067812e-01f, 6.343932842e-01f, 5.555702330e-01f, 4.713967368e-01f,
+                             3.826834324e-01f, 2.902846773e-01f, 1.950903220e-01f, 9.801714033e-02f, 0.0f};
+    if (m2 == 0) return a;
+    const float c = C[m2], sn = C[16 - m2];
+    return make_float2(fmaf(a.x, c, -a.y * sn), fmaf(a.x, sn, a.y * c));
+}
+
+// forward transform of inputs that carry only the per-register part of the
+// twist, v[m2] = (a_m + i a_{m+512}) w^{32 m2} (cw64): the lane's part w^{lane}
+// is applied with the stage-1 twiddles (tw512w, q2 = 0 included), the radix-2
+// twiddles come from constants.  Same output as ffft512_fwd on fully twisted
+// inputs.
+__device__ __forceinline__ void ffft512_fwd_tw(float2 v[16], float2 *xp, const Fft512TablesFold &T, int lane)
+{
+    fdft16<1>(v);
+#pragma unroll
+    for (int q2 = 0; q2 < 16; ++q2) v[q2] = fcmul(v[q2], T.tw512w[q2 * 32 + lane]);
+    __syncwarp();
+#pragma unroll
+    for (int q2 = 0; q2 < 16; ++q2) xp[xpf_index(lane, q2)] = v[q2];
+    __syncwarp();
+    const int h = lane >> 4, q2 = lane & 15;
+#pragma unroll
+    for (int m1p = 0; m1p < 16; ++m1p) v[m1p] = xp[xpf_index(2 * m1p + h, q2)];
+    fdft16<1>(v);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        float2 send = h ? v[j] : v[8 + j];
+        float2 recv = shfl_xor_f2(send, 16);
+        float2 a = h ? recv : v[j];
+        float2 b = h ? v[8 + j] : recv;
+        float2 t = j == 0 ? b : fcmul(b, w32_const(j));
+        if (h) t = make_float2(-t.y, t.x);
         v[j] = fadd2(a, t);
         v[8 + j] = fsub2(a, t);
     }
@@ -304,15 +353,16 @@ __device__ __forceinline__ void pdft16(CP v[16])
     for (int i = 0; i < 16; ++i) v[i] = t[i];
 }
 
-// inverse transform of two polynomials at once (the sequence of ffft512_inv);
+// inverse transform of two polynomials at once (the forward steps in reverse
+// with conjugate twiddles);
 // xp: this warp's FFT512_XP 8-byte entries, through which the real and the
 // imaginary parts are transposed one after the other.  Output v[m2] =
 // 512 z_{lane + 32 m2} (multiply by untwistp to finish); with FOLD the stage-1
 // twiddles (tw512u) also carry conj(w^{lane}) / 512, so the output is
 // z_{lane + 32 m2} w^{32 m2}... times the rest of the twist only, which
 // untwist_m2 removes with compile-time constants instead of a table read.
-template <bool FOLD>
-__device__ __forceinline__ void pfft512_inv(CP v[16], unsigned long long *xp, const Fft512TablesF &T, int lane)
+template <bool FOLD, class TT>
+__device__ __forceinline__ void pfft512_inv(CP v[16], unsigned long long *xp, const TT &T, int lane)
 {
     const int h = lane >> 4, q2 = lane & 15;
 #pragma unroll
@@ -369,29 +419,5 @@ __device__ __forceinline__ CP untwist_m2(CP a, int m2)
     return pmulc_t(a, make_float4(C[m2], C[m2], C[16 - m2], C[16 - m2]));
 }
 
-__device__ __forceinline__ void ffft512_inv(float2 v[16], float2 *xp, const Fft512TablesF &T, int lane)
-{
-    const int h = lane >> 4, q2 = lane & 15;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        float2 a = v[j], b = v[8 + j];
-        float2 g0 = fadd2(a, b);
-        float2 g1 = fcmulc(fsub2(a, b), T.w32[j + 8 * h]);
-        float2 send = h ? g0 : g1;
-        float2 recv = shfl_xor_f2(send, 16);
-        v[j] = h ? recv : g0;
-        v[8 + j] = h ? g1 : recv;
-    }
-    fdft16<-1>(v);
-    __syncwarp();
-#pragma unroll
-    for (int m1p = 0; m1p < 16; ++m1p) xp[xpf_index(2 * m1p + h, q2)] = v[m1p];
-    __syncwarp();
-#pragma unroll
-    for (int k = 0; k < 16; ++k) v[k] = xp[xpf_index(lane, k)];
-#pragma unroll
-    for (int k = 1; k < 16; ++k) v[k] = fcmulc(v[k], T.tw512[k * 32 + lane]);
-    fdft16<-1>(v);
-}
 
 }  // namespace cfdb

@@ -28,12 +28,12 @@
 
 namespace cfdb {
 
-template <int W, int S>
+template <int W, int S, int TBYTES>
 struct Pbs01SplitSmem {
     static constexpr int RING_OFF = RING_HEADER_BYTES;
     static constexpr int CHUNK_BYTES = 16384;   // 16 slots x 2 outputs x 32 lanes x float4(hi, lo)
     static constexpr int TAB_OFF = RING_OFF + S * CHUNK_BYTES;
-    static constexpr int WARP_OFF = TAB_OFF + ((int)sizeof(Fft512TablesF) + 127) / 128 * 128;
+    static constexpr int WARP_OFF = TAB_OFF + (TBYTES + 127) / 128 * 128;
     static constexpr int XP_BYTES = FFT512_XP * 8;
     static constexpr int ACC_BYTES = 2 * N1 * 4;
     static constexpr int ABAR_BYTES = ((N0 * 2) + 127) / 128 * 128;
@@ -54,14 +54,18 @@ __device__ __forceinline__ void digit_words1(uint32_t w[32], const uint32_t *pol
     }
 }
 
-// v[m2] = (dig_d(m) + i dig_d(m+512)) * w^m from the cached words
+// v[m2] = (dig_d(m) + i dig_d(m+512)) * w^m from the cached words; with FOLD
+// only the per-register part w^{32 m2} (the transform applies w^{lane})
+template <bool FOLD, class TT>
 __device__ __forceinline__ void digits_from_words_f(float2 v[16], const uint32_t w[32], int d, int lane,
-                                                    const Fft512TablesF &T)
+                                                    const TT &T)
 {
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int d0 = digit_field1(w[2 * m2], d), d1 = digit_field1(w[2 * m2 + 1], d);
-        v[m2] = fcmul(make_float2((float)d0, (float)d1), T.twist[m2 * 32 + lane]);
+        const float2 x = make_float2((float)d0, (float)d1);
+        if constexpr (FOLD) v[m2] = cw64(x, m2);
+        else v[m2] = fcmul(x, T.twist[m2 * 32 + lane]);
     }
 }
 
@@ -70,15 +74,17 @@ __device__ __forceinline__ void digits_from_words_f(float2 v[16], const uint32_t
 // output as pairs, inverse-transformed together.  The hi limb's products
 // round exactly; the lo limb's FP32 error stays far below the bootstrapping
 // noise.
-template <bool FOLD>
+template <bool FOLD, class TT>
 __device__ __forceinline__ void add_inverse_split(uint32_t *poly, CP f[16], unsigned long long *xp, int lane,
-                                                  const Fft512TablesF &T)
+                                                  const TT &T)
 {
     pfft512_inv<FOLD>(f, xp, T, lane);
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int m = lane + 32 * m2;
-        const CP y = FOLD ? untwist_m2(f[m2], m2) : pmul_t(f[m2], T.untwistp[m2 * 32 + lane]);
+        CP y;
+        if constexpr (FOLD) y = untwist_m2(f[m2], m2);
+        else y = pmul_t(f[m2], T.untwistp[m2 * 32 + lane]);
         const float2 re = unpk2(y.re), im = unpk2(y.im);   // (hi, lo) of coefficients m and m + 512
         poly[m] += ((uint32_t)__float2int_rn(re.x) << 24) + (uint32_t)__float2ll_rn(re.y);
         poly[m + 512] += ((uint32_t)__float2int_rn(im.x) << 24) + (uint32_t)__float2ll_rn(im.y);
@@ -105,9 +111,12 @@ __device__ __forceinline__ CP pmul_first(unsigned long long vr, unsigned long lo
 template <int W, int S, bool PRODUCER>
 __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_kernel(Pbs01Args a)
 {
-    using L = Pbs01SplitSmem<W, S>;
+    // the 7-per-CTA shape (with the producer warp) uses the folded tables
+    constexpr bool FOLD = PRODUCER;
+    using TT = std::conditional_t<FOLD, Fft512TablesFold, Fft512TablesPlain>;
+    using L = Pbs01SplitSmem<W, S, (int)sizeof(TT)>;
     extern __shared__ __align__(128) unsigned char smem[];
-    Fft512TablesF *T = reinterpret_cast<Fft512TablesF *>(smem + L::TAB_OFF);
+    TT *T = reinterpret_cast<TT *>(smem + L::TAB_OFF);
     const int ngroups = (a.B + W - 1) / W;
     constexpr int CHUNKS = N0 * 2 * L1;
     using Feed = std::conditional_t<PRODUCER, ProducerRing<S, L::CHUNK_BYTES, W>, KeyRing<S, L::CHUNK_BYTES, W>>;
@@ -117,9 +126,10 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) ring.init_by_thread0();
     {
-        const float4 *src = reinterpret_cast<const float4 *>(a.tables);
+        const Fft512TablesF *all = reinterpret_cast<const Fft512TablesF *>(a.tables);
+        const float4 *src = reinterpret_cast<const float4 *>(FOLD ? (const void *)&all->fold : (const void *)&all->plain);
         float4 *dst = reinterpret_cast<float4 *>(T);
-        for (int i = threadIdx.x; i < (int)(sizeof(Fft512TablesF) / 16); i += blockDim.x) dst[i] = src[i];
+        for (int i = threadIdx.x; i < (int)(sizeof(TT) / 16); i += blockDim.x) dst[i] = src[i];
     }
     __syncthreads();
     if constexpr (PRODUCER) {
@@ -163,8 +173,9 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
                 const float4 *bkc = reinterpret_cast<const float4 *>(ring.acquire(c, a.err));
                 if (active) {
                     float2 v[16];
-                    digits_from_words_f(v, w, r % L1, lane, *T);
-                    ffft512_fwd<PRODUCER>(v, reinterpret_cast<float2 *>(xp), *T, lane);
+                    digits_from_words_f<FOLD>(v, w, r % L1, lane, *T);
+                    if constexpr (FOLD) ffft512_fwd_tw(v, reinterpret_cast<float2 *>(xp), *T, lane);
+                    else ffft512_fwd(v, reinterpret_cast<float2 *>(xp), *T, lane);
                     if (r == 0) {
 #pragma unroll
                         for (int s = 0; s < 16; ++s) {
@@ -188,11 +199,8 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
                 ring.release(c, lane);
             }
             if (active) {
-                // the folded untwist measured faster with the producer-warp
-                // shape (7 per CTA: 10.47 -> 10.12 ms per 1,024) and slower
-                // without it (8 per CTA: 11.10 -> 11.27 ms per 1,184)
-                add_inverse_split<PRODUCER>(acc, f0, xp, lane, *T);
-                add_inverse_split<PRODUCER>(acc + N1, f1, xp, lane, *T);
+                add_inverse_split<FOLD>(acc, f0, xp, lane, *T);
+                add_inverse_split<FOLD>(acc + N1, f1, xp, lane, *T);
                 __syncwarp();
             }
         }
@@ -209,9 +217,15 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
     }
 }
 
-// key-ring depth: 6 slots with 7 ciphertexts per CTA, 5 with 8 (shared memory)
+// key-ring depth: 7 slots with 7 ciphertexts per CTA (more than one CMux of
+// key rows in flight), 5 with 8 (shared memory)
 template <int W>
-constexpr int PBS01S_S = W == 7 ? 6 : 5;
+constexpr int PBS01S_S = W == 7 ? 7 : 5;
+
+// shared-memory layout of each shape: 7 per CTA keeps the folded tables, 8 the
+// plain ones
+template <int W>
+using SplitLayout = Pbs01SplitSmem<W, PBS01S_S<W>, (int)(W == 7 ? sizeof(Fft512TablesFold) : sizeof(Fft512TablesPlain))>;
 
 // 7 ciphertexts per CTA run with a producer warp (8 warps), 8 per CTA without
 // one (8 warps): both keep 2 warps per SM sub-partition (up to 255 registers)
@@ -219,7 +233,7 @@ template <int W>
 static cudaError_t launch_pbs01_split_t(const Pbs01Args &a, int grid, cudaStream_t st)
 {
     constexpr bool PROD = W == 7;
-    using L = Pbs01SplitSmem<W, PBS01S_S<W>>;
+    using L = SplitLayout<W>;
     static_assert(L::TOTAL <= 227 * 1024, "shared memory budget");
     pbs01_split_kernel<W, PBS01S_S<W>, PROD><<<grid, (W + (PROD ? 1 : 0)) * 32, L::TOTAL, st>>>(a);
     return cudaGetLastError();
@@ -237,10 +251,10 @@ cudaError_t init_pbs01_split()
 {
     cudaError_t e = cudaFuncSetAttribute(pbs01_split_kernel<7, PBS01S_S<7>, true>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         Pbs01SplitSmem<7, PBS01S_S<7>>::TOTAL);
+                                         SplitLayout<7>::TOTAL);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(pbs01_split_kernel<8, PBS01S_S<8>, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                Pbs01SplitSmem<8, PBS01S_S<8>>::TOTAL);
+                                SplitLayout<8>::TOTAL);
 }
 
 }  // namespace cfdb
