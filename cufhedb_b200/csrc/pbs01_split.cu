@@ -54,18 +54,14 @@ __device__ __forceinline__ void digit_words1(uint32_t w[32], const uint32_t *pol
     }
 }
 
-// v[m2] = (dig_d(m) + i dig_d(m+512)) * w^m from the cached words; with FOLD
-// only the per-register part w^{32 m2} (the transform applies w^{lane})
-template <bool FOLD, class TT>
-__device__ __forceinline__ void digits_from_words_f(float2 v[16], const uint32_t w[32], int d, int lane,
-                                                    const TT &T)
+// v[m2] = (dig_d(m) + i dig_d(m+512)) * w^{32 m2} from the cached words: the
+// per-register part of the twist (ffft512_fwd_tw applies the lane's part)
+__device__ __forceinline__ void digits_from_words_f(float2 v[16], const uint32_t w[32], int d)
 {
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int d0 = digit_field1(w[2 * m2], d), d1 = digit_field1(w[2 * m2 + 1], d);
-        const float2 x = make_float2((float)d0, (float)d1);
-        if constexpr (FOLD) v[m2] = cw64(x, m2);
-        else v[m2] = fcmul(x, T.twist[m2 * 32 + lane]);
+        v[m2] = cw64(make_float2((float)d0, (float)d1), m2);
     }
 }
 
@@ -74,17 +70,14 @@ __device__ __forceinline__ void digits_from_words_f(float2 v[16], const uint32_t
 // output as pairs, inverse-transformed together.  The hi limb's products
 // round exactly; the lo limb's FP32 error stays far below the bootstrapping
 // noise.
-template <bool FOLD, class TT>
 __device__ __forceinline__ void add_inverse_split(uint32_t *poly, CP f[16], unsigned long long *xp, int lane,
-                                                  const TT &T)
+                                                  const Fft512TablesFold &T)
 {
-    pfft512_inv<FOLD>(f, xp, T, lane);
+    pfft512_inv<true>(f, xp, T, lane);
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int m = lane + 32 * m2;
-        CP y;
-        if constexpr (FOLD) y = untwist_m2(f[m2], m2);
-        else y = pmul_t(f[m2], T.untwistp[m2 * 32 + lane]);
+        const CP y = untwist_m2(f[m2], m2);
         const float2 re = unpk2(y.re), im = unpk2(y.im);   // (hi, lo) of coefficients m and m + 512
         poly[m] += ((uint32_t)__float2int_rn(re.x) << 24) + (uint32_t)__float2ll_rn(re.y);
         poly[m + 512] += ((uint32_t)__float2int_rn(im.x) << 24) + (uint32_t)__float2ll_rn(im.y);
@@ -111,9 +104,9 @@ __device__ __forceinline__ CP pmul_first(unsigned long long vr, unsigned long lo
 template <int W, int S, bool PRODUCER>
 __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_kernel(Pbs01Args a)
 {
-    // the 7-per-CTA shape (with the producer warp) uses the folded tables
-    constexpr bool FOLD = PRODUCER;
-    using TT = std::conditional_t<FOLD, Fft512TablesFold, Fft512TablesPlain>;
+    // the folded tables (fft_f32.cuh): the twist and untwist ride on the
+    // stage-1 twiddles, so the kernel reads 12.3 KB of tables instead of 24.4
+    using TT = Fft512TablesFold;
     using L = Pbs01SplitSmem<W, S, (int)sizeof(TT)>;
     extern __shared__ __align__(128) unsigned char smem[];
     TT *T = reinterpret_cast<TT *>(smem + L::TAB_OFF);
@@ -127,7 +120,7 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
     if (threadIdx.x == 0) ring.init_by_thread0();
     {
         const Fft512TablesF *all = reinterpret_cast<const Fft512TablesF *>(a.tables);
-        const float4 *src = reinterpret_cast<const float4 *>(FOLD ? (const void *)&all->fold : (const void *)&all->plain);
+        const float4 *src = reinterpret_cast<const float4 *>(&all->fold);
         float4 *dst = reinterpret_cast<float4 *>(T);
         for (int i = threadIdx.x; i < (int)(sizeof(TT) / 16); i += blockDim.x) dst[i] = src[i];
     }
@@ -173,9 +166,8 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
                 const float4 *bkc = reinterpret_cast<const float4 *>(ring.acquire(c, a.err));
                 if (active) {
                     float2 v[16];
-                    digits_from_words_f<FOLD>(v, w, r % L1, lane, *T);
-                    if constexpr (FOLD) ffft512_fwd_tw(v, reinterpret_cast<float2 *>(xp), *T, lane);
-                    else ffft512_fwd(v, reinterpret_cast<float2 *>(xp), *T, lane);
+                    digits_from_words_f(v, w, r % L1);
+                    ffft512_fwd_tw(v, reinterpret_cast<float2 *>(xp), *T, lane);
                     if (r == 0) {
 #pragma unroll
                         for (int s = 0; s < 16; ++s) {
@@ -199,8 +191,8 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
                 ring.release(c, lane);
             }
             if (active) {
-                add_inverse_split<FOLD>(acc, f0, xp, lane, *T);
-                add_inverse_split<FOLD>(acc + N1, f1, xp, lane, *T);
+                add_inverse_split(acc, f0, xp, lane, *T);
+                add_inverse_split(acc + N1, f1, xp, lane, *T);
                 __syncwarp();
             }
         }
@@ -218,14 +210,12 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
 }
 
 // key-ring depth: 7 slots with 7 ciphertexts per CTA (more than one CMux of
-// key rows in flight), 5 with 8 (shared memory)
+// key rows in flight), 6 with 8 (shared memory)
 template <int W>
-constexpr int PBS01S_S = W == 7 ? 7 : 5;
+constexpr int PBS01S_S = W == 7 ? 7 : 6;
 
-// shared-memory layout of each shape: 7 per CTA keeps the folded tables, 8 the
-// plain ones
 template <int W>
-using SplitLayout = Pbs01SplitSmem<W, PBS01S_S<W>, (int)(W == 7 ? sizeof(Fft512TablesFold) : sizeof(Fft512TablesPlain))>;
+using SplitLayout = Pbs01SplitSmem<W, PBS01S_S<W>, (int)sizeof(Fft512TablesFold)>;
 
 // 7 ciphertexts per CTA run with a producer warp (8 warps), 8 per CTA without
 // one (8 warps): both keep 2 warps per SM sub-partition (up to 255 registers)
