@@ -54,3 +54,31 @@ def test_no_cpu_fallback():
     from cufhedb_b200 import CufhedbError, Engine
     with pytest.raises(CufhedbError):
         Engine(0)
+
+
+def test_every_context_entry_point_rejects_a_null_context():
+    """Every entry point that takes a context validates it before anything
+    else: with a null context (and every other argument null or 1, so that no
+    empty-batch shortcut applies) it returns CUFHEDB_ERR_ARG with a message and
+    touches no device."""
+    from cufhedb_b200 import _lib
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    lib.cufhedb_last_error.restype = ctypes.c_char_p
+    checked = 0
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        txt = open(h).read()
+        for name, args in re.findall(r"CUFHEDB_API\s+int\s+(cufhedb_\w+)\s*\(([^)]*)\)", txt):
+            params = [a.strip() for a in args.split(",")]
+            if not params[0].startswith("cufhedb_ctx *") or name in ("cufhedb_ctx_destroy",):
+                continue
+            call = []
+            for p in params[1:]:
+                call.append(None if "*" in p else 1)
+            f = getattr(lib, name)
+            f.restype = ctypes.c_int
+            f.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p if a is None else ctypes.c_uint64 for a in call]
+            rc = f(None, *call)
+            assert rc == _lib.ERR_ARG, (name, rc)
+            assert lib.cufhedb_last_error(), name
+            checked += 1
+    assert checked >= 40
