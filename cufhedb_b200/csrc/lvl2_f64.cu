@@ -26,10 +26,12 @@ namespace {
 
 constexpr uint64_t DEC2_XOR = (256ull << 55) | (256ull << 46) | (256ull << 37) | (256ull << 28);
 
-// signed 9-bit field d (0 = most significant) of x, sign-extended by two shifts
-__device__ __forceinline__ long long digit_field2(uint64_t x, int d)
+// signed 9-bit field d (0 = most significant) of x, sign-extended by two
+// shifts; the field lies in the top word after the first, so the second
+// shift and the conversion to double work on 32 bits
+__device__ __forceinline__ int digit_field2(uint64_t x, int d)
 {
-    return (long long)(x << (BGBIT2 * d)) >> (64 - BGBIT2);
+    return (int)((x << (BGBIT2 * d)) >> 32) >> (32 - BGBIT2);
 }
 
 // digit-extraction words of (X^a - 1) * poly (or of poly when ROT is false)
