@@ -1,7 +1,5 @@
-// Negacyclic FFT of M = 8 T complex points spread over T threads (8 values
-// per thread), FP64 (double2) or FP32 (float2).  Used with T = 128 for the
-// lvl2 ring (N = 2048, M = 1024: four warps per polynomial) and T = 64 for
-// the lvl1 ring (N = 1024, M = 512: two warps per polynomial).
+// Negacyclic FFT of M = 1024 complex points spread over T = 128 threads (8
+// values per thread, four warps), FP64: the lvl2 ring (N = 2048).
 //
 // Transform (TFHEpp TwistIFFT / TwistFFT, thirdparty/TFHEpp/include/
 // mulfft.hpp:57-121, spqlios layout restated in oracle/tfhe_oracle.c):
@@ -9,21 +7,23 @@
 //            W_P = exp(2 pi i / P), w = exp(2 pi i / 4M)
 //   inverse  M z_m = sum_q V(q) W_M^{-mq}
 //
-// Factorisation (L = T / 8 lanes per group):
+// Factorisation M = 8 x 8 x 16 (L = 16 lanes per group):
 //   A. thread t holds z_{t + T j}, j < 8: 8-point DFT over j in registers
 //      (output k), twiddle W_M^{t k};
-//   B. one shared-memory transpose: thread u = a + L k (a < L) receives the
-//      values of threads t = a + L b, b < 8, for its k; 8-point DFT over b
-//      (output q1), twiddle W_T^{a q1};
-//   C. L-point DFT over a across the L lanes of each group: log2(L) radix-2
-//      decimation-in-frequency steps through warp shuffles.  In step i
-//      (lane bit h = L >> (i+1), register bit beta_i = 4 >> (i mod 3)) each
-//      thread trades the half of its registers selected by beta_i with lane
-//      u ^ h and then owns both inputs of 4 butterflies.
+//   B. shared-memory transpose across the four warps: thread u = a + L k
+//      (a < L) receives the values of threads t = a + L b, b < 8, for its k;
+//      8-point DFT over b (output q1), twiddle W_T^{a q1};
+//   C. the 16-point DFT over a, as 2 x 8: a second transpose, inside each warp
+//      (the 16 values of a (k, q1) sit in the 16 lanes of one warp with that
+//      k), gives thread u' = q1 + 8 a0 + 16 k the values a = a0 + 2 j, j < 8;
+//      an 8-point DFT over j in registers (output r); then one radix-2 step
+//      with the partner lane u' ^ 8 (the other a0): the pair trades half of
+//      its registers, and thread a0 keeps r = rl + 4 a0, rl < 4, computing
+//      Y0[r] +- W_16^r Y1[r] for q2 = r and r + 8.
 // The frequency q = k + 8 (q1 + 8 q2) then sits in register slot s of thread
-// u as given by fft8x_freq() below; the bootstrapping key is stored in the
-// same [s][u] order, so the per-frequency products need no data exchange and
-// the inverse transform (the same steps in reverse) starts from the same
+// u' as given by fft8x_freq() below; the bootstrapping key is stored in the
+// same [s][u'] order, so the per-frequency products need no data exchange
+// and the inverse transform (the same steps in reverse) starts from the same
 // registers.
 #pragma once
 #include "common.cuh"
@@ -189,13 +189,13 @@ __device__ __forceinline__ C cx_w32(C a, int j)
 // ---- tables ---------------------------------------------------------------------
 //   twA[k T + t]   = w^t W_M^{t k}        (M entries, k < 8: stage A twiddle with the twist's w^t)
 //   twB[q1 L + a]  = W_T^{a q1}           (8 L = T entries)
-//   wC[j]          = W_L^j, j < L / 2
+// (stage C's twiddles W_16^r, r < 8, are compile-time constants)
 template <typename C, int T>
 struct Fft8xTables {
+    static_assert(T == 128, "the transform is written for 128 threads (M = 1024)");
     static constexpr int M = 8 * T, L = T / 8;
     C twA[M];
     C twB[T];
-    C wC[L / 2];
 };
 
 // host: the FP64 tables, computed in long double
@@ -212,39 +212,16 @@ inline void build_fft8x_tables(Fft8xTables<double2, T> &tab)
         for (int t = 0; t < T; ++t) tab.twA[k * T + t] = cis((long long)t * (1 + 4 * k) % (4 * M), 4 * M);
     for (int q1 = 0; q1 < 8; ++q1)
         for (int a = 0; a < L; ++a) tab.twB[q1 * L + a] = cis((long long)(a * q1) % T, T);
-    for (int j = 0; j < L / 2; ++j) tab.wC[j] = cis(j, L);
 }
 
-__host__ __device__ constexpr int ilog2c(int x) { return x <= 1 ? 0 : 1 + ilog2c(x >> 1); }
-
-// frequency held in register slot s of thread u after the forward transform
+// frequency held in register slot s of thread u after the forward transform:
+// u = q1 + 8 a0 + 16 k, s = rl + 4 e, q2 = rl + 4 a0 + 8 e
 template <int T>
 __host__ __device__ __forceinline__ int fft8x_freq(int u, int s)
 {
-    constexpr int L = T / 8, NST = ilog2c(L);
-    const int a = u % L, k = u / L;
-    // meaning of each register bit / lane bit: (is_q2, bit position)
-    int slot_kind[3] = {0, 0, 0}, slot_pos[3] = {0, 1, 2};
-    int lane_kind[4] = {0, 0, 0, 0}, lane_pos[4] = {0, 0, 0, 0};
-    for (int i = 0; i < NST; ++i) {
-        const int hb = NST - 1 - i;               // lane bit index of h = L >> (i+1)
-        const int rb = 2 - (i % 3);               // register bit index of beta = 4 >> (i mod 3)
-        lane_kind[hb] = slot_kind[rb];
-        lane_pos[hb] = slot_pos[rb];
-        slot_kind[rb] = 1;
-        slot_pos[rb] = i;
-    }
-    int q1 = 0, q2 = 0;
-    for (int b = 0; b < 3; ++b)
-        if (s & (1 << b)) {
-            if (slot_kind[b]) q2 |= 1 << slot_pos[b];
-            else q1 |= 1 << slot_pos[b];
-        }
-    for (int b = 0; b < NST; ++b)
-        if (a & (1 << b)) {
-            if (lane_kind[b]) q2 |= 1 << lane_pos[b];
-            else q1 |= 1 << lane_pos[b];
-        }
+    static_assert(T == 128, "the transform is written for 128 threads (M = 1024)");
+    const int q1 = u & 7, a0 = (u >> 3) & 1, k = u >> 4;
+    const int q2 = (s & 3) + 4 * a0 + 8 * (s >> 2);
     return k + 8 * (q1 + 8 * q2);
 }
 
@@ -269,17 +246,23 @@ __device__ __forceinline__ int fft8x_xp(int t, int k)
     return t * 9 + k;
 }
 
+// Scratch discipline: both transforms end by reading only rows of xp that
+// belong to the reading thread's own warp, and each starts by writing only
+// such rows, so a __syncwarp() orders one transform after the previous one;
+// the writes into other warps' rows (and the reads after them) are fenced by
+// the group's named barrier.
+
 // forward: v[j] = z_{t + T j} / w^t in (the inputs multiplied by W_32^j only),
 // v[s] = V(fft8x_freq<T>(t, s)) out.  xp: FFT8X_XP<T>-entry scratch shared
 // by the group; bar: its named barrier.
 template <typename C, int T>
 __device__ __forceinline__ void fft8x_fwd(C v[8], C *xp, const Fft8xTables<C, T> &tab, int t, int bar)
 {
-    constexpr int L = T / 8, NST = ilog2c(L);
+    constexpr int L = T / 8;
     cx_dft8<1>(v);
 #pragma unroll
     for (int k = 0; k < 8; ++k) v[k] = cx_mul(v[k], tab.twA[k * T + t]);
-    group_sync<T>(bar);
+    __syncwarp();
 #pragma unroll
     for (int k = 0; k < 8; ++k) xp[fft8x_xp<C>(t, k)] = v[k];
     group_sync<T>(bar);
@@ -289,21 +272,25 @@ __device__ __forceinline__ void fft8x_fwd(C v[8], C *xp, const Fft8xTables<C, T>
     cx_dft8<1>(v);
 #pragma unroll
     for (int q1 = 1; q1 < 8; ++q1) v[q1] = cx_mul(v[q1], tab.twB[q1 * L + a]);
+    // C: the second transpose stays inside the warp (rows t of this warp),
+    // but other warps may still be reading these rows from the first one
+    group_sync<T>(bar);
 #pragma unroll
-    for (int i = 0; i < NST; ++i) {
-        const int h = L >> (i + 1), beta = 4 >> (i % 3);
-        const bool hi_lane = (a & h) != 0;
-        const C tw = tab.wC[(a & (h - 1)) * (L / (2 * h))];
+    for (int q1 = 0; q1 < 8; ++q1) xp[fft8x_xp<C>(t, q1)] = v[q1];
+    __syncwarp();
+    const int q1p = t & 7, a0 = (t >> 3) & 1, kp = t >> 4;
 #pragma unroll
-        for (int s = 0; s < 8; ++s) {
-            if (s & beta) continue;
-            const C send = hi_lane ? v[s] : v[s | beta];
-            const C recv = cx_shfl_xor(send, h);
-            const C lo = hi_lane ? recv : v[s];
-            const C hi = hi_lane ? v[s | beta] : recv;
-            v[s] = cx_add(lo, hi);
-            v[s | beta] = cx_mul(cx_sub(lo, hi), tw);
-        }
+    for (int j = 0; j < 8; ++j) v[j] = xp[fft8x_xp<C>(a0 + 2 * j + L * kp, q1p)];
+    cx_dft8<1>(v);
+#pragma unroll
+    for (int rl = 0; rl < 4; ++rl) {
+        const C send = a0 ? v[rl] : v[rl + 4];
+        const C recv = cx_shfl_xor(send, 8);
+        const C p = a0 ? recv : v[rl];
+        C q = cx_w32<1>(a0 ? v[rl + 4] : recv, 2 * rl);   // W_16^rl
+        if (a0) q = cx_mul_i<1>(q);                        // W_16^4 = i
+        v[rl] = cx_add(p, q);
+        v[rl + 4] = cx_sub(p, q);
     }
 }
 
@@ -312,24 +299,28 @@ __device__ __forceinline__ void fft8x_fwd(C v[8], C *xp, const Fft8xTables<C, T>
 template <typename C, int T>
 __device__ __forceinline__ void fft8x_inv(C v[8], C *xp, const Fft8xTables<C, T> &tab, int t, int bar)
 {
-    constexpr int L = T / 8, NST = ilog2c(L);
+    constexpr int L = T / 8;
     const int a = t % L, k = t / L;
+    const int q1p = t & 7, a0 = (t >> 3) & 1, kp = t >> 4;
+    // C inverse: the radix-2 step (2 Y0[r], 2 W_16^r Y1[r] from X[r] +- X[r + 8]),
+    // the pair's trade back, the 8-point inverse DFT over r, the transpose
+    // back inside the warp
 #pragma unroll
-    for (int i = NST - 1; i >= 0; --i) {
-        const int h = L >> (i + 1), beta = 4 >> (i % 3);
-        const bool hi_lane = (a & h) != 0;
-        const C tw = tab.wC[(a & (h - 1)) * (L / (2 * h))];
-#pragma unroll
-        for (int s = 0; s < 8; ++s) {
-            if (s & beta) continue;
-            const C y0 = v[s], y1 = cx_mulc(v[s | beta], tw);
-            const C lo = cx_add(y0, y1), hi = cx_sub(y0, y1);
-            const C send = hi_lane ? lo : hi;
-            const C recv = cx_shfl_xor(send, h);
-            v[s] = hi_lane ? recv : lo;
-            v[s | beta] = hi_lane ? hi : recv;
-        }
+    for (int rl = 0; rl < 4; ++rl) {
+        const C p = cx_add(v[rl], v[rl + 4]);
+        C q = cx_w32<-1>(cx_sub(v[rl], v[rl + 4]), 2 * rl);   // conj(W_16^rl)
+        if (a0) q = cx_mul_i<-1>(q);                           // conj(W_16^4) = -i
+        const C recv = cx_shfl_xor(a0 ? p : q, 8);
+        v[rl] = a0 ? recv : p;
+        v[rl + 4] = a0 ? q : recv;
     }
+    cx_dft8<-1>(v);
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 8; ++j) xp[fft8x_xp<C>(a0 + 2 * j + L * kp, q1p)] = v[j];
+    __syncwarp();
+#pragma unroll
+    for (int q1 = 0; q1 < 8; ++q1) v[q1] = xp[fft8x_xp<C>(t, q1)];
 #pragma unroll
     for (int q1 = 1; q1 < 8; ++q1) v[q1] = cx_mulc(v[q1], tab.twB[q1 * L + a]);
     cx_dft8<-1>(v);
