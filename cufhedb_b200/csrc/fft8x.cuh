@@ -187,15 +187,20 @@ __device__ __forceinline__ C cx_w32(C a, int j)
 }
 
 // ---- tables ---------------------------------------------------------------------
-//   twA[k T + t]   = w^t W_M^{t k}        (M entries, k < 8: stage A twiddle with the twist's w^t)
-//   twB[q1 L + a]  = W_T^{a q1}           (8 L = T entries)
+// Each thread's twiddles are powers of one step, so the tables hold the
+// steps and the transforms form the powers by repeated multiplication (FP64:
+// seven products add a few ulp, far inside the transform's error; the
+// shared-memory reads they replace were a fifth of the kernel's traffic):
+//   twA0[t] = w^t, twAs[t] = W_M^t     stage A twiddle w^t W_M^{t k} = twA0 twAs^k, k < 8
+//   twB1[a] = W_T^a                    stage B twiddle W_T^{a q1} = twB1^q1, q1 < 8
 // (stage C's twiddles W_16^r, r < 8, are compile-time constants)
 template <typename C, int T>
 struct Fft8xTables {
     static_assert(T == 128, "the transform is written for 128 threads (M = 1024)");
     static constexpr int M = 8 * T, L = T / 8;
-    C twA[M];
-    C twB[T];
+    C twA0[T];
+    C twAs[T];
+    C twB1[L];
 };
 
 // host: the FP64 tables, computed in long double
@@ -208,10 +213,34 @@ inline void build_fft8x_tables(Fft8xTables<double2, T> &tab)
         const long double a = 2.0L * PI * (long double)num / (long double)den;
         return make_double2((double)cosl(a), (double)sinl(a));
     };
-    for (int k = 0; k < 8; ++k)
-        for (int t = 0; t < T; ++t) tab.twA[k * T + t] = cis((long long)t * (1 + 4 * k) % (4 * M), 4 * M);
-    for (int q1 = 0; q1 < 8; ++q1)
-        for (int a = 0; a < L; ++a) tab.twB[q1 * L + a] = cis((long long)(a * q1) % T, T);
+    for (int t = 0; t < T; ++t) {
+        tab.twA0[t] = cis(t, 4 * M);
+        tab.twAs[t] = cis(t, M);
+    }
+    for (int a = 0; a < L; ++a) tab.twB1[a] = cis(a, T);
+}
+
+// v[0..7] *= base * step^k (S = +1) or conj(base * step^k) (S = -1)
+template <int S, typename C>
+__device__ __forceinline__ void fft8x_twiddle_powers(C v[8], C base, C step)
+{
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        if (k > 0) base = cx_mul(base, step);
+        v[k] = S > 0 ? cx_mul(v[k], base) : cx_mulc(v[k], base);
+    }
+}
+
+// v[1..7] *= step^k (S = +1) or conj(step^k) (S = -1); v[0] unchanged
+template <int S, typename C>
+__device__ __forceinline__ void fft8x_step_powers(C v[8], C step)
+{
+    C p = step;
+#pragma unroll
+    for (int k = 1; k < 8; ++k) {
+        if (k > 1) p = cx_mul(p, step);
+        v[k] = S > 0 ? cx_mul(v[k], p) : cx_mulc(v[k], p);
+    }
 }
 
 // frequency held in register slot s of thread u after the forward transform:
@@ -260,8 +289,7 @@ __device__ __forceinline__ void fft8x_fwd(C v[8], C *xp, const Fft8xTables<C, T>
 {
     constexpr int L = T / 8;
     cx_dft8<1>(v);
-#pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = cx_mul(v[k], tab.twA[k * T + t]);
+    fft8x_twiddle_powers<1>(v, tab.twA0[t], tab.twAs[t]);
     __syncwarp();
 #pragma unroll
     for (int k = 0; k < 8; ++k) xp[fft8x_xp<C>(t, k)] = v[k];
@@ -270,8 +298,7 @@ __device__ __forceinline__ void fft8x_fwd(C v[8], C *xp, const Fft8xTables<C, T>
 #pragma unroll
     for (int b = 0; b < 8; ++b) v[b] = xp[fft8x_xp<C>(a + L * b, k)];
     cx_dft8<1>(v);
-#pragma unroll
-    for (int q1 = 1; q1 < 8; ++q1) v[q1] = cx_mul(v[q1], tab.twB[q1 * L + a]);
+    fft8x_step_powers<1>(v, tab.twB1[a]);
     // C: the second transpose stays inside the warp (rows t of this warp),
     // but other warps may still be reading these rows from the first one
     group_sync<T>(bar);
@@ -321,8 +348,7 @@ __device__ __forceinline__ void fft8x_inv(C v[8], C *xp, const Fft8xTables<C, T>
     __syncwarp();
 #pragma unroll
     for (int q1 = 0; q1 < 8; ++q1) v[q1] = xp[fft8x_xp<C>(t, q1)];
-#pragma unroll
-    for (int q1 = 1; q1 < 8; ++q1) v[q1] = cx_mulc(v[q1], tab.twB[q1 * L + a]);
+    fft8x_step_powers<-1>(v, tab.twB1[a]);
     cx_dft8<-1>(v);
     group_sync<T>(bar);
 #pragma unroll
@@ -330,8 +356,7 @@ __device__ __forceinline__ void fft8x_inv(C v[8], C *xp, const Fft8xTables<C, T>
     group_sync<T>(bar);
 #pragma unroll
     for (int kk = 0; kk < 8; ++kk) v[kk] = xp[fft8x_xp<C>(t, kk)];
-#pragma unroll
-    for (int kk = 0; kk < 8; ++kk) v[kk] = cx_mulc(v[kk], tab.twA[kk * T + t]);
+    fft8x_twiddle_powers<-1>(v, tab.twA0[t], tab.twAs[t]);
     cx_dft8<-1>(v);
 }
 

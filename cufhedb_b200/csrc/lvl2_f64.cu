@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(T2) extprod2_kernel(ExtProd2Args a)
     }
 }
 
-constexpr int PBS02_P = 3, PBS02_S = 3;
+constexpr int PBS02_P = 3, PBS02_S = 4;
 
 }  // namespace
 
