@@ -30,7 +30,7 @@
 
 namespace cfdb {
 
-// ---- complex arithmetic for both precisions ------------------------------------
+// ---- complex arithmetic ---------------------------------------------------------
 __device__ __forceinline__ double2 cx_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 cx_sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double2 cx_mul(double2 a, double2 b)
@@ -54,45 +54,8 @@ __device__ __forceinline__ double2 cx_shfl_xor(double2 v, int m)
 }
 __device__ __forceinline__ double2 cx_scale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
 
-__device__ __forceinline__ unsigned long long fx_bits(float2 a) { return *reinterpret_cast<unsigned long long *>(&a); }
-__device__ __forceinline__ float2 fx_from(unsigned long long a) { return *reinterpret_cast<float2 *>(&a); }
-// FP32 complex additions as one packed two-lane instruction (add/sub.rn.f32x2)
-__device__ __forceinline__ float2 cx_add(float2 a, float2 b)
-{
-    unsigned long long r;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(fx_bits(a)), "l"(fx_bits(b)));
-    return fx_from(r);
-}
-__device__ __forceinline__ float2 cx_sub(float2 a, float2 b)
-{
-    unsigned long long r;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(fx_bits(a)), "l"(fx_bits(b)));
-    return fx_from(r);
-}
-__device__ __forceinline__ float2 cx_mul(float2 a, float2 b)
-{
-    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
-}
-__device__ __forceinline__ float2 cx_mulc(float2 a, float2 b)
-{
-    return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
-}
-__device__ __forceinline__ void cx_fma(float2 &acc, float2 a, float2 b)
-{
-    acc.x = fmaf(a.x, b.x, acc.x);
-    acc.x = fmaf(-a.y, b.y, acc.x);
-    acc.y = fmaf(a.x, b.y, acc.y);
-    acc.y = fmaf(a.y, b.x, acc.y);
-}
-__device__ __forceinline__ float2 cx_shfl_xor(float2 v, int m)
-{
-    return fx_from(__shfl_xor_sync(0xffffffffu, fx_bits(v), m));
-}
-__device__ __forceinline__ float2 cx_scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
-
 template <typename C> struct cx_real;
 template <> struct cx_real<double2> { using type = double; };
-template <> struct cx_real<float2> { using type = float; };
 
 // multiply by i^S (S = +1) or (-i) (S = -1)
 template <int S, typename C>
