@@ -12,10 +12,11 @@
 // path (TFHEpp's own round trip error bound is 2^14, test/polymul.cpp:57-68).
 //
 // Layout: four warps (T2 = 128 threads, 8 complex values each) per ciphertext,
-// P ciphertexts and one bulk-copy producer warp per CTA.  The key streams
-// through the shared-memory ring in 16 KB chunks, one per (CMux i, TRGSW row
-// r, output o), shared by all ciphertexts of the CTA; a chunk is stored
-// [slot s][thread u], so each thread reads exactly the frequencies it owns.
+// P ciphertexts per CTA and no producer warp (ring.cuh KeyRing: the last warp
+// to release a slot refills it).  The key streams through the shared-memory
+// ring in 16 KB chunks, one per (CMux i, TRGSW row r, output o), shared by all
+// ciphertexts of the CTA; a chunk is stored [slot s][thread u], so each thread
+// reads exactly the frequencies it owns.
 #include "fft1024_f64.cuh"
 #include "lvl2.cuh"
 #include "ring.cuh"
