@@ -47,7 +47,7 @@ WORKLOAD = ("1,024 lvl1 HomNAND gate bootstraps (IKS10 + PBS01 each) over unifor
             "TFHEpp 128-bit params (n=672, N=1024, l=3, Bg=2^6, IKS10 basebit 10 t 2)")
 # DRAM bytes (read + write) of one 1,024-ciphertext PBS launch, from the ncu
 # captures summarised under profiles/ (pbs01_*_batch1024.md)
-TRAFFIC = {"split32": 69_288_704 + 3_700_480, "fp64": 69_385_472 + 3_819_008}
+TRAFFIC = {"split32": 69_165_824 + 3_885_824, "fp64": 69_385_472 + 3_819_008}
 
 
 def parse(argv=None):
