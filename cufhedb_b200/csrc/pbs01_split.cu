@@ -41,62 +41,41 @@ struct Pbs01SplitSmem {
     static constexpr int TOTAL = WARP_OFF + W * PER_WARP;
 };
 
-// Two equivalent forms of the integer <-> float steps (the same bits out):
-// FULLRATE = false uses the conversion instructions; FULLRATE = true builds
-// the floats from the integer bits with a logic op and an add on the
-// full-rate pipes.  Which is faster depends on the launch shape (measured:
-// 7 per CTA 9.73 -> 9.62 ms per 1,024 with the full-rate form, 8 per CTA
-// 10.95 -> 11.19 ms per 1,184), so each shape takes its faster form.
-
 // the decomposition words of (X^a - 1) * poly, once per polynomial:
-// w[2 m2 + h] = ((X^a - 1) poly)[m + 512 h] + offset + round, m = lane + 32 m2
-// (XORed with DEC1_XOR in the conversion form, whose digits are then the
-// sign-extended fields); digit d of a coefficient is the unsigned 6-bit field
-// d of its plain word minus Bg/2 (TFHEpp trgsw.cpp:31)
-template <bool FULLRATE>
+// w[2 m2 + h] = (((X^a - 1) poly)[m + 512 h] + offset + round) ^ DEC1_XOR,
+// m = lane + 32 m2; each of the l = 3 digits is then a field of these words
 __device__ __forceinline__ void digit_words1(uint32_t w[32], const uint32_t *poly, uint32_t abar, int lane)
 {
-    constexpr uint32_t X = FULLRATE ? 0u : DEC1_XOR;
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int m = lane + 32 * m2;
-        w[2 * m2] = ((rot_coef<N1>(poly, m, abar) - poly[m]) + DEC1_OFFSET + DEC1_ROUND) ^ X;
-        w[2 * m2 + 1] = ((rot_coef<N1>(poly, m + 512, abar) - poly[m + 512]) + DEC1_OFFSET + DEC1_ROUND) ^ X;
+        w[2 * m2] = ((rot_coef<N1>(poly, m, abar) - poly[m]) + DEC1_OFFSET + DEC1_ROUND) ^ DEC1_XOR;
+        w[2 * m2 + 1] = ((rot_coef<N1>(poly, m + 512, abar) - poly[m + 512]) + DEC1_OFFSET + DEC1_ROUND) ^ DEC1_XOR;
     }
-}
-
-// digit d of word x as a float.  Full-rate form: the 6-bit field f placed in
-// the mantissa of 2^23 reads as 2^23 + f, and subtracting 2^23 + Bg/2 leaves
-// f - 32 exactly.
-template <bool FULLRATE>
-__device__ __forceinline__ float digit_float1(uint32_t x, int d)
-{
-    if constexpr (FULLRATE)
-        return __uint_as_float(((x >> (32 - BGBIT1 * (d + 1))) & 63u) | 0x4B000000u) - 8388640.0f;
-    else
-        return (float)digit_field1(x, d);
 }
 
 // v[m2] = (dig_d(m) + i dig_d(m+512)) * w^{32 m2} from the cached words: the
 // per-register part of the twist (ffft512_fwd_tw applies the lane's part)
-template <bool FULLRATE>
 __device__ __forceinline__ void digits_from_words_f(float2 v[16], const uint32_t w[32], int d)
 {
 #pragma unroll
-    for (int m2 = 0; m2 < 16; ++m2)
-        v[m2] = cw64(make_float2(digit_float1<FULLRATE>(w[2 * m2], d), digit_float1<FULLRATE>(w[2 * m2 + 1], d)),
-                     m2);
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int d0 = digit_field1(w[2 * m2], d), d1 = digit_field1(w[2 * m2 + 1], d);
+        v[m2] = cw64(make_float2((float)d0, (float)d1), m2);
+    }
 }
 
-// round(h) * 2^24 mod 2^32.  Full-rate form: adding 1.5 * 2^23 leaves
-// round-to-nearest-even of h in the low mantissa bits (|h| < 2^22, ~40
-// standard deviations of the hi products), and the term needs only their low
-// 8 bits.
-template <bool FULLRATE>
+// round(h) * 2^24 mod 2^32 without a conversion instruction: adding
+// 1.5 * 2^23 leaves round-to-nearest-even of h in the low mantissa bits
+// (|h| < 2^22, ~40 standard deviations of the hi products), and the term
+// needs only their low 8 bits.  Same bits as __float2int_rn(h) << 24, on the
+// FMA and ALU pipes instead of the conversion unit (measured: 1,024 PBS
+// 9.73 -> 9.41 ms, 1,184 in the 8-per-CTA shape 10.95 -> 10.5 ms; building
+// the digits from their bits the same way measured slower in both shapes, so
+// they keep the int -> float conversion)
 __device__ __forceinline__ uint32_t hi_term(float h)
 {
-    if constexpr (FULLRATE) return __float_as_uint(h + 12582912.0f) << 24;
-    else return (uint32_t)__float2int_rn(h) << 24;
+    return __float_as_uint(h + 12582912.0f) << 24;
 }
 
 // poly[m] += round(hi_m) * 2^24 + round(lo_m) (mod 2^32), one read-modify-write
@@ -104,7 +83,6 @@ __device__ __forceinline__ uint32_t hi_term(float h)
 // output as pairs, inverse-transformed together.  The hi limb's products
 // round exactly; the lo limb's FP32 error stays far below the bootstrapping
 // noise.
-template <bool FULLRATE>
 __device__ __forceinline__ void add_inverse_split(uint32_t *poly, CP f[16], unsigned long long *xp, int lane,
                                                   const Fft512TablesFold &T)
 {
@@ -114,8 +92,8 @@ __device__ __forceinline__ void add_inverse_split(uint32_t *poly, CP f[16], unsi
         const int m = lane + 32 * m2;
         const CP y = untwist_m2(f[m2], m2);
         const float2 re = unpk2(y.re), im = unpk2(y.im);   // (hi, lo) of coefficients m and m + 512
-        poly[m] += hi_term<FULLRATE>(re.x) + (uint32_t)__float2ll_rn(re.y);
-        poly[m + 512] += hi_term<FULLRATE>(im.x) + (uint32_t)__float2ll_rn(im.y);
+        poly[m] += hi_term(re.x) + (uint32_t)__float2ll_rn(re.y);
+        poly[m + 512] += hi_term(im.x) + (uint32_t)__float2ll_rn(im.y);
     }
 }
 
@@ -143,8 +121,6 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
     // stage-1 twiddles, so the kernel reads 12.3 KB of tables instead of 24.4
     using TT = Fft512TablesFold;
     using L = Pbs01SplitSmem<W, S, (int)sizeof(TT)>;
-    // the faster integer <-> float form for this shape (measured, digit_words1)
-    constexpr bool FULLRATE = W == 7;
     extern __shared__ __align__(128) unsigned char smem[];
     TT *T = reinterpret_cast<TT *>(smem + L::TAB_OFF);
     const int ngroups = (a.B + W - 1) / W;
@@ -199,11 +175,11 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
             uint32_t w[32];
 #pragma unroll 1
             for (int r = 0; r < 2 * L1; ++r, ++c) {
-                if (active && r % L1 == 0) digit_words1<FULLRATE>(w, acc + (r / L1) * N1, ab, lane);
+                if (active && r % L1 == 0) digit_words1(w, acc + (r / L1) * N1, ab, lane);
                 const float4 *bkc = reinterpret_cast<const float4 *>(ring.acquire(c, a.err));
                 if (active) {
                     float2 v[16];
-                    digits_from_words_f<FULLRATE>(v, w, r % L1);
+                    digits_from_words_f(v, w, r % L1);
                     ffft512_fwd_tw(v, reinterpret_cast<float2 *>(xp), *T, lane);
                     if (r == 0) {
 #pragma unroll
@@ -228,8 +204,8 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
                 ring.release(c, lane);
             }
             if (active) {
-                add_inverse_split<FULLRATE>(acc, f0, xp, lane, *T);
-                add_inverse_split<FULLRATE>(acc + N1, f1, xp, lane, *T);
+                add_inverse_split(acc, f0, xp, lane, *T);
+                add_inverse_split(acc + N1, f1, xp, lane, *T);
                 __syncwarp();
             }
         }
