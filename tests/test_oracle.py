@@ -144,6 +144,33 @@ def test_golden_vectors(oracle, keys):
         assert (signed_diff(oracle.phase32(mine, s1), 0) > 0) == (signed_diff(oracle.phase32(out, s1), 0) > 0)
 
 
+def test_golden_vectors_lvl2(oracle, keys):
+    """lvl2 fixtures produced by the reference's TFHEpp (tests/golden/make_golden.py):
+    transforms, decomposition, both lvl2 key switches and the lvl02 PBS."""
+    g = np.load(os.path.join(GOLD, "tfhepp_lvl2.npz"))
+    assert int(g["seed"]) == SEED
+    for a, v, back in zip(g["fft_in"], g["fft_out"], g["fft_back"]):
+        assert np.max(np.abs(oracle.twist_ifft64(a) - v)) <= 1e-13 * np.max(np.abs(v))
+        # lvl2 round trip error is intrinsic to FP64 (TFHEpp test/polymul.cpp:57-68 allows 2^14)
+        assert max(abs(int(x)) for x in signed_diff(oracle.twist_fft64(v), back, 64)) <= 2 ** 14
+    for a, digits in zip(g["fft_in"], g["dec"]):
+        for d in range(4):
+            assert np.array_equal(oracle.decomp64(a, d), digits[d])
+    for kind in (20, 21):
+        for x, out in zip(g[f"iks{kind}_in"], g[f"iks{kind}_out"]):
+            assert np.array_equal(oracle.iks(kind, x, SEED, keys), out)
+    s0, _, s2 = keys
+    bk = oracle.bk02(SEED, s0, s2)
+    assert np.array_equal(bk[5, 6, 1, :8], g["bk_sample"])
+    bkf = np.stack([oracle.trgsw64_fft(row) for row in bk])
+    tv = np.full(N2, 1 << 61, np.uint64)
+    for x0, bit, out in zip(g["pbs_in"], g["pbs_bit"], g["pbs_out"]):
+        theirs = int(signed_diff(oracle.phase64(out, s2), 0, 64))
+        mine = int(signed_diff(oracle.phase64(oracle.pbs02(x0, bkf, tv), s2), 0, 64))
+        expect = (1 << 61) if bit else -(1 << 61)
+        assert abs(theirs - expect) < 2 ** 56 and abs(mine - theirs) < 2 ** 56
+
+
 def test_arcedb_digit_matches_reference(oracle, ref, keys):
     """The oracle's ArcEDB encodings and single-digit comparisons against the
     reference's own TFHEpp steps (FFT external product and FFT PolyMul, so a
