@@ -62,7 +62,9 @@ def parse(argv=None):
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--filter-rows", type=int, default=16384,
                    help="rows of the encrypted range filter timed at N=1 (0: skip)")
-    p.add_argument("--error-bootstraps", type=int, default=262144,
+    p.add_argument("--noise-samples", type=int, default=2048,
+                   help="lvl01 bootstraps compared with the FP64 (TFHEpp) and exact CPU oracles at N=1 (0: skip)")
+    p.add_argument("--error-bootstraps", type=int, default=1048576,
                    help="HomNAND bootstraps per path decrypted for the error rate at N=1 (0: skip)")
     p.add_argument("--filter-only", action="store_true", help="run only the range-filter measurement")
     p.add_argument("--error-only", action="store_true", help="run only the error-rate / noise measurement")
@@ -85,6 +87,18 @@ def parse(argv=None):
     p.add_argument("--profile-iks", type=int, choices=[10, 20, 21], default=0,
                    help="run only the identity key switch of this kind on `--batch` random inputs (its key only)")
     return p.parse_args(argv)
+
+
+def tensor_peak():
+    """(dense bf16 tensor-core TFLOP/s of this pool's B200s, source): the
+    measured burst figure of MEASURED_PEAKS.json when present, else the
+    earlier measurement on this pool (1,590 TFLOP/s)."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["bf16_tflops"]), "measured (MEASURED_PEAKS.json bf16_tflops, burst)"
+    except Exception:
+        return 1590.0, "fallback (earlier measurement on this pool)"
 
 
 def dist_env():
@@ -162,20 +176,35 @@ class ClockSampler:
 
 
 class CpuReference:
-    """The reference's TFHEpp HomNAND (oracle/_ref) on host threads over the
-    deterministic key set: keys are set up once, each run() is one bounded
-    sample."""
+    """The reference's TFHEpp / HEDB CPU code (oracle/_ref) on host threads
+    over the deterministic key set: keys are set up once, each run() is one
+    bounded sample."""
 
     def __init__(self, nthreads: int):
         from oracle.oracle import Oracle, RefTFHEpp
         self.nthreads = nthreads
         self.o, self.r = Oracle(), RefTFHEpp()
-        s0, s1, s2 = self.o.secret_keys(SEED)
+        self.keys = self.o.secret_keys(SEED)
+        s0, s1, s2 = self.keys
         self.s1 = s1
         self.r.set_secret(s0, s1, s2)
-        self.r.set_bk01(self.o.bk01(SEED, s0, s1, nthreads))
+        self.bk01 = self.o.bk01(SEED, s0, s1, nthreads)
+        self.r.set_bk01(self.bk01)
         ptr, _ = self.r.ksk_view(10)
-        self.o.ksk_full_into(10, SEED, (s0, s1, s2), ptr, nthreads)
+        self.o.ksk_full_into(10, SEED, self.keys, ptr, nthreads)
+        self.lvl2 = False
+
+    def load_lvl2(self):
+        """the lvl02 bootstrapping key and the lvl20 / lvl21 key-switching keys
+        (the HEDB lvl2 comparison chains need them)"""
+        if self.lvl2:
+            return
+        s0, _, s2 = self.keys
+        self.r.set_bk02(self.o.bk02(SEED, s0, s2, self.nthreads))
+        for kind in (20, 21):
+            ptr, _ = self.r.ksk_view(kind)
+            self.o.ksk_full_into(kind, SEED, self.keys, ptr, self.nthreads)
+        self.lvl2 = True
 
     def inputs(self, n: int):
         import numpy as np
@@ -185,41 +214,46 @@ class CpuReference:
                                                       base + i) for i, t in enumerate(b)])
         return enc(bits[0], 0), enc(bits[1], n)
 
-    def run(self, ca, cb) -> float:
-        """gates per second over the given pairs"""
+    def run(self, ca, cb, nthreads: int | None = None) -> float:
+        """HomNANDs per second over the given pairs"""
         t0 = time.perf_counter()
-        self.r.homnand_batch(ca, cb, self.nthreads)
+        self.r.homnand_batch(ca, cb, nthreads or self.nthreads)
         return ca.shape[0] / (time.perf_counter() - t0)
 
     def close(self):
         self.r.close()
 
 
-def cpu_sample_size(nthreads: int) -> int:
-    # ~20 CPU-seconds of TFHEpp HomNAND at ~25 ms per gate, at least 4 per thread
-    return max(800, 4 * nthreads)
-
-
 def run_reference(args):
+    """The reference's own TFHEpp HomNAND (oracle/_ref) on all host threads:
+    each step is one batch of the workload (--batch gates, 1,024 by default),
+    timed by the host clock."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
     nthreads = os.cpu_count() or 1
-    n = cpu_sample_size(nthreads)
+    n = args.batch
     ref = CpuReference(nthreads)
     ca, cb = ref.inputs(n)
     for _ in range(max(1, args.warmup)):
-        ref.run(ca[:nthreads], cb[:nthreads])
-    rates = [ref.run(ca, cb) for _ in range(args.steps)]
+        ref.run(ca, cb)
+    step_ms = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ref.r.homnand_batch(ca, cb, nthreads)
+        step_ms.append(1000.0 * (time.perf_counter() - t0))
     ref.close()
-    value = statistics.median(rates)
+    total_ms = sum(step_ms)
+    value = n * args.steps / (total_ms / 1000.0)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "PBS/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * args.batch / value,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "batch": args.batch, "l2": "n/a (host)"},
+        "config": {"workload": WORKLOAD, "batch_per_gpu": n, "precision": "fp64 (TFHEpp spqlios FFT)",
+                   "l2": "n/a (host)", "parallelism": f"{nthreads} host threads, row-parallel"},
         "cpu_baseline": {"value": value, "unit": "PBS/s", "cores": nthreads, "kind": "reference",
-                         "sample": f"{n} HomNANDs per step on {nthreads} host threads (TFHEpp from oracle/_ref)"},
+                         "sample": f"{n} HomNANDs per step (the whole batch) on {nthreads} host threads "
+                                   "(TFHEpp from oracle/_ref)"},
         "e2e": {"value": value, "unit": "PBS/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -292,6 +326,78 @@ def error_rate(eng, nboot: int, stream, chunk: int = 8192):
     return outd
 
 
+def noise_vs_oracles(eng, cref, n: int, stream):
+    """Per-bootstrap output noise of the GPU lvl01 PBS on both paths against
+    two CPU oracles, on the same keys and lvl0 inputs: the reference's own
+    TFHEpp GateBootstrappingTLWE2TLWEFFT<lvl01param> (FP64 FFT) and the exact
+    integer PBS (orc_pbs01_exact_batch: every negacyclic product exact).
+    Inputs are HomNAND gate inputs of fresh encryptions, key-switched on the
+    GPU (bit-exact with TFHEpp's IdentityKeySwitch).  Reported per path
+    (split32, fp64 on the GPU; tfhepp on the CPU): the output noise variance
+    (phase minus the encoded +-mu, torus units of 2^-32), its ratio to the
+    exact oracle's, the variance and largest size of the phase difference from
+    each oracle, and decryption errors."""
+    import numpy as np
+    import torch
+    from cufhedb_b200 import FP64, SPLIT32, testvec_const
+    rng = np.random.default_rng(4343)
+    bits = rng.integers(0, 2, (2, n))
+    s1 = cref.s1
+    from oracle.oracle import NS_LVL1
+    enc = lambda b, base: np.stack([cref.o.tlwe32(MU if t else (-MU) & 0xFFFFFFFF, s1, NS_LVL1, SEED, 0x7F, base + i)
+                                    for i, t in enumerate(b)])
+    ca, cb = enc(bits[0], 0), enc(bits[1], n)
+    x = ((0 - ca.astype(np.uint64) - cb.astype(np.uint64)) & 0xFFFFFFFF).astype(np.uint32)
+    x[:, N1] = (x[:, N1].astype(np.uint64) + MU).astype(np.uint32)   # HomNAND: (0, mu) - ca - cb
+    xd = torch.from_numpy(x.view(np.int32).copy()).cuda()
+    lvl0 = torch.empty(n * (N0 + 1), dtype=torch.int32, device="cuda")
+    eng.iks(10, xd, lvl0, stream)
+    outs = {}
+    for name, prec in (("split32", SPLIT32), ("fp64", FP64)):
+        o = torch.empty(n * (N1 + 1), dtype=torch.int32, device="cuda")
+        eng.pbs_lvl01(lvl0, o, testvec_const(MU), prec, stream)
+        outs[name] = o
+    stream.synchronize()
+    eng.sync(stream)
+    l0h = lvl0.cpu().numpy().view(np.uint32).reshape(n, N0 + 1)
+    tv = np.full(N1, MU, np.uint32)
+    t0 = time.perf_counter()
+    outs_h = {k: v.cpu().numpy().view(np.uint32).reshape(n, N1 + 1) for k, v in outs.items()}
+    outs_h["tfhepp"] = cref.r.pbs01_batch(l0h, tv, cref.nthreads)
+    t_ref = time.perf_counter() - t0
+    prep = cref.o.bk01_exact_prepare(cref.bk01)
+    t0 = time.perf_counter()
+    exact, max_dev = cref.o.pbs01_exact_batch(l0h, prep, tv, cref.nthreads)
+    t_exact = time.perf_counter() - t0
+    s1u = s1.astype(np.uint64)
+
+    def phase(c):
+        c = c.astype(np.uint64)
+        p = (c[:, N1] - (c[:, :N1] @ s1u)) & 0xFFFFFFFF
+        return np.where(p >= 2 ** 31, p.astype(np.float64) - 2 ** 32, p.astype(np.float64))
+
+    want = 1 - (bits[0] & bits[1])
+    expect = np.where(want == 1, float(MU), float(-MU))
+    p_exact = phase(exact)
+    p_ref = phase(outs_h["tfhepp"])
+    res = {"samples": n, "workload": "HomNAND inputs key-switched on the GPU, lvl01 PBS with mu = 2^29",
+           "exact": {"noise_var": float(np.var(p_exact - expect)), "decrypt_errors": int(np.sum((p_exact > 0) != want)),
+                     "max_fft_rounding_distance": max_dev, "cpu_s": t_exact,
+                     "oracle": "orc_pbs01_exact_batch (16-bit key limbs, FP64 FFT, every product rounded to its "
+                               "integer; equal to the schoolbook product)"},
+           "tfhepp_cpu_s": t_ref, "threads": cref.nthreads}
+    for name in ("split32", "fp64", "tfhepp"):
+        p = phase(outs_h[name])
+        nv = float(np.var(p - expect))
+        res[name] = {"noise_var": nv, "noise_var_over_exact": nv / res["exact"]["noise_var"],
+                     "decrypt_errors": int(np.sum((p > 0) != want)),
+                     "diff_vs_exact": {"var": float(np.var(p - p_exact)), "max_abs": float(np.max(np.abs(p - p_exact)))}}
+        if name != "tfhepp":
+            res[name]["noise_var_over_tfhepp"] = nv / float(np.var(p_ref - expect))
+            res[name]["diff_vs_tfhepp"] = {"var": float(np.var(p - p_ref)), "max_abs": float(np.max(np.abs(p - p_ref)))}
+    return res
+
+
 def range_filter(eng, rows: int, precision: int, steps: int = 1):
     """Encrypted range filter x <= c over a synthetic 20-bit column at lvl2
     (the reference's HomComp / TPC-H filter shape: less_than_equal<Lvl2>, 6 lvl02
@@ -324,7 +430,25 @@ def range_filter(eng, rows: int, precision: int, steps: int = 1):
     eng.phase_lvl1(out, ph)
     got = (ph > 0).cpu().numpy().astype(int)
     errors = int(np.sum(got != (x <= c).astype(int)))
-    return rows / (ms / 1000.0), ms, errors
+    return rows / (ms / 1000.0), ms, errors, (c1, c2, x, c)
+
+
+def filter_cpu_baseline(cref, c1, c2, x, c, rows: int):
+    """The reference's HEDB less_than_equal<Lvl2> (src/HEDB/comparison/
+    HomCompare.h:55-66) on all host threads over the first `rows` rows of the
+    filter's own ciphertexts: (rows/s, decrypt errors)."""
+    import numpy as np
+    cref.load_lvl2()
+    a = c1[:rows * (N2 + 1)].cpu().numpy().view(np.uint64).reshape(rows, N2 + 1)
+    b = c2[:rows * (N2 + 1)].cpu().numpy().view(np.uint64).reshape(rows, N2 + 1)
+    t0 = time.perf_counter()
+    out = cref.r.compare_batch(2, a, b, 3, 20, True, cref.nthreads)
+    rate = rows / (time.perf_counter() - t0)
+    s1u = cref.s1.astype(np.uint64)
+    o = out.astype(np.uint64)
+    ph = (o[:, N1] - (o[:, :N1] @ s1u)) & 0xFFFFFFFF
+    got = ((ph > 0) & (ph < 2 ** 31)).astype(int)
+    return rate, int(np.sum(got != (x[:rows] <= c).astype(int)))
 
 
 def run_ours(args):
@@ -431,20 +555,35 @@ def run_ours(args):
         "cuda")
 
     extra = {}
+    cref = None
+    if single and rank == 0 and not args.no_cpu_baseline:
+        cref = CpuReference(os.cpu_count() or 1)
     if single and rank == 0:
         if args.filter_rows:
-            rate, ms, ferr = range_filter(eng, args.filter_rows, PREC[head])
+            rate, ms, ferr, finputs = range_filter(eng, args.filter_rows, PREC[head])
             extra["filter"] = {"rows": args.filter_rows, "rows_per_s": rate, "ms": ms, "decrypt_errors": ferr,
                                "workload": "x <= c (30th percentile), 20-bit column at lvl2, less_than_equal<Lvl2>",
                                "bootstraps_per_row": {"lvl02": 6, "lvl01": 3},
                                "lvl01_path": head}
+            if cref is not None:
+                nrows = min(args.filter_rows, max(64, 4 * cref.nthreads))
+                crate, cerr = filter_cpu_baseline(cref, *finputs, nrows)
+                extra["filter"]["cpu_baseline"] = {
+                    "value": crate, "unit": "rows/s", "cores": cref.nthreads, "kind": "reference",
+                    "decrypt_errors": cerr,
+                    "sample": f"first {nrows} rows of the same ciphertexts, HEDB less_than_equal<Lvl2> "
+                              "(oracle/_ref) on all host threads"}
+            del finputs
         if args.error_bootstraps:
             extra["error_rate"] = error_rate(eng, args.error_bootstraps, stream)
+        if cref is not None and args.noise_samples:
+            extra["noise_vs_oracles"] = noise_vs_oracles(eng, cref, args.noise_samples, stream)
 
     if rank == 0:
         value = whole_job_rate(world, B, args.steps, t_head)
         v_other = whole_job_rate(world, B, args.steps, t_other)
         e2e_value = whole_job_rate(world, B, args.steps, t_e2e)
+        bf16, bf16_src = tensor_peak()
 
         def roof(name):
             ach = B * F1 / (res[name]["pbs_ms"] / 1000.0) / 1e12
@@ -453,6 +592,8 @@ def run_ours(args):
                     "traffic": TRAFFIC[name], "algorithmic_bytes": 66_060_288 + B * (2692 + 4100),
                     "peak_source": f"measured {'FP64' if name == 'fp64' else 'FP32'} CUDA-core FMA throughput "
                                    "(cufhedb_measure_fma_peak), this GPU, this run",
+                    "frac_of_bf16_tensor_peak": ach / bf16, "bf16_tensor_peak": bf16,
+                    "bf16_tensor_peak_source": bf16_src,
                     "algorithmic_flop_per_launch": B * F1}
 
         line = {
@@ -478,23 +619,24 @@ def run_ours(args):
                     "h2d_bytes_per_step": 2 * B * (N1 + 1) * 4, "d2h_bytes_per_step": B * (N1 + 1) * 4},
         }
         line.update(extra)
-        if single and not args.no_cpu_baseline:
+        if cref is not None:
             try:
-                nthreads = os.cpu_count() or 1
-                n = cpu_sample_size(nthreads)
+                nthreads = cref.nthreads
                 c_a = ca.cpu().numpy().view(np.uint32).reshape(B, N1 + 1)
                 c_b = cb.cpu().numpy().view(np.uint32).reshape(B, N1 + 1)
-                reps = -(-n // B)
-                c_a, c_b = np.tile(c_a, (reps, 1))[:n], np.tile(c_b, (reps, 1))[:n]
-                cref = CpuReference(nthreads)
                 cref.run(c_a[:nthreads], c_b[:nthreads])
                 rate = cref.run(c_a, c_b)
-                cref.close()
+                n1 = 16
+                rate1 = cref.run(c_a[:n1], c_b[:n1], 1)
                 line["cpu_baseline"] = {"value": rate, "unit": "PBS/s", "cores": nthreads, "kind": "reference",
-                                        "sample": f"{n} HomNANDs (TFHEpp from oracle/_ref) on {nthreads} host threads"}
+                                        "sample": f"the step's {B} HomNANDs (TFHEpp from oracle/_ref) on {nthreads} "
+                                                  "host threads",
+                                        "one_core": {"value": rate1, "unit": "PBS/s", "cores": 1,
+                                                     "sample": f"{n1} of the same HomNANDs on one thread"}}
             except Exception as exc:  # the GPU number stands without it
                 line["cpu_baseline"] = {"value": None, "unit": "PBS/s", "cores": None, "kind": "reference",
                                         "sample": f"unavailable: {exc}"}
+            cref.close()
         print(json.dumps(line), flush=True)
     eng.close()
     if world > 1:
@@ -508,7 +650,7 @@ def run_filter_only(args):
     eng = Engine(0)
     eng.keygen(SEED, GEN_ALL)
     rows = args.filter_rows or 16384
-    rate, ms, errors = range_filter(eng, rows, prec, max(1, args.steps))
+    rate, ms, errors, _ = range_filter(eng, rows, prec, max(1, args.steps))
     print(json.dumps({"workload": "range filter x <= c, 20-bit lvl2 column", "rows": rows,
                       "precision": args.precision, "rows_per_s": rate, "ms": ms, "decrypt_errors": errors,
                       "pbs_per_row": {"lvl02": 6, "lvl01": 3}}))

@@ -186,7 +186,7 @@ int cufhedb_arc_compare(cufhedb_ctx *ctx, int op, const uint32_t *trlwe, const v
     if (precision != CUFHEDB_FP64 && precision != CUFHEDB_SPLIT32) return set_error(CUFHEDB_ERR_ARG, "unsupported precision");
     if (D > 1 && !ctx->ksk[0]) return set_error(CUFHEDB_ERR_NOKEY, "lvl10 key-switching key not loaded");
     if (D > 1 && !ctx->bk01) return set_error(CUFHEDB_ERR_NOKEY, "lvl01 bootstrapping key not loaded");
-    cudaSetDevice(ctx->device);
+    DeviceGuard guard(ctx->device);
     Arc A{ctx, (cudaStream_t)stream, precision, B};
     const size_t trl = (size_t)B * 2 * N1, tlw = (size_t)B * (N1 + 1);
     const size_t gbytes = (size_t)B * 98304;   // prepared lvl1 TRGSW per row
@@ -229,7 +229,7 @@ int cufhedb_polymul_lvl1(cufhedb_ctx *ctx, const uint32_t *a, const double *m_fd
     if (!ctx || B < 0) return set_error(CUFHEDB_ERR_ARG, "bad argument");
     if (B == 0) return CUFHEDB_OK;
     if (!a || !m_fd || !out) return set_error(CUFHEDB_ERR_ARG, "null buffer");
-    cudaSetDevice(ctx->device);
+    DeviceGuard guard(ctx->device);
     cudaStream_t st = (cudaStream_t)stream;
     double *fd = nullptr;
     cudaError_t e = cudaMallocAsync((void **)&fd, (size_t)B * N1 * sizeof(double), st);
@@ -246,7 +246,7 @@ int cufhedb_polymul_lvl2(cufhedb_ctx *ctx, const uint64_t *a, const double *m_fd
     if (!ctx || B < 0) return set_error(CUFHEDB_ERR_ARG, "bad argument");
     if (B == 0) return CUFHEDB_OK;
     if (!a || !m_fd || !out) return set_error(CUFHEDB_ERR_ARG, "null buffer");
-    cudaSetDevice(ctx->device);
+    DeviceGuard guard(ctx->device);
     cudaStream_t st = (cudaStream_t)stream;
     double *fd = nullptr;
     cudaError_t e = cudaMallocAsync((void **)&fd, (size_t)B * N2 * sizeof(double), st);

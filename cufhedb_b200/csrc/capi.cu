@@ -190,10 +190,6 @@ int gate_enqueue(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint32_t 
     return CUFHEDB_OK;
 }
 
-struct DeviceGuard {
-    explicit DeviceGuard(int dev) { cudaSetDevice(dev); }
-};
-
 }  // namespace
 
 // Internal entry points shared with other translation units of the library
@@ -317,7 +313,8 @@ int cufhedb_ctx_create(cufhedb_ctx **out, int device)
     CK(cudaGetDeviceProperties(&prop, device));
     if (prop.major < 10)
         return fail(CUFHEDB_ERR_UNSUPPORTED, "cufhedb_b200 needs an sm_100 (Blackwell) device");
-    CK(cudaSetDevice(device));
+    DeviceGuard guard;
+    CK(guard.set(device));
     cufhedb_ctx *ctx = new cufhedb_ctx();
     ctx->device = device;
     ctx->num_sms = prop.multiProcessorCount;
@@ -340,6 +337,7 @@ int cufhedb_ctx_create(cufhedb_ctx **out, int device)
     if (e == cudaSuccess) e = init_pbs01_f64();
     if (e == cudaSuccess) e = init_pbs01_split();
     if (e == cudaSuccess) e = init_pbs02_f64();
+    if (e == cudaSuccess) e = noalloc_scratch_address(&ctx->noalloc_scratch);
     if (e != cudaSuccess) {
         cufhedb_ctx_destroy(ctx);
         return cuda_fail(e, "context set-up");
@@ -351,7 +349,7 @@ int cufhedb_ctx_create(cufhedb_ctx **out, int device)
 int cufhedb_ctx_destroy(cufhedb_ctx *ctx)
 {
     if (!ctx) return CUFHEDB_OK;
-    cudaSetDevice(ctx->device);
+    DeviceGuard g(ctx->device);
     if (ctx->io) cudaStreamSynchronize(ctx->io);
     cudaFree(ctx->tab512);
     cudaFree(ctx->tab512f);

@@ -33,9 +33,39 @@ struct cufhedb_ctx {
     float pbs01_pass_ms[2][2] = {{1.0f, 1.0f}, {1.0f, 1.0f}};
     uint32_t *s0_d = nullptr, *s1_d = nullptr;
     uint64_t *s2_d = nullptr;
+    // device address of the allocation-free gate's fixed intermediate
+    // (noalloc.cu), looked up when the context is created
+    uint32_t *noalloc_scratch = nullptr;
 };
 
 namespace cfdb {
+// Makes `dev` the calling thread's current device for the guard's lifetime
+// and gives the caller back its own current device afterwards.
+struct DeviceGuard {
+    int prev = -1;
+    DeviceGuard() = default;
+    explicit DeviceGuard(int dev) { set(dev); }
+    DeviceGuard(const DeviceGuard &) = delete;
+    DeviceGuard &operator=(const DeviceGuard &) = delete;
+    cudaError_t set(int dev)
+    {
+        int cur = -1;
+        cudaError_t e = cudaGetDevice(&cur);
+        if (e != cudaSuccess) return e;
+        if (cur == dev) return cudaSuccess;
+        e = cudaSetDevice(dev);
+        if (e == cudaSuccess && prev < 0) prev = cur;
+        return e;
+    }
+    ~DeviceGuard()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+// device address of the allocation-free gate's intermediate on the current
+// device (noalloc.cu); loads that module, so the array is reserved then
+cudaError_t noalloc_scratch_address(uint32_t **out);
 int set_error(int code, const char *msg);
 int cuda_error(cudaError_t e, const char *what);
 // PBS01 / PBS02 of a device batch with an optional constant added to each output's b

@@ -14,22 +14,21 @@
 //    with CUFHEDB_ERR_ARG; split them into several calls);
 //  * the array (NOALLOC_MAX_GATES x 673 x 4 bytes = 2.63 MiB) exists once per
 //    GPU that loads this library and stays reserved until the process exits;
+//    cufhedb_ctx_create looks up its device address (which loads this file's
+//    module, and so reserves the array) with the context's device current, so
+//    the reservation happens when the context is created, never inside a call;
 //  * every call on a device uses the same array: calls whose work overlaps on
-//    the GPU (different streams, or different host threads without ordering)
-//    race on it; order them on one stream.  The array keeps the last call's
-//    contents; every word a call reads is first written by that call.
-//  * the first call on each device looks up the device address of the array
-//    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture begins.
-#include <mutex>
+//    the GPU (different streams, different contexts on one device, or
+//    different host threads without ordering) race on it; order them on one
+//    stream.  The array keeps the last call's contents; every word a call
+//    reads is first written by that call.
 #include <string>
 
 #include "common.cuh"
 #include "cufhedb_b200.h"
+#include "ctx.cuh"
 
 namespace cfdb {
-int set_error(int code, const char *msg);
-int ctx_device(const cufhedb_ctx *ctx);
 int gate_enqueue_into(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint32_t *cb, uint32_t *out, int B,
                       int precision, cudaStream_t st, uint32_t *scratch_lvl0);
 }  // namespace cfdb
@@ -37,32 +36,23 @@ int gate_enqueue_into(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint
 namespace {
 
 constexpr int NOALLOC_MAX_GATES = 1024;
-constexpr int kMaxDevices = 64;
 
 // the lvl0 intermediate of up to NOALLOC_MAX_GATES gates
 static __device__ __align__(256) uint32_t g_gate_scratch[NOALLOC_MAX_GATES * (cfdb::N0 + 1)];
 
-std::mutex g_mu;
-uint32_t *g_scratch_addr[kMaxDevices] = {};
+}  // namespace
 
-// device address of g_gate_scratch on `dev` (current device), looked up once
-int scratch_for(int dev, uint32_t **out)
+namespace cfdb {
+
+cudaError_t noalloc_scratch_address(uint32_t **out)
 {
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch_addr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_gate_scratch);
-        if (e != cudaSuccess) {
-            std::string m = std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e);
-            return cfdb::set_error(CUFHEDB_ERR_CUDA, m.c_str());
-        }
-        g_scratch_addr[dev] = static_cast<uint32_t *>(p);
-    }
-    *out = g_scratch_addr[dev];
-    return CUFHEDB_OK;
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_gate_scratch);
+    *out = (e == cudaSuccess) ? static_cast<uint32_t *>(p) : nullptr;
+    return e;
 }
 
-}  // namespace
+}  // namespace cfdb
 
 extern "C" CUFHEDB_API int cufhedb_gate_lvl1_noalloc(cufhedb_ctx *ctx, int gate, const uint32_t *ca,
                                                      const uint32_t *cb, uint32_t *out, int B, int precision,
@@ -75,11 +65,9 @@ extern "C" CUFHEDB_API int cufhedb_gate_lvl1_noalloc(cufhedb_ctx *ctx, int gate,
                                "batch exceeds the allocation-free limit of 1024 gates per call; split the batch");
     if (B == 0) return CUFHEDB_OK;
     if (!ca || !cb || !out) return cfdb::set_error(CUFHEDB_ERR_ARG, "null buffer");
-    const int dev = cfdb::ctx_device(ctx);
-    if (dev < 0 || dev >= kMaxDevices) return cfdb::set_error(CUFHEDB_ERR_ARG, "device index out of range");
-    if (cudaSetDevice(dev) != cudaSuccess) return cfdb::set_error(CUFHEDB_ERR_CUDA, "cudaSetDevice failed");
-    uint32_t *scratch = nullptr;
-    int rc = scratch_for(dev, &scratch);
-    if (rc != CUFHEDB_OK) return rc;
-    return cfdb::gate_enqueue_into(ctx, gate, ca, cb, out, B, precision, (cudaStream_t)stream, scratch);
+    if (!ctx->noalloc_scratch) return cfdb::set_error(CUFHEDB_ERR_CUDA, "allocation-free intermediate not set up");
+    cfdb::DeviceGuard guard;
+    if (guard.set(ctx->device) != cudaSuccess) return cfdb::set_error(CUFHEDB_ERR_CUDA, "cudaSetDevice failed");
+    return cfdb::gate_enqueue_into(ctx, gate, ca, cb, out, B, precision, (cudaStream_t)stream,
+                                   ctx->noalloc_scratch);
 }

@@ -45,6 +45,7 @@ struct Ops {
     cudaStream_t st;
     int prec;
     int B;
+    DeviceGuard guard;   // the context's device while the operator enqueues
 
     template <typename T>
     int alloc(T **p, size_t words)
@@ -292,7 +293,7 @@ int begin_ops(cufhedb_ctx *ctx, int B, int precision, Ops &o, cufhedb_stream_t s
     if (B < 0) return set_error(CUFHEDB_ERR_ARG, "negative batch");
     if (precision != CUFHEDB_FP64 && precision != CUFHEDB_SPLIT32)
         return set_error(CUFHEDB_ERR_ARG, "unsupported precision");
-    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_error(CUFHEDB_ERR_CUDA, "cudaSetDevice failed");
+    if (o.guard.set(ctx->device) != cudaSuccess) return set_error(CUFHEDB_ERR_CUDA, "cudaSetDevice failed");
     o.c = ctx;
     o.st = (cudaStream_t)stream;
     o.prec = precision;
@@ -416,7 +417,7 @@ struct cufhedb_graph {
 CUFHEDB_API int cufhedb_graph_begin(cufhedb_ctx *ctx, cufhedb_stream_t stream)
 {
     if (!ctx || !stream) return cfdb::set_error(CUFHEDB_ERR_ARG, "capture needs a context and a non-default stream");
-    cudaSetDevice(ctx->device);
+    cfdb::DeviceGuard g(ctx->device);
     cudaError_t e = cudaStreamBeginCapture((cudaStream_t)stream, cudaStreamCaptureModeThreadLocal);
     return e == cudaSuccess ? CUFHEDB_OK : cfdb::cuda_error(e, "cudaStreamBeginCapture");
 }
@@ -424,7 +425,7 @@ CUFHEDB_API int cufhedb_graph_begin(cufhedb_ctx *ctx, cufhedb_stream_t stream)
 CUFHEDB_API int cufhedb_graph_end(cufhedb_ctx *ctx, cufhedb_stream_t stream, cufhedb_graph **out)
 {
     if (!ctx || !stream || !out) return cfdb::set_error(CUFHEDB_ERR_ARG, "bad argument");
-    cudaSetDevice(ctx->device);
+    cfdb::DeviceGuard g(ctx->device);
     cufhedb_graph *gr = new cufhedb_graph();
     cudaError_t e = cudaStreamEndCapture((cudaStream_t)stream, &gr->g);
     if (e == cudaSuccess) e = cudaGraphInstantiate(&gr->x, gr->g, 0);

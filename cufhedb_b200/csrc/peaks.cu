@@ -29,6 +29,13 @@ __global__ void fma_loop(T *out, int iters, T a, T b)
 extern "C" CUFHEDB_API int cufhedb_measure_fma_peak(int device, int fp64, double *tflops)
 {
     if (!tflops) return CUFHEDB_ERR_ARG;
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) return CUFHEDB_ERR_CUDA;
+    // the caller's current device is given back on every return below
+    struct Restore {
+        int dev;
+        ~Restore() { cudaSetDevice(dev); }
+    } restore{prev};
     if (cudaSetDevice(device) != cudaSuccess) return CUFHEDB_ERR_CUDA;
     cudaDeviceProp p;
     if (cudaGetDeviceProperties(&p, device) != cudaSuccess) return CUFHEDB_ERR_CUDA;

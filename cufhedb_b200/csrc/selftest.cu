@@ -39,7 +39,7 @@ int cufhedb_selftest_wait_timeout(cufhedb_ctx *ctx, uint32_t polls)
 {
     if (!ctx) return set_error(CUFHEDB_ERR_ARG, "ctx is null");
     if (polls == 0 || polls > (1u << 20)) return set_error(CUFHEDB_ERR_ARG, "polls must be in [1, 2^20]");
-    cudaSetDevice(ctx->device);
+    DeviceGuard guard(ctx->device);
     ring_timeout_selftest_kernel<<<1, ST_W * 32>>>(ctx->err, polls);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_error(e, "wait self-test launch");

@@ -190,10 +190,11 @@ CUFHEDB_API int cufhedb_gate_lvl1(cufhedb_ctx *ctx, int gate, const uint32_t *ca
  * device memory up front, or an allocator that owns the device).  No
  * counterpart in the reference.  The key-switched intermediate lives in a
  * fixed per-device array inside the library (2.63 MiB, held by every GPU that
- * loads the library until exit): B <= 1024 gates per call, larger batches are
- * rejected with CUFHEDB_ERR_ARG.  All calls on a device share that array, so
- * calls that overlap on the GPU race; order them on one stream.  The first
- * call on a device looks the array up (make it before any stream capture). */
+ * loads the library until exit; reserved by cufhedb_ctx_create, which looks
+ * up its address, so no call of this entry point allocates): B <= 1024 gates
+ * per call, larger batches are rejected with CUFHEDB_ERR_ARG.  All calls on a
+ * device share that array, so calls that overlap on the GPU race; order them
+ * on one stream.  The caller's current device is left as it was. */
 CUFHEDB_API int cufhedb_gate_lvl1_noalloc(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint32_t *cb,
                                           uint32_t *out, int B, int precision, cufhedb_stream_t stream);
 /* Prepared (frequency-domain) TRGSWs for the external product: 98,304 bytes

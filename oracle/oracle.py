@@ -77,6 +77,10 @@ class Oracle:
         self._g64fft = _sig(L, "orc_trgsw64_fft", [_f64p, _u64p])
         self._pbs01 = _sig(L, "orc_pbs01", [_u32p, _u32p, _f64p, _u32p])
         self._pbs01x = _sig(L, "orc_pbs01_exact", [_u32p, _u32p, _u32p, _u32p])
+        self._bkxprep = _sig(L, "orc_bk01_exact_prepare", [_f64p, _u32p])
+        self._ep32xs = _sig(L, "orc_extprod32_exact_split", [_u32p, _u32p, _f64p, C.POINTER(C.c_double)])
+        self._pbs01xb = _sig(L, "orc_pbs01_exact_batch", [_u32p, _u32p, i32, _f64p, _u32p, i32,
+                                                           C.POINTER(C.c_double)])
         self._pbs02 = _sig(L, "orc_pbs02", [_u64p, _u32p, _f64p, _u64p])
         self._br01 = _sig(L, "orc_blind_rotate01", [_u32p, _u32p, _f64p, _u32p])
         self._iks10 = _sig(L, "orc_iks10", [_u32p, _u32p, u64, _u32p, _u32p, C.c_void_p])
@@ -240,6 +244,32 @@ class Oracle:
         self._pbs01x(out, np.ascontiguousarray(in0, np.uint32), bk, np.ascontiguousarray(tv, np.uint32))
         return out
 
+    def bk01_exact_prepare(self, bk):
+        """the integer lvl01 key [672][6][2][1024] in the form the fast exact
+        PBS reads: each polynomial split into signed 16-bit limbs, transformed
+        ([672][6][2][2][1024] doubles, 132 MB)"""
+        bk = np.ascontiguousarray(bk, np.uint32)
+        prep = np.zeros((bk.shape[0], bk.shape[1], 2, 2, N1), np.float64)
+        self._bkxprep(prep, bk)
+        return prep
+
+    def extprod32_exact_split(self, trlwe, prep_trgsw):
+        """(exact external product, largest distance of an FFT product from an integer)"""
+        res = np.zeros((2, N1), np.uint32)
+        dev = C.c_double(0.0)
+        self._ep32xs(res, np.ascontiguousarray(trlwe, np.uint32), np.ascontiguousarray(prep_trgsw, np.float64),
+                     C.byref(dev))
+        return res, dev.value
+
+    def pbs01_exact_batch(self, in0, prep, tv, nthreads=os.cpu_count() or 1):
+        """exact lvl01 PBS of n lvl0 ciphertexts on host threads: (n x 1025
+        outputs, largest distance of an FFT product from an integer)"""
+        in0 = np.ascontiguousarray(in0, np.uint32).reshape(-1, N0 + 1)
+        out = np.zeros((in0.shape[0], N1 + 1), np.uint32)
+        dev = C.c_double(0.0)
+        self._pbs01xb(out, in0, in0.shape[0], prep, np.ascontiguousarray(tv, np.uint32), nthreads, C.byref(dev))
+        return out, dev.value
+
     def pbs02(self, in0, bkfft, tv):
         out = np.zeros(N2 + 1, np.uint64)
         self._pbs02(out, np.ascontiguousarray(in0, np.uint32), bkfft, np.ascontiguousarray(tv, np.uint64))
@@ -337,6 +367,8 @@ class RefTFHEpp:
         _sig(L, "tref_compare_lvl1", [vp, _u32p, _u32p, _u32p, i32, u32, i32])
         _sig(L, "tref_compare_lvl2", [vp, _u32p, _u64p, _u64p, i32, u32, i32])
         _sig(L, "tref_homand", [vp, _u32p, _u32p, _u32p, i32])
+        _sig(L, "tref_compare_lvl1_batch", [vp, _u32p, _u32p, _u32p, i32, i32, u32, i32, i32])
+        _sig(L, "tref_compare_lvl2_batch", [vp, _u32p, _u64p, _u64p, i32, i32, u32, i32, i32])
         _sig(L, "tref_arc_digit_lvl1", [_u32p, i32, _u32p, _f64p])
         _sig(L, "tref_arc_compare_batch", [vp, _u32p, i32, _u32p, _f64p, i32, i32, i32])
         self.L = L
@@ -463,6 +495,22 @@ class RefTFHEpp:
         out = np.zeros(N1 + 1, np.uint32)
         self.L.tref_compare_lvl2(self.ctx, out, np.ascontiguousarray(c1, np.uint64),
                                  np.ascontiguousarray(c2, np.uint64), op, plain_bits, int(logic))
+        return out
+
+    def compare_batch(self, level, c1, c2, op, plain_bits, logic=True, nthreads=os.cpu_count() or 1):
+        """n rows of HEDB::{greater_than, greater_than_equal, less_than,
+        less_than_equal, equal}<level> (op 0..4) on host threads; c1, c2: n x
+        (N+1) ciphertexts of that level; returns n lvl1 TLWEs"""
+        n = c1.shape[0]
+        out = np.zeros((n, N1 + 1), np.uint32)
+        if level == 1:
+            self.L.tref_compare_lvl1_batch(self.ctx, out, np.ascontiguousarray(c1, np.uint32),
+                                           np.ascontiguousarray(c2, np.uint32), n, op, plain_bits, int(logic),
+                                           nthreads)
+        else:
+            self.L.tref_compare_lvl2_batch(self.ctx, out, np.ascontiguousarray(c1, np.uint64),
+                                           np.ascontiguousarray(c2, np.uint64), n, op, plain_bits, int(logic),
+                                           nthreads)
         return out
 
     def homand(self, ca, cb, logic=True):

@@ -397,6 +397,45 @@ void tref_compare_lvl2(void *p, uint32_t *res, const uint64_t *c1, const uint64_
     std::memcpy(res, r.data(), sizeof(r));
 }
 
+// n rows of tref_compare_lvl1 / tref_compare_lvl2 on `nthreads` host threads
+// (row-parallel, as the reference's query drivers run the HEDB operators under
+// `omp parallel for`); rows are back to back in c1, c2 and res.
+void tref_compare_lvl1_batch(void *p, uint32_t *res, const uint32_t *c1, const uint32_t *c2, int n,
+                             int op, uint32_t plain_bits, int logic, int nthreads)
+{
+    const size_t w = lvl1param::n + 1;
+    std::atomic<int> next(0);
+    auto work = [&]() {
+        for (;;) {
+            const int i = next.fetch_add(1);
+            if (i >= n) break;
+            tref_compare_lvl1(p, res + i * w, c1 + i * w, c2 + i * w, op, plain_bits, logic);
+        }
+    };
+    if (nthreads <= 1) { work(); return; }
+    std::vector<std::thread> th;
+    for (int t = 0; t < nthreads; t++) th.emplace_back(work);
+    for (auto &t : th) t.join();
+}
+
+void tref_compare_lvl2_batch(void *p, uint32_t *res, const uint64_t *c1, const uint64_t *c2, int n,
+                             int op, uint32_t plain_bits, int logic, int nthreads)
+{
+    const size_t w2 = lvl2param::n + 1, w1 = lvl1param::n + 1;
+    std::atomic<int> next(0);
+    auto work = [&]() {
+        for (;;) {
+            const int i = next.fetch_add(1);
+            if (i >= n) break;
+            tref_compare_lvl2(p, res + i * w1, c1 + i * w2, c2 + i * w2, op, plain_bits, logic);
+        }
+    };
+    if (nthreads <= 1) { work(); return; }
+    std::vector<std::thread> th;
+    for (int t = 0; t < nthreads; t++) th.emplace_back(work);
+    for (auto &t : th) t.join();
+}
+
 void tref_homand(void *p, uint32_t *res, const uint32_t *ca, const uint32_t *cb, int logic)
 {
     RefCtx *c = static_cast<RefCtx *>(p);

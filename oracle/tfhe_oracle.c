@@ -322,6 +322,7 @@ static int bitrev(int x, int bits)
 /* twiddle tables, computed once in long double: rt[M][k] = exp(2 pi i k / M)
  * for k < M (M = 512 or 1024), tw[N][m] = exp(pi i m / N) for m < N/2 */
 static cpx *rt_tab[2], *tw_tab[2];
+static int *rev_tab[2];
 static pthread_once_t tab_once = PTHREAD_ONCE_INIT;
 
 static void build_tables(void)
@@ -330,6 +331,8 @@ static void build_tables(void)
         int N = t == 0 ? ORC_N1 : ORC_N2, M = N / 2;
         rt_tab[t] = (cpx *)malloc(sizeof(cpx) * M);
         tw_tab[t] = (cpx *)malloc(sizeof(cpx) * M);
+        rev_tab[t] = (int *)malloc(sizeof(int) * M);
+        for (int k = 0; k < M; k++) rev_tab[t][k] = bitrev(k, ilog2(M));
         for (int k = 0; k < M; k++) {
             long double a = 2.0L * PI_L * (long double)k / (long double)M;
             rt_tab[t][k].re = (double)cosl(a);
@@ -350,9 +353,9 @@ static int tab_id(int N)
 /* in-place radix-2 DIT; X[q] = sum x[m] exp(sign*2 pi i m q / M) */
 static void fft_inplace(cpx *x, int M, int sign, const cpx *rt)
 {
-    int bits = ilog2(M);
+    const int *rev = rev_tab[M == ORC_N1 / 2 ? 0 : 1];
     for (int i = 0; i < M; i++) {
-        int j = bitrev(i, bits);
+        int j = rev[i];
         if (i < j) { cpx t = x[i]; x[i] = x[j]; x[j] = t; }
     }
     for (int len = 2; len <= M; len <<= 1) {
@@ -371,7 +374,7 @@ static void fft_inplace(cpx *x, int M, int sign, const cpx *rt)
 
 static void twist_fwd(double *out, const double *ar, int N)
 {
-    int M = N / 2, bits = ilog2(M), t = tab_id(N);
+    int M = N / 2, t = tab_id(N);
     cpx z[ORC_N2 / 2];
     for (int m = 0; m < M; m++) {
         double c = tw_tab[t][m].re, s = tw_tab[t][m].im;
@@ -381,7 +384,7 @@ static void twist_fwd(double *out, const double *ar, int N)
     }
     fft_inplace(z, M, +1, rt_tab[t]);
     for (int idx = 0; idx < M; idx++) {
-        int q = bitrev(idx, bits);
+        int q = rev_tab[t][idx];
         out[idx] = z[q].re;
         out[idx + M] = z[q].im;
     }
@@ -390,10 +393,10 @@ static void twist_fwd(double *out, const double *ar, int N)
 /* returns the real coefficient values a_0..a_{N-1} (before torus conversion) */
 static void twist_inv(double *ar, const double *in, int N)
 {
-    int M = N / 2, bits = ilog2(M), t = tab_id(N);
+    int M = N / 2, t = tab_id(N);
     cpx z[ORC_N2 / 2];
     for (int idx = 0; idx < M; idx++) {
-        int q = bitrev(idx, bits);
+        int q = rev_tab[t][idx];
         z[q].re = in[idx];
         z[q].im = in[idx + M];
     }
@@ -697,6 +700,127 @@ void orc_pbs01_exact(uint32_t *out, const uint32_t *in0, const uint32_t *bk, con
         for (int j = 0; j < 2 * N; j++) acc[j] += prod[j];
     }
     orc_sample_extract32(out, acc, N);
+}
+
+/*
+ * Exact lvl01 PBS at FFT speed, for noise measurements over thousands of
+ * bootstraps (the schoolbook orc_pbs01_exact takes seconds per bootstrap).
+ * The external product is the same integer sum as orc_extprod32_exact,
+ * sum_{k,d} dec_d(acc_k) * trgsw[k l + d][m] in Z[X]/(X^N+1) mod 2^32, with
+ * every key polynomial g split into signed 16-bit limbs g = g1 * 2^16 + g0
+ * (g0 in [-2^15, 2^15), g1 in [-2^15, 2^15]).  Each limb product sum is an
+ * integer below 6 * 1024 * 32 * 2^15 = 2^32.6 in magnitude, so the FP64
+ * negacyclic FFT computes it to far better than 1/2 and rounding recovers it
+ * exactly; the result is v0 + v1 * 2^16 mod 2^32.  Every rounding is checked:
+ * the largest distance of an FFT output from its nearest integer is reported
+ * (a value below 1/4 certifies that every product was exact).
+ */
+#define PREP_ROW ((size_t)2 * 2 * ORC_N1)   /* per TRGSW row: [m][limb][N] doubles */
+
+void orc_bk01_exact_prepare(double *prep, const uint32_t *bk)
+{
+    double ar[ORC_N1];
+    for (size_t r = 0; r < (size_t)ORC_N0 * 2 * ORC_L1; r++)
+        for (int m = 0; m < 2; m++) {
+            const uint32_t *g = bk + (r * 2 + m) * ORC_N1;
+            for (int limb = 0; limb < 2; limb++) {
+                for (int j = 0; j < ORC_N1; j++) {
+                    int32_t v = (int32_t)g[j];
+                    int32_t g0 = (int32_t)(((uint32_t)v + 0x8000u) & 0xFFFFu) - 0x8000;
+                    ar[j] = limb == 0 ? (double)g0 : (double)(((int64_t)v - g0) >> 16);
+                }
+                twist_fwd(prep + r * PREP_ROW + ((size_t)m * 2 + limb) * ORC_N1, ar, ORC_N1);
+            }
+        }
+}
+
+static void extprod32_exact_split(uint32_t *res, const uint32_t *trlwe, const double *prep, double *max_dev)
+{
+    const int N = ORC_N1, L = ORC_L1;
+    double dfd[2 * ORC_L1][ORC_N1], acc[ORC_N1];
+    uint32_t dec[ORC_N1];
+    int64_t v[2][ORC_N1];
+    for (int k = 0; k < 2; k++)
+        for (int d = 0; d < L; d++) {
+            orc_decomp32(dec, trlwe + k * N, d);
+            double x[ORC_N1];
+            for (int j = 0; j < N; j++) x[j] = (double)(int32_t)dec[j];
+            twist_fwd(dfd[k * L + d], x, N);
+        }
+    for (int m = 0; m < 2; m++) {
+        for (int limb = 0; limb < 2; limb++) {
+            for (int r = 0; r < 2 * L; r++)
+                fma_fd(acc, dfd[r], prep + (size_t)r * PREP_ROW + ((size_t)m * 2 + limb) * N, N, r == 0);
+            double a[ORC_N1];
+            twist_inv(a, acc, N);
+            for (int j = 0; j < N; j++) {
+                double rj = nearbyint(a[j]);
+                double dev = fabs(a[j] - rj);
+                if (dev > *max_dev) *max_dev = dev;
+                v[limb][j] = (int64_t)rj;
+            }
+        }
+        for (int j = 0; j < N; j++) res[m * N + j] = (uint32_t)(uint64_t)(v[0][j] + v[1][j] * 65536);
+    }
+}
+
+void orc_extprod32_exact_split(uint32_t *res, const uint32_t *trlwe, const double *prep_trgsw, double *max_dev)
+{
+    *max_dev = 0.0;
+    extprod32_exact_split(res, trlwe, prep_trgsw, max_dev);
+}
+
+static void pbs01_exact_split(uint32_t *out, const uint32_t *in0, const double *prep, const uint32_t *tv,
+                              double *max_dev)
+{
+    const int N = ORC_N1;
+    uint32_t acc[2 * ORC_N1], tmp[2 * ORC_N1], prod[2 * ORC_N1];
+    uint32_t bbar = 2 * N - (in0[ORC_N0] >> 21);
+    memset(acc, 0, N * sizeof(uint32_t));
+    mulxai32(acc + N, tv, bbar, N);
+    for (int i = 0; i < ORC_N0; i++) {
+        uint32_t abar = (in0[i] + (1U << 20)) >> 21;
+        if (abar == 0) continue;
+        for (int k = 0; k < 2; k++) mulxai_minus1_32(tmp + k * N, acc + k * N, abar, N);
+        extprod32_exact_split(prod, tmp, prep + (size_t)i * 2 * ORC_L1 * PREP_ROW, max_dev);
+        for (int j = 0; j < 2 * N; j++) acc[j] += prod[j];
+    }
+    orc_sample_extract32(out, acc, N);
+}
+
+typedef struct {
+    uint32_t *out;
+    const uint32_t *in0, *tv;
+    const double *prep;
+    int t0, t1;
+    double max_dev;
+} pbsx_job_t;
+
+static void *pbsx_job(void *arg)
+{
+    pbsx_job_t *j = (pbsx_job_t *)arg;
+    for (int b = j->t0; b < j->t1; b++)
+        pbs01_exact_split(j->out + (size_t)b * (ORC_N1 + 1), j->in0 + (size_t)b * (ORC_N0 + 1), j->prep, j->tv,
+                          &j->max_dev);
+    return NULL;
+}
+
+void orc_pbs01_exact_batch(uint32_t *out, const uint32_t *in0, int n, const double *prep, const uint32_t *tv,
+                           int nthreads, double *max_dev)
+{
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    pthread_t th[256];
+    pbsx_job_t jobs[256];
+    for (int t = 0; t < nthreads; t++) {
+        jobs[t] = (pbsx_job_t){out, in0, tv, prep, (int)((long)n * t / nthreads), (int)((long)n * (t + 1) / nthreads), 0.0};
+        pthread_create(&th[t], NULL, pbsx_job, &jobs[t]);
+    }
+    *max_dev = 0.0;
+    for (int t = 0; t < nthreads; t++) {
+        pthread_join(th[t], NULL);
+        if (jobs[t].max_dev > *max_dev) *max_dev = jobs[t].max_dev;
+    }
 }
 
 void orc_pbs02(uint64_t *out, const uint32_t *in0, const double *bkfft, const uint64_t *tv)

@@ -96,6 +96,13 @@ void orc_blind_rotate01(uint32_t *acc, const uint32_t *in0, const double *bkfft,
 void orc_pbs01(uint32_t *out, const uint32_t *in0, const double *bkfft, const uint32_t *tv);
 void orc_pbs02(uint64_t *out, const uint32_t *in0, const double *bkfft, const uint64_t *tv);
 void orc_pbs01_exact(uint32_t *out, const uint32_t *in0, const uint32_t *bk, const uint32_t *tv);
+/* the exact PBS at FFT speed: key prepared once ([672][6][2 outputs][2 limbs][1024]
+ * doubles, 132 MB), n bootstraps on nthreads threads; *max_dev is the largest
+ * distance of an FFT product from its nearest integer (< 1/4: all exact) */
+void orc_bk01_exact_prepare(double *prep, const uint32_t *bk);
+void orc_extprod32_exact_split(uint32_t *res, const uint32_t *trlwe, const double *prep_trgsw, double *max_dev);
+void orc_pbs01_exact_batch(uint32_t *out, const uint32_t *in0, int n, const double *prep, const uint32_t *tv,
+                           int nthreads, double *max_dev);
 void orc_sample_extract32(uint32_t *out, const uint32_t *acc, int N);
 void orc_sample_extract64(uint64_t *out, const uint64_t *acc, int N);
 

@@ -115,6 +115,29 @@ def test_pbs01_decrypts_like_reference(oracle, ref_keyed, keys, bkfft01):
         assert abs(pr - expect) < 2 ** 26 and abs(po - expect) < 2 ** 26
 
 
+def test_fast_exact_pbs_equals_schoolbook(oracle, keys, bk01):
+    """The exact PBS used for noise measurements (16-bit key limbs through the
+    FP64 FFT, every product rounded to its integer) equals the schoolbook
+    integer product bit for bit: external products on random accumulators,
+    and a whole bootstrap against orc_pbs01_exact; its exactness certificate
+    (largest distance of an FFT product from an integer) stays far below 1/4."""
+    s0, _, _ = keys
+    prep = oracle.bk01_exact_prepare(bk01)
+    rng = np.random.default_rng(0x5C)
+    for i in (0, 1, 671):
+        trl = rng.integers(0, 2 ** 32, (2, N1), dtype=np.uint64).astype(np.uint32)
+        got, dev = oracle.extprod32_exact_split(trl, prep[i])
+        assert np.array_equal(got, oracle.extprod32_exact(trl, bk01[i])) and dev < 1e-3
+    x = np.stack([oracle.tlwe32((1 << 29) if i else (-(1 << 29)) & 0xFFFFFFFF, s0, NS_LVL0, SEED, 0x5D, i)
+                  for i in range(2)])
+    tv = np.full(N1, 1 << 29, np.uint32)
+    out, dev = oracle.pbs01_exact_batch(x, prep, tv)
+    assert dev < 1e-3
+    assert np.array_equal(out[0], oracle.pbs01_exact(x[0], bk01, tv))
+    ph = [int(signed_diff(oracle.phase32(o, keys[1]), 0)) for o in out]
+    assert ph[0] < 0 < ph[1]
+
+
 def test_golden_vectors(oracle, keys):
     """Fixtures produced by the reference's TFHEpp (tests/golden/make_golden.py)."""
     g = np.load(os.path.join(GOLD, "tfhepp_lvl1.npz"))
