@@ -47,7 +47,7 @@ WORKLOAD = ("1,024 lvl1 HomNAND gate bootstraps (IKS10 + PBS01 each) over unifor
             "TFHEpp 128-bit params (n=672, N=1024, l=3, Bg=2^6, IKS10 basebit 10 t 2)")
 # DRAM bytes (read + write) of one 1,024-ciphertext PBS launch, from the ncu
 # captures summarised under profiles/ (pbs01_*_batch1024.md)
-TRAFFIC = {"split32": 69_165_824 + 3_885_824, "fp64": 69_385_472 + 3_819_008}
+TRAFFIC = {"split32": 68_939_264 + 3_732_480, "fp64": 69_385_472 + 3_819_008}
 
 
 def parse(argv=None):
@@ -491,13 +491,13 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    # ---- launch-shape autotuning (untimed): one pass with 7 and with 8 ----------
-    tune = {}
-    for name in (head, other):
-        ms7, ms8 = eng.autotune_pbs01(PREC[name])
-        passes = lambda w: -(-(-(-B // w)) // eng.num_sms)
-        w = 8 if passes(8) * ms8 < passes(7) * ms7 else 7
-        tune[name] = {"pass_ms_w7": ms7, "pass_ms_w8": ms8, "ciphertexts_per_cta": w}
+    # ---- launch-shape autotuning (untimed): one full pass of every shape ----------
+    tuned = eng.autotune(levels=(1, 2) if (single and args.filter_rows) else (1,))
+    tune = {f"pbs01_{name}": {"pass_ms_by_shape": tuned[f"pbs01_{name}"],
+                              "ciphertexts_per_cta": eng.launch_shape(1, PREC[name], B)} for name in (head, other)}
+    if single and args.filter_rows:
+        tune["pbs02"] = {"pass_ms_by_shape": tuned["pbs02"],
+                         "ciphertexts_per_cta_filter": eng.launch_shape(2, FP64, args.filter_rows)}
 
     # ---- the timed gate steps, headline path then the other path ----------------
     res = {}
@@ -809,11 +809,10 @@ def run_profile_iks(args):
 
 
 def _engine_all_keys_tuned():
-    from cufhedb_b200 import FP64, GEN_ALL, SPLIT32, Engine
+    from cufhedb_b200 import GEN_ALL, Engine
     eng = Engine(0)
     eng.keygen(SEED, GEN_ALL)
-    tune = {name: eng.autotune_pbs01(p) for name, p in (("split32", SPLIT32), ("fp64", FP64))}
-    return eng, tune
+    return eng, eng.autotune()
 
 
 def run_agg(args):
@@ -872,7 +871,7 @@ def run_arc(args):
     rows, D = args.arc_rows, args.arc_digits
     eng = Engine(0)
     eng.keygen(SEED, GEN_BK01 | GEN_KSK10)
-    tune = {name: eng.autotune_pbs01(p) for name, p in (("split32", SPLIT32), ("fp64", FP64))}
+    tune = eng.autotune(levels=(1,))
     o = Oracle()
     s0, s1, s2 = o.secret_keys(SEED)
     # 256 distinct encrypted rows (a quarter equal values, a quarter equal top

@@ -62,6 +62,11 @@ SIGNATURES = {
     "cufhedb_encrypt_lvl2": [_vp, _u64, _u64, _u64, _vp, _vp, _i32, _vp],
     "cufhedb_phase_lvl1": [_vp, _vp, _vp, _vp, _i32, _vp],
     "cufhedb_autotune_pbs01": [_vp, _i32, _vp, _vp],
+    "cufhedb_autotune_pbs02": [_vp, _vp],
+    "cufhedb_autotune_table": [_vp, _i32, _i32, _vp, _vp],
+    "cufhedb_launch_shape": [_vp, _i32, _i32, _i32, _vp],
+    "cufhedb_autotune_save": [_vp, C.c_char_p],
+    "cufhedb_autotune_load": [_vp, C.c_char_p],
     "cufhedb_load_keyfile": [_vp, C.c_char_p, _vp],
     "cufhedb_arc_compare": [_vp, _i32, _vp, _vp, _vp, _i32, _i32, _i32, _vp],
     "cufhedb_polymul_lvl1": [_vp, _vp, _vp, _vp, _i32, _i32, _vp],

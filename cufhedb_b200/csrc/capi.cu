@@ -240,7 +240,7 @@ int pbs02_run(cufhedb_ctx *ctx, const uint32_t *in, uint64_t *out, int B, const 
     a.tv = tv;
     a.out_b_add = b_add;
     a.err = ctx->err;
-    CK(launch_pbs02_f64(a, ctx->num_sms, st));
+    CK(launch_pbs02_f64(a, ctx->num_sms, pbs02_choose_p(B, ctx->num_sms, ctx->pbs02_pass_ms), st));
     return CUFHEDB_OK;
 }
 
@@ -735,54 +735,71 @@ int cufhedb_pbs_lvl01(cufhedb_ctx *ctx, const uint32_t *in_lvl0, uint32_t *out_l
     return pbs01_enqueue(ctx, in_lvl0, out_lvl1, B, tv, precision, (cudaStream_t)stream);
 }
 
-int cufhedb_autotune_pbs01(cufhedb_ctx *ctx, int precision, float *ms_w7, float *ms_w8)
+// One full pass (w ciphertexts on every SM) of each launch shape of a PBS
+// kernel over uniform random lvl0 inputs: the best of two timed runs after
+// one warm-up run.  level 1: precision FP64 or split; level 2: FP64.
+static int autotune_level(cufhedb_ctx *ctx, int level, int precision, float out_ms[NSHAPES])
 {
-    NEED(ctx != nullptr, "ctx is null");
-    NEED(precision == CUFHEDB_FP64 || precision == CUFHEDB_SPLIT32, "unsupported precision");
-    if (!ctx->bk01) return fail(CUFHEDB_ERR_NOKEY, "lvl01 bootstrapping key not loaded");
-    DeviceGuard g(ctx->device);
-    const int Bmax = 8 * ctx->num_sms;
+    const int *shapes = level == 1 ? PBS01_SHAPES : PBS02_SHAPES;
+    int wmax = 0;
+    for (int i = 0; i < NSHAPES; ++i) wmax = std::max(wmax, shapes[i]);
+    const int Bmax = wmax * ctx->num_sms;
+    const size_t out_words = (size_t)Bmax * (level == 1 ? (N1 + 1) : 2 * (N2 + 1));
     uint32_t *in = nullptr, *out = nullptr;
     cudaStream_t st = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    float best[2] = {0.0f, 0.0f};
     int rc = CUFHEDB_OK;
     cudaError_t e = cudaMalloc((void **)&in, (size_t)Bmax * (N0 + 1) * 4);
-    if (e == cudaSuccess) e = cudaMalloc((void **)&out, (size_t)Bmax * (N1 + 1) * 4);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&out, out_words * 4);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&e0);
     if (e == cudaSuccess) e = cudaEventCreate(&e1);
     if (e == cudaSuccess) e = fill_random32(in, (size_t)Bmax * (N0 + 1), 0x7A5E, 1, st);
     if (e != cudaSuccess) rc = cuda_fail(e, "autotune setup");
-    const cufhedb_testvec tv{CUFHEDB_TV_CONST, 0, 1u << 29, nullptr};
-    for (int w = 7; w <= 8 && rc == CUFHEDB_OK; ++w) {
-        // one full pass: w ciphertexts on every SM
-        Pbs01Args a{};
-        a.in = in;
-        a.out = out;
-        a.B = w * ctx->num_sms;
-        a.tv = to_tv(&tv);
-        a.err = ctx->err;
-        a.bk = precision == CUFHEDB_FP64 ? ctx->bk01 : reinterpret_cast<const double2 *>(ctx->bk01_split);
-        a.tables = precision == CUFHEDB_FP64 ? (const void *)ctx->tab512 : (const void *)ctx->tab512f;
-        if (!a.bk) {
-            rc = fail(CUFHEDB_ERR_NOKEY, "split-precision lvl01 key not prepared");
-            break;
-        }
+    for (int i = 0; i < NSHAPES && rc == CUFHEDB_OK; ++i) {
+        const int w = shapes[i];
         float t_best = 0.0f;
         for (int it = 0; it < 3 && rc == CUFHEDB_OK; ++it) {
             e = cudaEventRecord(e0, st);
-            if (e == cudaSuccess)
-                e = precision == CUFHEDB_FP64 ? launch_pbs01_f64(a, ctx->num_sms, w, st)
-                                              : launch_pbs01_split(a, ctx->num_sms, w, st);
+            if (e == cudaSuccess) {
+                if (level == 1) {
+                    const cufhedb_testvec tv{CUFHEDB_TV_CONST, 0, 1u << 29, nullptr};
+                    Pbs01Args a{};
+                    a.in = in;
+                    a.out = out;
+                    a.B = w * ctx->num_sms;
+                    a.tv = to_tv(&tv);
+                    a.err = ctx->err;
+                    if (precision == CUFHEDB_FP64) {
+                        a.bk = ctx->bk01;
+                        a.tables = ctx->tab512;
+                        e = launch_pbs01_f64(a, ctx->num_sms, w, st);
+                    } else {
+                        a.bk = reinterpret_cast<const double2 *>(ctx->bk01_split);
+                        a.tables = ctx->tab512f;
+                        e = launch_pbs01_split(a, ctx->num_sms, w, st);
+                    }
+                } else {
+                    const cufhedb_testvec tv{CUFHEDB_TV_CONST, 0, 1ull << 61, nullptr};
+                    Pbs02Args a{};
+                    a.in = in;
+                    a.out = reinterpret_cast<uint64_t *>(out);
+                    a.B = w * ctx->num_sms;
+                    a.bk = ctx->bk02;
+                    a.tables = ctx->tab1024;
+                    a.tv = to_tv(&tv);
+                    a.err = ctx->err;
+                    e = launch_pbs02_f64(a, ctx->num_sms, w, st);
+                }
+            }
             if (e == cudaSuccess) e = cudaEventRecord(e1, st);
             if (e == cudaSuccess) e = cudaEventSynchronize(e1);
             float ms = 0.0f;
             if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
             if (e != cudaSuccess) rc = cuda_fail(e, "autotune run");
-            else if (it > 0 && (t_best == 0.0f || ms < t_best)) t_best = ms;   // first run warms up
+            else if (it > 0 && (t_best == 0.0f || ms < t_best)) t_best = ms;   // the first run warms up
         }
-        best[w - 7] = t_best;
+        out_ms[i] = t_best;
     }
     if (rc == CUFHEDB_OK) rc = cufhedb_sync(ctx, st);
     if (st) cudaStreamDestroy(st);
@@ -790,11 +807,150 @@ int cufhedb_autotune_pbs01(cufhedb_ctx *ctx, int precision, float *ms_w7, float 
     if (e1) cudaEventDestroy(e1);
     cudaFree(in);
     cudaFree(out);
+    return rc;
+}
+
+int cufhedb_autotune_pbs01(cufhedb_ctx *ctx, int precision, float *ms_w7, float *ms_w8)
+{
+    NEED(ctx != nullptr, "ctx is null");
+    NEED(precision == CUFHEDB_FP64 || precision == CUFHEDB_SPLIT32, "unsupported precision");
+    if (!ctx->bk01) return fail(CUFHEDB_ERR_NOKEY, "lvl01 bootstrapping key not loaded");
+    if (precision == CUFHEDB_SPLIT32 && !ctx->bk01_split)
+        return fail(CUFHEDB_ERR_NOKEY, "split-precision lvl01 key not prepared");
+    DeviceGuard g(ctx->device);
+    float ms[NSHAPES];
+    const int rc = autotune_level(ctx, 1, precision, ms);
     if (rc != CUFHEDB_OK) return rc;
-    ctx->pbs01_pass_ms[precision][0] = best[0];
-    ctx->pbs01_pass_ms[precision][1] = best[1];
-    if (ms_w7) *ms_w7 = best[0];
-    if (ms_w8) *ms_w8 = best[1];
+    for (int i = 0; i < NSHAPES; ++i) ctx->pbs01_pass_ms[precision][i] = ms[i];
+    if (ms_w7) *ms_w7 = ms[0];
+    if (ms_w8) *ms_w8 = ms[1];
+    return CUFHEDB_OK;
+}
+
+int cufhedb_autotune_pbs02(cufhedb_ctx *ctx, float *ms)
+{
+    NEED(ctx != nullptr, "ctx is null");
+    if (!ctx->bk02) return fail(CUFHEDB_ERR_NOKEY, "lvl02 bootstrapping key not loaded");
+    DeviceGuard g(ctx->device);
+    float t[NSHAPES];
+    const int rc = autotune_level(ctx, 2, CUFHEDB_FP64, t);
+    if (rc != CUFHEDB_OK) return rc;
+    for (int i = 0; i < NSHAPES; ++i) {
+        ctx->pbs02_pass_ms[i] = t[i];
+        if (ms) ms[i] = t[i];
+    }
+    return CUFHEDB_OK;
+}
+
+static float *shape_table(cufhedb_ctx *ctx, int level, int precision)
+{
+    if (level == 1 && (precision == CUFHEDB_FP64 || precision == CUFHEDB_SPLIT32))
+        return ctx->pbs01_pass_ms[precision];
+    if (level == 2 && precision == CUFHEDB_FP64) return ctx->pbs02_pass_ms;
+    return nullptr;
+}
+
+int cufhedb_autotune_table(cufhedb_ctx *ctx, int level, int precision, int *shapes, float *pass_ms)
+{
+    NEED(ctx != nullptr, "ctx is null");
+    const float *t = shape_table(ctx, level, precision);
+    NEED(t != nullptr, "no launch shapes for this level and precision");
+    for (int i = 0; i < NSHAPES; ++i) {
+        if (shapes) shapes[i] = level == 1 ? PBS01_SHAPES[i] : PBS02_SHAPES[i];
+        if (pass_ms) pass_ms[i] = t[i];
+    }
+    return NSHAPES;
+}
+
+int cufhedb_launch_shape(cufhedb_ctx *ctx, int level, int precision, int B, int *shape)
+{
+    NEED(ctx != nullptr && shape != nullptr, "null argument");
+    const float *t = shape_table(ctx, level, precision);
+    NEED(t != nullptr && B > 0, "bad level, precision or batch");
+    *shape = level == 1 ? pbs01_choose_w(B, ctx->num_sms, t) : pbs02_choose_p(B, ctx->num_sms, t);
+    return CUFHEDB_OK;
+}
+
+// A table is valid for one device model, SM count and parameter set: the
+// hash covers the parameters the kernels are compiled for and the shape lists.
+static uint64_t param_hash()
+{
+    char buf[160];
+    std::snprintf(buf, sizeof buf, "n0=%d n1=%d l1=%d bg1=%d n2=%d l2=%d bg2=%d s1=%d,%d,%d s2=%d,%d,%d", N0, N1, L1,
+                  BGBIT1, N2, L2, BGBIT2, PBS01_SHAPES[0], PBS01_SHAPES[1], PBS01_SHAPES[2], PBS02_SHAPES[0],
+                  PBS02_SHAPES[1], PBS02_SHAPES[2]);
+    uint64_t h = 1469598103934665603ull;   // FNV-1a
+    for (const char *c = buf; *c; ++c) h = (h ^ (unsigned char)*c) * 1099511628211ull;
+    return h;
+}
+
+static std::string device_tag(int device)
+{
+    cudaDeviceProp prop;
+    std::string name = cudaGetDeviceProperties(&prop, device) == cudaSuccess ? prop.name : "unknown";
+    for (char &c : name)
+        if (c == ' ') c = '_';
+    return name;
+}
+
+int cufhedb_autotune_save(cufhedb_ctx *ctx, const char *path)
+{
+    NEED(ctx && path, "null argument");
+    FILE *f = std::fopen(path, "w");
+    if (!f) return fail(CUFHEDB_ERR_ARG, std::string("cannot write ") + path);
+    std::fprintf(f, "cufhedb_b200 autotune 1\ndevice %s sms %d params %016llx\n", device_tag(ctx->device).c_str(),
+                 ctx->num_sms, (unsigned long long)param_hash());
+    const char *names[2] = {"fp64", "split32"};
+    for (int p = 0; p < 2; ++p) {
+        std::fprintf(f, "pbs01 %s", names[p]);
+        for (int i = 0; i < NSHAPES; ++i) std::fprintf(f, " %d %.6f", PBS01_SHAPES[i], ctx->pbs01_pass_ms[p][i]);
+        std::fprintf(f, "\n");
+    }
+    std::fprintf(f, "pbs02 fp64");
+    for (int i = 0; i < NSHAPES; ++i) std::fprintf(f, " %d %.6f", PBS02_SHAPES[i], ctx->pbs02_pass_ms[i]);
+    std::fprintf(f, "\n");
+    const bool ok = std::fclose(f) == 0;
+    return ok ? CUFHEDB_OK : fail(CUFHEDB_ERR_ARG, std::string("cannot write ") + path);
+}
+
+int cufhedb_autotune_load(cufhedb_ctx *ctx, const char *path)
+{
+    NEED(ctx && path, "null argument");
+    FILE *f = std::fopen(path, "r");
+    if (!f) return fail(CUFHEDB_ERR_ARG, std::string("cannot read ") + path);
+    char dev[256] = {0}, kind[16] = {0}, prec[16] = {0};
+    int version = 0, sms = 0;
+    unsigned long long hash = 0;
+    bool ok = std::fscanf(f, "cufhedb_b200 autotune %d device %255s sms %d params %llx", &version, dev, &sms,
+                          &hash) == 4 &&
+              version == 1;
+    const bool same = ok && device_tag(ctx->device) == dev && sms == ctx->num_sms && hash == param_hash();
+    float t01[2][NSHAPES], t02[NSHAPES];
+    int seen = 0;
+    while (same && std::fscanf(f, "%15s %15s", kind, prec) == 2) {
+        float *dst = nullptr;
+        const int *shapes = nullptr;
+        if (!std::strcmp(kind, "pbs01") && !std::strcmp(prec, "fp64")) dst = t01[0], shapes = PBS01_SHAPES;
+        else if (!std::strcmp(kind, "pbs01") && !std::strcmp(prec, "split32")) dst = t01[1], shapes = PBS01_SHAPES;
+        else if (!std::strcmp(kind, "pbs02") && !std::strcmp(prec, "fp64")) dst = t02, shapes = PBS02_SHAPES;
+        if (!dst) {
+            ok = false;
+            break;
+        }
+        for (int i = 0; i < NSHAPES && ok; ++i) {
+            int w = 0;
+            ok = std::fscanf(f, "%d %f", &w, &dst[i]) == 2 && w == shapes[i] && dst[i] > 0.0f;
+        }
+        seen |= dst == t02 ? 4 : dst == t01[0] ? 1 : 2;
+    }
+    std::fclose(f);
+    if (!same) return fail(CUFHEDB_ERR_ARG, "autotune table is for another device, SM count or parameter set");
+    if (!ok || seen != 7) return fail(CUFHEDB_ERR_ARG, "malformed autotune table");
+    for (int i = 0; i < NSHAPES; ++i) {
+        ctx->pbs01_pass_ms[0][i] = t01[0][i];
+        ctx->pbs01_pass_ms[1][i] = t01[1][i];
+        ctx->pbs02_pass_ms[i] = t02[i];
+    }
     return CUFHEDB_OK;
 }
 
@@ -908,7 +1064,7 @@ static int pbs02_enqueue(cufhedb_ctx *ctx, const uint32_t *in, uint64_t *out, in
     a.tables = ctx->tab1024;
     a.tv = to_tv(tv);
     a.err = ctx->err;
-    CK(launch_pbs02_f64(a, ctx->num_sms, st));
+    CK(launch_pbs02_f64(a, ctx->num_sms, pbs02_choose_p(B, ctx->num_sms, ctx->pbs02_pass_ms), st));
     return CUFHEDB_OK;
 }
 

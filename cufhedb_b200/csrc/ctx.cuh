@@ -28,9 +28,10 @@ struct cufhedb_ctx {
     cudaStream_t io = nullptr;        // stream of the host-buffer entry points
     std::mutex io_mu;
     bool have_sk = false;
-    // measured time of one pass of the lvl01 PBS kernel with 7 / 8 ciphertexts
-    // per CTA, per precision (FP64, split); equal until cufhedb_autotune runs
-    float pbs01_pass_ms[2][2] = {{1.0f, 1.0f}, {1.0f, 1.0f}};
+    // measured time of one full pass of each launch shape (PBS01_SHAPES per
+    // precision FP64 / split, PBS02_SHAPES); all equal until the autotuner runs
+    float pbs01_pass_ms[2][NSHAPES] = {{1.0f, 1.0f, 1.0f}, {1.0f, 1.0f, 1.0f}};
+    float pbs02_pass_ms[NSHAPES] = {1.0f, 1.0f, 1.0f};
     uint32_t *s0_d = nullptr, *s1_d = nullptr;
     uint64_t *s2_d = nullptr;
     // device address of the allocation-free gate's fixed intermediate

@@ -25,7 +25,8 @@ struct ExtProd2Args {
     const Fft1024Tables *tables;
 };
 
-cudaError_t launch_pbs02_f64(const Pbs02Args &a, int num_sms, cudaStream_t st);
+// p: ciphertexts per CTA, one of PBS02_SHAPES
+cudaError_t launch_pbs02_f64(const Pbs02Args &a, int num_sms, int p, cudaStream_t st);
 cudaError_t init_pbs02_f64();
 cudaError_t launch_extprod2(const ExtProd2Args &a, cudaStream_t st);
 cudaError_t bk02_to_fft(double2 *dst, const uint64_t *src, int rows, const Fft1024Tables *T, cudaStream_t st);

@@ -324,25 +324,44 @@ __global__ void __launch_bounds__(T2) extprod2_kernel(ExtProd2Args a)
     }
 }
 
-constexpr int PBS02_P = 3, PBS02_S = 4;
+// key-ring depth per shape: what the shared memory left by P ciphertexts holds
+template <int P>
+constexpr int PBS02_S = P == 3 ? 4 : P == 2 ? 7 : 8;
 
 }  // namespace
 
-cudaError_t launch_pbs02_f64(const Pbs02Args &a, int num_sms, cudaStream_t st)
+template <int P>
+static cudaError_t launch_pbs02_t(const Pbs02Args &a, int num_sms, cudaStream_t st)
+{
+    using L = Pbs02Smem<P, PBS02_S<P>>;
+    static_assert(L::TOTAL <= 227 * 1024, "shared memory budget");
+    const int groups = (a.B + P - 1) / P;
+    pbs02_f64_kernel<P, PBS02_S<P>><<<groups < num_sms ? groups : num_sms, 4 * P * 32, L::TOTAL, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pbs02_f64(const Pbs02Args &a, int num_sms, int p, cudaStream_t st)
 {
     if (a.B <= 0) return cudaSuccess;
-    using L = Pbs02Smem<PBS02_P, PBS02_S>;
-    static_assert(L::TOTAL <= 227 * 1024, "shared memory budget");
-    const int groups = (a.B + PBS02_P - 1) / PBS02_P;
-    pbs02_f64_kernel<PBS02_P, PBS02_S>
-        <<<groups < num_sms ? groups : num_sms, 4 * PBS02_P * 32, L::TOTAL, st>>>(a);
-    return cudaGetLastError();
+    if (p == 3) return launch_pbs02_t<3>(a, num_sms, st);
+    if (p == 2) return launch_pbs02_t<2>(a, num_sms, st);
+    if (p == 1) return launch_pbs02_t<1>(a, num_sms, st);
+    return cudaErrorInvalidValue;
+}
+
+template <int P>
+static cudaError_t init_pbs02_t()
+{
+    return cudaFuncSetAttribute(pbs02_f64_kernel<P, PBS02_S<P>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                Pbs02Smem<P, PBS02_S<P>>::TOTAL);
 }
 
 cudaError_t init_pbs02_f64()
 {
-    return cudaFuncSetAttribute(pbs02_f64_kernel<PBS02_P, PBS02_S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                Pbs02Smem<PBS02_P, PBS02_S>::TOTAL);
+    cudaError_t e = init_pbs02_t<3>();
+    if (e == cudaSuccess) e = init_pbs02_t<2>();
+    if (e == cudaSuccess) e = init_pbs02_t<1>();
+    return e;
 }
 
 cudaError_t bk02_to_fft(double2 *dst, const uint64_t *src, int rows, const Fft1024Tables *T, cudaStream_t st)

@@ -165,27 +165,40 @@ static cudaError_t launch_pbs01_f64_t(const Pbs01Args &a, int grid, cudaStream_t
 // producer warp), each looping over groups of W ciphertexts.  At most 8 warps
 // keep 2 warps per SM sub-partition, so every thread may hold 255 registers
 // (the 16 complex FFT values plus two 16-complex frequency accumulators per
-// lane).  W = 7 or 8 is chosen per launch (pbs01_choose_w).
-constexpr int PBS01_S = 4;
+// lane).  W = 7, 8 or 4 is chosen per launch (pbs01_choose_w); W = 4 puts one
+// warp on each sub-partition, the shortest pass, with a deeper key ring in
+// the shared memory the fewer warps leave.
+template <int W>
+constexpr int PBS01_S = W == 4 ? 6 : 4;
 
 cudaError_t launch_pbs01_f64(const Pbs01Args &a, int num_sms, int w, cudaStream_t st)
 {
     if (a.B <= 0) return cudaSuccess;
-    static_assert(Pbs01Smem<8, PBS01_S>::TOTAL <= 227 * 1024, "shared memory budget");
+    static_assert(Pbs01Smem<8, PBS01_S<8>>::TOTAL <= 227 * 1024, "shared memory budget");
+    static_assert(Pbs01Smem<4, PBS01_S<4>>::TOTAL <= 227 * 1024, "shared memory budget");
     const int groups = (a.B + w - 1) / w;
     const int grid = groups < num_sms ? groups : num_sms;
-    return w == 7 ? launch_pbs01_f64_t<7, PBS01_S>(a, grid, st) : launch_pbs01_f64_t<8, PBS01_S>(a, grid, st);
+    if (w == 7) return launch_pbs01_f64_t<7, PBS01_S<7>>(a, grid, st);
+    if (w == 8) return launch_pbs01_f64_t<8, PBS01_S<8>>(a, grid, st);
+    if (w == 4) return launch_pbs01_f64_t<4, PBS01_S<4>>(a, grid, st);
+    return cudaErrorInvalidValue;
 }
 
 // the dynamic shared-memory opt-in, set once per device when a context is
 // created (so no attribute call happens inside a stream capture)
+template <int W>
+static cudaError_t init_pbs01_f64_t()
+{
+    return cudaFuncSetAttribute(pbs01_f64_kernel<W, PBS01_S<W>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                Pbs01Smem<W, PBS01_S<W>>::TOTAL);
+}
+
 cudaError_t init_pbs01_f64()
 {
-    cudaError_t e = cudaFuncSetAttribute(pbs01_f64_kernel<7, PBS01_S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         Pbs01Smem<7, PBS01_S>::TOTAL);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(pbs01_f64_kernel<8, PBS01_S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                Pbs01Smem<8, PBS01_S>::TOTAL);
+    cudaError_t e = init_pbs01_f64_t<7>();
+    if (e == cudaSuccess) e = init_pbs01_f64_t<8>();
+    if (e == cudaSuccess) e = init_pbs01_f64_t<4>();
+    return e;
 }
 
 }  // namespace cfdb

@@ -222,20 +222,24 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
     }
 }
 
-// key-ring depth: 7 slots with 7 ciphertexts per CTA (more than one CMux of
-// key rows in flight), 6 with 8 (shared memory)
+// key-ring depth: 7 slots with 7 (or 4) ciphertexts per CTA (more than one
+// CMux of key rows in flight), 6 with 8 (shared memory)
 template <int W>
-constexpr int PBS01S_S = W == 7 ? 7 : 6;
+constexpr int PBS01S_S = W == 8 ? 6 : 7;
 
 template <int W>
 using SplitLayout = Pbs01SplitSmem<W, PBS01S_S<W>, (int)sizeof(Fft512TablesFold)>;
 
-// 7 ciphertexts per CTA run with a producer warp (8 warps), 8 per CTA without
-// one (8 warps): both keep 2 warps per SM sub-partition (up to 255 registers)
+// 7 and 4 ciphertexts per CTA run with a producer warp (8 or 5 warps), 8 per
+// CTA without one (8 warps): at most 2 warps per SM sub-partition (up to 255
+// registers); 4 per CTA leaves one consumer warp per sub-partition
+template <int W>
+constexpr bool PBS01S_PROD = W != 8;
+
 template <int W>
 static cudaError_t launch_pbs01_split_t(const Pbs01Args &a, int grid, cudaStream_t st)
 {
-    constexpr bool PROD = W == 7;
+    constexpr bool PROD = PBS01S_PROD<W>;
     using L = SplitLayout<W>;
     static_assert(L::TOTAL <= 227 * 1024, "shared memory budget");
     pbs01_split_kernel<W, PBS01S_S<W>, PROD><<<grid, (W + (PROD ? 1 : 0)) * 32, L::TOTAL, st>>>(a);
@@ -247,17 +251,25 @@ cudaError_t launch_pbs01_split(const Pbs01Args &a, int num_sms, int w, cudaStrea
     if (a.B <= 0) return cudaSuccess;
     const int groups = (a.B + w - 1) / w;
     const int grid = groups < num_sms ? groups : num_sms;
-    return w == 7 ? launch_pbs01_split_t<7>(a, grid, st) : launch_pbs01_split_t<8>(a, grid, st);
+    if (w == 7) return launch_pbs01_split_t<7>(a, grid, st);
+    if (w == 8) return launch_pbs01_split_t<8>(a, grid, st);
+    if (w == 4) return launch_pbs01_split_t<4>(a, grid, st);
+    return cudaErrorInvalidValue;
+}
+
+template <int W>
+static cudaError_t init_pbs01_split_t()
+{
+    return cudaFuncSetAttribute(pbs01_split_kernel<W, PBS01S_S<W>, PBS01S_PROD<W>>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, SplitLayout<W>::TOTAL);
 }
 
 cudaError_t init_pbs01_split()
 {
-    cudaError_t e = cudaFuncSetAttribute(pbs01_split_kernel<7, PBS01S_S<7>, true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         SplitLayout<7>::TOTAL);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(pbs01_split_kernel<8, PBS01S_S<8>, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                SplitLayout<8>::TOTAL);
+    cudaError_t e = init_pbs01_split_t<7>();
+    if (e == cudaSuccess) e = init_pbs01_split_t<8>();
+    if (e == cudaSuccess) e = init_pbs01_split_t<4>();
+    return e;
 }
 
 }  // namespace cfdb

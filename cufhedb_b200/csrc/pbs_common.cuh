@@ -68,21 +68,46 @@ struct Pbs01Args {
     int *err;
 };
 
-// w: ciphertexts (warps) per CTA, 7 or 8
+// w: ciphertexts (warps) per CTA, one of PBS01_SHAPES
 cudaError_t launch_pbs01_f64(const Pbs01Args &a, int num_sms, int w, cudaStream_t st);
 // bk: split-precision key (float4 hi/lo chunk layout), tables: Fft512TablesF
 cudaError_t launch_pbs01_split(const Pbs01Args &a, int num_sms, int w, cudaStream_t st);
 
-// Launch shape of the lvl01 PBS: each CTA works through ceil(B / w / SMs)
-// passes of w ciphertexts, one pass taking pass_ms[w - 7]; the choice
-// minimises passes x pass time (ties go to w = 7, the lighter pass).
-inline int pbs01_choose_w(int B, int num_sms, const float pass_ms[2])
+// Launch shapes of the persistent PBS kernels, as ciphertexts per CTA: lvl01
+// 7 (with a producer warp on the split path), 8 and 4 (one warp per SM
+// sub-partition: the shortest pass, for batches that leave SMs idle); lvl02
+// 3, 2 and 1 (four warps per ciphertext).  Each CTA works through
+// ceil(ceil(B / w) / SMs) passes of w ciphertexts; the autotuner measures
+// one full pass of every shape, and a launch takes the shape with the least
+// passes x pass time.  Ties go to the earlier shape in the list, so with no
+// measurement (all pass times equal) the fewest passes win and a one-pass
+// batch runs 7 (lvl01) or 3 (lvl02) per CTA.
+constexpr int NSHAPES = 3;
+constexpr int PBS01_SHAPES[NSHAPES] = {7, 8, 4};
+constexpr int PBS02_SHAPES[NSHAPES] = {3, 2, 1};
+
+inline int choose_shape(int B, int num_sms, const int shapes[NSHAPES], const float pass_ms[NSHAPES])
 {
-    auto cost = [&](int w) {
+    int best = 0;
+    float best_cost = 0.0f;
+    for (int i = 0; i < NSHAPES; ++i) {
+        const int w = shapes[i];
         const int groups = (B + w - 1) / w;
-        return (float)((groups + num_sms - 1) / num_sms) * pass_ms[w - 7];
-    };
-    return cost(8) < cost(7) ? 8 : 7;
+        const float cost = (float)((groups + num_sms - 1) / num_sms) * pass_ms[i];
+        if (i == 0 || cost < best_cost) {
+            best = i;
+            best_cost = cost;
+        }
+    }
+    return shapes[best];
+}
+inline int pbs01_choose_w(int B, int num_sms, const float pass_ms[NSHAPES])
+{
+    return choose_shape(B, num_sms, PBS01_SHAPES, pass_ms);
+}
+inline int pbs02_choose_p(int B, int num_sms, const float pass_ms[NSHAPES])
+{
+    return choose_shape(B, num_sms, PBS02_SHAPES, pass_ms);
 }
 cudaError_t init_pbs01_f64();
 cudaError_t init_pbs01_split();

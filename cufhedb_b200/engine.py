@@ -146,11 +146,61 @@ class Engine:
                                             _stream(stream)))
 
     def autotune_pbs01(self, precision: int = _lib.FP64):
-        """time one full pass of the lvl01 PBS with 7 and 8 ciphertexts per CTA;
-        later launches pick the faster shape for their batch.  Returns (ms7, ms8)."""
+        """time one full pass of each lvl01 launch shape (7, 8 and 4
+        ciphertexts per CTA); later launches pick the shape with the least
+        passes x pass time for their batch.  Returns (ms7, ms8)."""
         a, b = C.c_float(0.0), C.c_float(0.0)
         check(self.lib.cufhedb_autotune_pbs01(self.ctx, precision, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def autotune_pbs02(self):
+        """time one full pass of each lvl02 launch shape (3, 2, 1 per CTA);
+        returns the three pass times"""
+        ms = (C.c_float * 3)()
+        check(self.lib.cufhedb_autotune_pbs02(self.ctx, ms))
+        return list(ms)
+
+    def autotune_table(self, level: int, precision: int = _lib.FP64):
+        """{shape: pass time (ms)} of a level's launch shapes in this context"""
+        shapes, ms = (C.c_int * 3)(), (C.c_float * 3)()
+        n = self.lib.cufhedb_autotune_table(self.ctx, level, precision, shapes, ms)
+        if n != 3:
+            check(n)
+        return {int(w): float(t) for w, t in zip(shapes, ms)}
+
+    def launch_shape(self, level: int, precision: int, B: int) -> int:
+        """ciphertexts per CTA a launch of B bootstraps would use now"""
+        w = C.c_int(0)
+        check(self.lib.cufhedb_launch_shape(self.ctx, level, precision, B, C.byref(w)))
+        return w.value
+
+    def autotune_save(self, path: str):
+        check(self.lib.cufhedb_autotune_save(self.ctx, path.encode()))
+
+    def autotune_load(self, path: str) -> bool:
+        """restore pass times saved for this device and parameter set; False
+        (and nothing changed) when the file is missing or made for another"""
+        import os
+        if not os.path.exists(path):
+            return False
+        return self.lib.cufhedb_autotune_load(self.ctx, path.encode()) == 0
+
+    def autotune(self, path: str | None = None, levels=(1, 2)):
+        """the persisted launch-shape table: loaded from `path` when it was made
+        for this device and parameter set, else measured for every loaded key
+        (lvl01 on both precisions, lvl02) and saved to `path`.  Returns
+        {"loaded": bool, "pbs01_fp64": {...}, "pbs01_split32": {...}, "pbs02": {...}}"""
+        loaded = bool(path) and self.autotune_load(path)
+        if not loaded:
+            if 1 in levels:
+                self.autotune_pbs01(_lib.FP64)
+                self.autotune_pbs01(_lib.SPLIT32)
+            if 2 in levels:
+                self.autotune_pbs02()
+            if path:
+                self.autotune_save(path)
+        return {"loaded": loaded, "pbs01_fp64": self.autotune_table(1, _lib.FP64),
+                "pbs01_split32": self.autotune_table(1, _lib.SPLIT32), "pbs02": self.autotune_table(2, _lib.FP64)}
 
     def phase_lvl1(self, ct_dev, phase_dev, key_dev=None, stream=None):
         """decryption phases b - <a, s1> of lvl1 TLWEs (key: device words, or the key set's)"""

@@ -312,14 +312,30 @@ CUFHEDB_API int cufhedb_gate_lvl1_host(cufhedb_ctx *ctx, int gate, const uint32_
 CUFHEDB_API int cufhedb_selftest_wait_timeout(cufhedb_ctx *ctx, uint32_t polls);
 
 /* ---- launch-shape autotuner --------------------------------------------------- */
-/* Times one full pass of the lvl01 PBS kernel (uniform random lvl0 inputs,
- * the loaded key) with 7 and with 8 ciphertexts per CTA for `precision`, and
- * keeps the two pass times in the context: afterwards every lvl01 bootstrap
- * launch (PBS, gates, operator chains) picks the shape with the least
- * (passes x pass time) for its batch size.  Without a run both times count
- * as equal.  Synchronous; call it outside stream capture.  No counterpart in
- * the reference, which runs one ciphertext per launch. */
+/* The persistent PBS kernels come in three launch shapes each (ciphertexts
+ * per CTA): lvl01 7, 8 and 4, lvl02 3, 2 and 1.  A launch of B ciphertexts
+ * takes ceil(ceil(B / shape) / SMs) passes; every launch (PBS, gates,
+ * operator chains) picks the shape with the least passes x measured pass
+ * time, ties to the earlier shape; without measurements all pass times count
+ * as equal.  No counterpart in the reference, which runs one ciphertext per
+ * launch.  The tuning calls are synchronous; call them outside stream capture. */
+/* times one full pass of each lvl01 shape for `precision` (uniform random lvl0
+ * inputs, the loaded key) and keeps them in the context; ms_w7 / ms_w8 (may be
+ * NULL) receive the 7- and 8-per-CTA pass times */
 CUFHEDB_API int cufhedb_autotune_pbs01(cufhedb_ctx *ctx, int precision, float *ms_w7, float *ms_w8);
+/* the same for the lvl02 shapes; ms (may be NULL) receives the 3 pass times */
+CUFHEDB_API int cufhedb_autotune_pbs02(cufhedb_ctx *ctx, float *ms);
+/* the context's table for a level (1 with FP64 or SPLIT32, 2 with FP64):
+ * shapes[3] and pass_ms[3] (either may be NULL); returns 3 */
+CUFHEDB_API int cufhedb_autotune_table(cufhedb_ctx *ctx, int level, int precision, int *shapes, float *pass_ms);
+/* the shape (ciphertexts per CTA) a launch of B ciphertexts would use now */
+CUFHEDB_API int cufhedb_launch_shape(cufhedb_ctx *ctx, int level, int precision, int B, int *shape);
+/* persist / restore the context's pass times: a text file keyed by the device
+ * name, the SM count and a hash of the parameter set and shape lists; load
+ * refuses a table made for anything else (CUFHEDB_ERR_ARG), after which the
+ * caller tunes again */
+CUFHEDB_API int cufhedb_autotune_save(cufhedb_ctx *ctx, const char *path);
+CUFHEDB_API int cufhedb_autotune_load(cufhedb_ctx *ctx, const char *path);
 
 /* ---- diagnostics ------------------------------------------------------------ */
 /* measured CUDA-core FMA throughput (TFLOP/s) of `device`, FP64 (fp64 != 0) or

@@ -75,14 +75,14 @@ inline void arc_one(int op, std::vector<arcedb::TRLWELvl1> &x, std::vector<arced
 inline void arc_gate(int gate, arcedb::TLWELvl1 &res, const arcedb::TLWELvl1 &ca, const arcedb::TLWELvl1 &cb,
                      const arcedb::TFHEEvalKey &ek, uint32_t stream_id)
 {
+    (void)stream_id;   // concurrent calls are coalesced into one batched gate launch
     ensure_ksk(ek, 10);
-    auto &s = op_slots().get(stream_id);
-    h2d(s.a, ca, s.st);
-    h2d(s.c, cb, s.st);
-    check(cufhedb_gate_lvl1(engine(), gate, (const uint32_t *)s.a, (const uint32_t *)s.c, (uint32_t *)s.b, 1,
-                            CUFHEDB_FP64, s.st));
-    d2h(res, s.b, s.st);
-    finish(s.st);
+    const int prec = precision();
+    coalesced_row(Coalescer::Key{OP_GATE, (uint64_t)gate, (uint64_t)prec}, res, ca, &cb,
+                  [&](const void *a, const void *b, void *out, int B, cudaStream_t st) {
+                      return cufhedb_gate_lvl1(engine(), gate, (const uint32_t *)a, (const uint32_t *)b,
+                                               (uint32_t *)out, B, prec, st);
+                  });
 }
 
 // lift_and_and: (c1 + c2 - mu) key-switched to lvl0, bootstrapped with the

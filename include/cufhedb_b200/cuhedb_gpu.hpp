@@ -17,8 +17,14 @@
 // The identity key switches these wrappers ran on the host
 // (TFHEpp::IdentityKeySwitch) run on the GPU: the first call that passes a
 // given TFHEEvalKey uploads its key-switching keys once.  Every call keeps the
-// reference's synchronous, one-row semantics; cuHEDB::batch:: adds the same
-// operators over vectors of rows, which is where the throughput is.
+// reference's synchronous, one-row semantics: it returns when its row's result
+// is in the caller's memory.  Calls of the same operator with the same
+// parameters that arrive together from several host threads (the reference's
+// OpenMP row loops, test/HE3_Query/TPCH_Q6.cu:179-193) are coalesced into one
+// batched launch (cufhedb_dropin::Coalescer); cuHEDB::batch:: takes whole
+// columns at once.  The lvl0 -> lvl1 bootstraps run on the split-precision
+// path unless CUFHEDB_PRECISION=fp64 is set in the environment or
+// cufhedb_dropin::set_precision(CUFHEDB_FP64) is called; lvl2 is FP64.
 //
 // Needs TFHEpp's headers and the HEDB type aliases (HEDB/utils/types.h), the
 // CUDA runtime, and libcufhedb_b200.so at link time.
@@ -28,9 +34,13 @@
 
 #include <array>
 #include <chrono>
+#include <condition_variable>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -150,6 +160,204 @@ inline void d2h(T &dst, const void *src, cudaStream_t st)
 }
 
 inline void finish(cudaStream_t st) { check(cufhedb_sync(engine(), st)); }
+
+// precision of the lvl0 -> lvl1 bootstraps behind the one-row operators
+inline int &precision_setting()
+{
+    static int p = [] {
+        const char *e = std::getenv("CUFHEDB_PRECISION");
+        return (e && std::string(e) == "fp64") ? (int)CUFHEDB_FP64 : (int)CUFHEDB_SPLIT32;
+    }();
+    return p;
+}
+inline int precision() { return precision_setting(); }
+inline void set_precision(int p)
+{
+    if (p != CUFHEDB_FP64 && p != CUFHEDB_SPLIT32) throw std::invalid_argument("cufhedb: unknown precision");
+    precision_setting() = p;
+}
+
+inline long env_long(const char *name, long dflt)
+{
+    const char *e = std::getenv(name);
+    return e ? std::strtol(e, nullptr, 10) : dflt;
+}
+
+// Gathers concurrent one-row calls of one operator (same parameters) into one
+// batched launch.  The first caller of a group is its leader: it keeps the
+// group open while rows keep arriving (each arrival within gap_us of the
+// previous one, at most window_us in all, at most max_rows rows), then closes
+// it, copies every row's inputs to the device in one transfer through pinned
+// staging, runs the batched operator once on its own stream, copies the
+// results back and writes each caller's row.  Every other caller sleeps until
+// its group is done; an error of the batched call is raised in every caller.
+// Several groups (other operators, or the next group of the same operator)
+// run at the same time on separate streams.  Limits come from the environment:
+// CUFHEDB_COALESCE_ROWS (default 8192), CUFHEDB_COALESCE_GAP_US (200) and
+// CUFHEDB_COALESCE_WINDOW_US (2000).
+class Coalescer {
+  public:
+    using Key = std::array<uint64_t, 3>;
+    // fn(in1, in2, out, rows, stream): the batched operator on device buffers
+    using Fn = std::function<int(const void *, const void *, void *, int, cudaStream_t)>;
+
+    static Coalescer &get()
+    {
+        static Coalescer c;
+        return c;
+    }
+
+    void run(const Key &key, const void *in1, const void *in2, size_t in_bytes, void *out, size_t out_bytes,
+             const Fn &fn)
+    {
+        std::unique_lock<std::mutex> lk(mu_);
+        std::shared_ptr<Group> &slot = open_[key];
+        const bool leader = !slot;
+        if (leader) slot = std::make_shared<Group>();
+        std::shared_ptr<Group> g = slot;
+        g->rows.push_back({in1, in2, out});
+        if (!leader) {
+            g->lead_cv.notify_one();
+            g->done_cv.wait(lk, [&] { return g->done; });
+            if (!g->err.empty()) throw std::runtime_error(g->err);
+            return;
+        }
+        using clk = std::chrono::steady_clock;
+        const auto hard = clk::now() + std::chrono::microseconds(window_us_);
+        auto last = clk::now();
+        size_t seen = g->rows.size();
+        while (g->rows.size() < max_rows_) {
+            const auto until = std::min(hard, last + std::chrono::microseconds(gap_us_));
+            g->lead_cv.wait_until(lk, until);
+            const auto now = clk::now();
+            if (g->rows.size() != seen) {
+                seen = g->rows.size();
+                last = now;
+            } else if (now >= until) {
+                break;
+            }
+            if (now >= hard) break;
+        }
+        auto it = open_.find(key);
+        if (it != open_.end() && it->second == g) open_.erase(it);   // later arrivals start a new group
+        Exec *x = take_exec();
+        std::vector<Row> rows = g->rows;
+        lk.unlock();
+        std::string err = execute(*x, rows, in_bytes, out_bytes, fn);
+        lk.lock();
+        idle_.push_back(x);
+        g->err = err;
+        g->done = true;
+        g->done_cv.notify_all();
+        if (!err.empty()) throw std::runtime_error(err);
+    }
+
+    ~Coalescer()
+    {
+        for (Exec *x : idle_) {
+            if (x->st) cudaStreamDestroy(x->st);
+            cudaFreeHost(x->h);
+            delete x;
+        }
+    }
+
+  private:
+    struct Row {
+        const void *in1, *in2;
+        void *out;
+    };
+    struct Group {
+        std::vector<Row> rows;
+        bool done = false;
+        std::string err;
+        std::condition_variable lead_cv, done_cv;
+    };
+    // a stream and pinned staging for one executing group
+    struct Exec {
+        cudaStream_t st = nullptr;
+        unsigned char *h = nullptr;
+        size_t cap = 0;
+    };
+
+    Coalescer()
+        : max_rows_((size_t)env_long("CUFHEDB_COALESCE_ROWS", 8192)),
+          gap_us_(env_long("CUFHEDB_COALESCE_GAP_US", 200)),
+          window_us_(env_long("CUFHEDB_COALESCE_WINDOW_US", 2000))
+    {
+        if (max_rows_ < 1) max_rows_ = 1;
+    }
+
+    Exec *take_exec()
+    {
+        if (!idle_.empty()) {
+            Exec *x = idle_.back();
+            idle_.pop_back();
+            return x;
+        }
+        return new Exec();
+    }
+
+    static std::string execute(Exec &x, const std::vector<Row> &rows, size_t in_bytes, size_t out_bytes,
+                               const Fn &fn)
+    {
+        try {
+            cufhedb_ctx *ctx = engine();
+            if (!x.st) check_cuda(cudaStreamCreateWithFlags(&x.st, cudaStreamNonBlocking));
+            const size_t n = rows.size();
+            const bool two = rows[0].in2 != nullptr;
+            const size_t in_total = n * in_bytes * (two ? 2 : 1), total = in_total + n * out_bytes;
+            if (x.cap < total) {
+                cudaFreeHost(x.h);
+                x.h = nullptr;
+                x.cap = 0;
+                check_cuda(cudaMallocHost((void **)&x.h, total));
+                x.cap = total;
+            }
+            for (size_t i = 0; i < n; i++) {
+                std::memcpy(x.h + i * in_bytes, rows[i].in1, in_bytes);
+                if (two) std::memcpy(x.h + (n + i) * in_bytes, rows[i].in2, in_bytes);
+            }
+            unsigned char *d = nullptr;
+            check_cuda(cudaMallocAsync((void **)&d, total, x.st));
+            int rc = CUFHEDB_OK;
+            cudaError_t e = cudaMemcpyAsync(d, x.h, in_total, cudaMemcpyHostToDevice, x.st);
+            if (e == cudaSuccess)
+                rc = fn(d, two ? d + n * in_bytes : nullptr, d + in_total, (int)n, x.st);
+            std::string msg = rc == CUFHEDB_OK ? "" : std::string("cufhedb: ") + cufhedb_last_error();
+            if (e == cudaSuccess && rc == CUFHEDB_OK)
+                e = cudaMemcpyAsync(x.h + in_total, d + in_total, n * out_bytes, cudaMemcpyDeviceToHost, x.st);
+            cudaFreeAsync(d, x.st);
+            if (e != cudaSuccess) return std::string("cufhedb (CUDA): ") + cudaGetErrorString(e);
+            if (!msg.empty()) {
+                cudaStreamSynchronize(x.st);
+                return msg;
+            }
+            if (cufhedb_sync(ctx, x.st) != CUFHEDB_OK) return std::string("cufhedb: ") + cufhedb_last_error();
+            for (size_t i = 0; i < n; i++) std::memcpy(rows[i].out, x.h + in_total + i * out_bytes, out_bytes);
+            return "";
+        } catch (const std::exception &ex) {
+            return ex.what();
+        }
+    }
+
+    std::mutex mu_;
+    std::map<Key, std::shared_ptr<Group>> open_;
+    std::vector<Exec *> idle_;
+    size_t max_rows_;
+    long gap_us_, window_us_;
+};
+
+// one row through the coalescer: `in2` may be null (one-input operators)
+template <typename In, typename Out>
+inline void coalesced_row(const Coalescer::Key &key, Out &res, const In &in1, const In *in2, const Coalescer::Fn &fn)
+{
+    Coalescer::get().run(key, in1.data(), in2 ? in2->data() : nullptr, sizeof(In), res.data(), sizeof(Out), fn);
+}
+
+// operator codes of the coalescing keys
+enum : uint64_t {
+    OP_PBS = 1, OP_MSB, OP_IDE, OP_AND, OP_OR, OP_LOG2ARI, OP_RESCALE, OP_HOMMSB, OP_COMPARE, OP_GATE
+};
 
 }  // namespace cufhedb_dropin
 
@@ -297,7 +505,7 @@ class CuFFT_Torus {
     // batched bootstraps: B lvl0 inputs -> B outputs in one launch
     void GateBootstrappingTLWE2TLWEFFT_batch(std::vector<std::array<typename P::T, P::n + 1>> &out,
                                              const std::vector<std::array<uint32_t, 673>> &in, const typename P::T u,
-                                             int precision = CUFHEDB_FP64)
+                                             int precision = cufhedb_dropin::precision())
     {
         out.resize(in.size());
         if (in.empty()) return;
@@ -343,16 +551,22 @@ class CuFFT_Torus {
     void pbs(std::array<typename P::T, P::n + 1> &tlwe, std::array<uint32_t, 673> &poly, const cufhedb_testvec &tv,
              uint32_t stream_id)
     {
-        auto &s = slots_.get(stream_id);
-        cufhedb_dropin::h2d(s.a, poly, s.st);
-        if constexpr (P::n == 1024)
-            cufhedb_dropin::check(cufhedb_pbs_lvl01(cufhedb_dropin::engine(), (const uint32_t *)s.a,
-                                                    (uint32_t *)s.b, 1, &tv, CUFHEDB_FP64, s.st));
-        else
-            cufhedb_dropin::check(cufhedb_pbs_lvl02(cufhedb_dropin::engine(), (const uint32_t *)s.a,
-                                                    (uint64_t *)s.b, 1, &tv, s.st));
-        cufhedb_dropin::d2h(tlwe, s.b, s.st);
-        cufhedb_dropin::finish(s.st);
+        (void)stream_id;   // concurrent calls are coalesced; each returns with its own result
+        const int prec = cufhedb_dropin::precision();
+        const cufhedb_dropin::Coalescer::Key key{
+            cufhedb_dropin::OP_PBS, ((uint64_t)P::n << 32) | ((uint64_t)tv.kind << 16) | ((uint64_t)tv.pad_bits << 8) |
+                                        (uint64_t)prec,
+            tv.value};
+        cufhedb_dropin::coalesced_row(
+            key, tlwe, poly, (const std::array<uint32_t, 673> *)nullptr,
+            [&](const void *in, const void *, void *out, int B, cudaStream_t st) {
+                if constexpr (P::n == 1024)
+                    return cufhedb_pbs_lvl01(cufhedb_dropin::engine(), (const uint32_t *)in, (uint32_t *)out, B,
+                                             &tv, prec, st);
+                else
+                    return cufhedb_pbs_lvl02(cufhedb_dropin::engine(), (const uint32_t *)in, (uint64_t *)out, B,
+                                             &tv, st);
+            });
     }
 
     template <typename F>
@@ -387,15 +601,33 @@ using HEDB::TLWELvl2;
 
 namespace detail {
 
-// runs one operator on one row through the per-stream_id staging
+using cufhedb_dropin::Coalescer;
+
+// one row of a one-input operator, coalesced with concurrent calls of the same
+// operator and parameters (the stream id orders nothing: the call is complete
+// when it returns, as in the reference)
 template <typename In, typename Out, typename F>
-inline void one_row(Out &res, const In &in, uint32_t stream_id, F &&op)
+inline void one_row(const Coalescer::Key &key, Out &res, const In &in, F &&op)
 {
-    auto &s = cufhedb_dropin::op_slots().get(stream_id);
-    cufhedb_dropin::h2d(s.a, in, s.st);
-    cufhedb_dropin::check(op(s.a, s.b, s.st));
-    cufhedb_dropin::d2h(res, s.b, s.st);
-    cufhedb_dropin::finish(s.st);
+    cufhedb_dropin::coalesced_row(key, res, in, (const In *)nullptr,
+                                  [&](const void *a, const void *, void *o, int B, cudaStream_t st) {
+                                      return op(a, o, B, st);
+                                  });
+}
+
+// one row of a two-input operator
+template <typename In, typename Out, typename F>
+inline void two_rows(const Coalescer::Key &key, Out &res, const In &a, const In &b, F &&op)
+{
+    cufhedb_dropin::coalesced_row(key, res, a, &b,
+                                  [&](const void *x, const void *y, void *o, int B, cudaStream_t st) {
+                                      return op(x, y, o, B, st);
+                                  });
+}
+
+inline Coalescer::Key key(uint64_t op, uint64_t a, uint64_t b = 0)
+{
+    return {op, a, (b << 1) | (uint64_t)cufhedb_dropin::precision()};
 }
 
 template <typename P>
@@ -407,59 +639,41 @@ constexpr int level()
 }  // namespace detail
 
 // ---- gatebootstrap_gpu.cuh ---------------------------------------------------
-inline void MSBGateBootstrapping(TLWELvl1 &res, const TLWELvl1 &tlwe, const TFHEEvalKey &ek, bool result_type,
-                                 uint32_t stream_id)
-{
-    cufhedb_dropin::ensure_ksk(ek, 10);
-    detail::one_row(res, tlwe, stream_id, [&](void *in, void *out, cudaStream_t st) {
-        return cufhedb_msb_bootstrap(cufhedb_dropin::engine(), 1, 1, in, out, 1, result_type, CUFHEDB_FP64, st);
-    });
-}
+#define CUFHEDB_MSB_ROW(RES, IN, LIN, LOUT, KSK)                                                              \
+    inline void MSBGateBootstrapping(RES &res, const IN &tlwe, const TFHEEvalKey &ek, bool result_type,       \
+                                     uint32_t stream_id)                                                      \
+    {                                                                                                         \
+        (void)stream_id;                                                                                      \
+        cufhedb_dropin::ensure_ksk(ek, KSK);                                                                  \
+        const int prec = cufhedb_dropin::precision();                                                         \
+        detail::one_row(detail::key(cufhedb_dropin::OP_MSB, LIN * 16 + LOUT, result_type), res, tlwe,        \
+                        [&](const void *in, void *out, int B, cudaStream_t st) {                              \
+                            return cufhedb_msb_bootstrap(cufhedb_dropin::engine(), LIN, LOUT, in, out, B,     \
+                                                         result_type, prec, st);                              \
+                        });                                                                                   \
+    }
+CUFHEDB_MSB_ROW(TLWELvl1, TLWELvl1, 1, 1, 10)
+CUFHEDB_MSB_ROW(TLWELvl1, TLWELvl2, 2, 1, 20)
+CUFHEDB_MSB_ROW(TLWELvl2, TLWELvl2, 2, 2, 20)
+#undef CUFHEDB_MSB_ROW
 
-inline void MSBGateBootstrapping(TLWELvl1 &res, const TLWELvl2 &tlwe, const TFHEEvalKey &ek, bool result_type,
-                                 uint32_t stream_id)
-{
-    cufhedb_dropin::ensure_ksk(ek, 20);
-    detail::one_row(res, tlwe, stream_id, [&](void *in, void *out, cudaStream_t st) {
-        return cufhedb_msb_bootstrap(cufhedb_dropin::engine(), 2, 1, in, out, 1, result_type, CUFHEDB_FP64, st);
-    });
-}
-
-inline void MSBGateBootstrapping(TLWELvl2 &res, const TLWELvl2 &tlwe, const TFHEEvalKey &ek, bool result_type,
-                                 uint32_t stream_id)
-{
-    cufhedb_dropin::ensure_ksk(ek, 20);
-    detail::one_row(res, tlwe, stream_id, [&](void *in, void *out, cudaStream_t st) {
-        return cufhedb_msb_bootstrap(cufhedb_dropin::engine(), 2, 2, in, out, 1, result_type, CUFHEDB_FP64, st);
-    });
-}
-
-inline void IdeGateBootstrapping(TLWELvl1 &res, const TLWELvl1 &tlwe, uint32_t scale_bits, const TFHEEvalKey &ek,
-                                 uint32_t stream_id)
-{
-    cufhedb_dropin::ensure_ksk(ek, 10);
-    detail::one_row(res, tlwe, stream_id, [&](void *in, void *out, cudaStream_t st) {
-        return cufhedb_ide_bootstrap(cufhedb_dropin::engine(), 1, 1, in, out, 1, scale_bits, CUFHEDB_FP64, st);
-    });
-}
-
-inline void IdeGateBootstrapping(TLWELvl1 &res, const TLWELvl2 &tlwe, uint32_t scale_bits, const TFHEEvalKey &ek,
-                                 uint32_t stream_id)
-{
-    cufhedb_dropin::ensure_ksk(ek, 20);
-    detail::one_row(res, tlwe, stream_id, [&](void *in, void *out, cudaStream_t st) {
-        return cufhedb_ide_bootstrap(cufhedb_dropin::engine(), 2, 1, in, out, 1, scale_bits, CUFHEDB_FP64, st);
-    });
-}
-
-inline void IdeGateBootstrapping(TLWELvl2 &res, const TLWELvl2 &tlwe, uint32_t scale_bits, const TFHEEvalKey &ek,
-                                 uint32_t stream_id)
-{
-    cufhedb_dropin::ensure_ksk(ek, 20);
-    detail::one_row(res, tlwe, stream_id, [&](void *in, void *out, cudaStream_t st) {
-        return cufhedb_ide_bootstrap(cufhedb_dropin::engine(), 2, 2, in, out, 1, scale_bits, CUFHEDB_FP64, st);
-    });
-}
+#define CUFHEDB_IDE_ROW(RES, IN, LIN, LOUT, KSK)                                                              \
+    inline void IdeGateBootstrapping(RES &res, const IN &tlwe, uint32_t scale_bits, const TFHEEvalKey &ek,    \
+                                     uint32_t stream_id)                                                      \
+    {                                                                                                         \
+        (void)stream_id;                                                                                      \
+        cufhedb_dropin::ensure_ksk(ek, KSK);                                                                  \
+        const int prec = cufhedb_dropin::precision();                                                         \
+        detail::one_row(detail::key(cufhedb_dropin::OP_IDE, LIN * 16 + LOUT, scale_bits), res, tlwe,         \
+                        [&](const void *in, void *out, int B, cudaStream_t st) {                              \
+                            return cufhedb_ide_bootstrap(cufhedb_dropin::engine(), LIN, LOUT, in, out, B,     \
+                                                         scale_bits, prec, st);                               \
+                        });                                                                                   \
+    }
+CUFHEDB_IDE_ROW(TLWELvl1, TLWELvl1, 1, 1, 10)
+CUFHEDB_IDE_ROW(TLWELvl1, TLWELvl2, 2, 1, 20)
+CUFHEDB_IDE_ROW(TLWELvl2, TLWELvl2, 2, 2, 20)
+#undef CUFHEDB_IDE_ROW
 
 template <typename P>
 inline void HomNOT(TFHEpp::TLWE<P> &res, const TFHEpp::TLWE<P> &tlwe)
@@ -470,71 +684,83 @@ inline void HomNOT(TFHEpp::TLWE<P> &res, const TFHEpp::TLWE<P> &tlwe)
 inline void HomAND(TLWELvl1 &res, const TLWELvl1 &ca, const TLWELvl1 &cb, const TFHEEvalKey &ek, bool result_type,
                    uint32_t stream_id)
 {
+    (void)stream_id;
     cufhedb_dropin::ensure_ksk(ek, 10);
-    auto &s = cufhedb_dropin::op_slots().get(stream_id);
-    cufhedb_dropin::h2d(s.a, ca, s.st);
-    cufhedb_dropin::h2d(s.c, cb, s.st);
-    cufhedb_dropin::check(cufhedb_hom_and(cufhedb_dropin::engine(), (const uint32_t *)s.a, (const uint32_t *)s.c,
-                                          (uint32_t *)s.b, 1, result_type, CUFHEDB_FP64, s.st));
-    cufhedb_dropin::d2h(res, s.b, s.st);
-    cufhedb_dropin::finish(s.st);
+    const int prec = cufhedb_dropin::precision();
+    detail::two_rows(detail::key(cufhedb_dropin::OP_AND, 0, result_type), res, ca, cb,
+                     [&](const void *a, const void *b, void *out, int B, cudaStream_t st) {
+                         return cufhedb_hom_and(cufhedb_dropin::engine(), (const uint32_t *)a, (const uint32_t *)b,
+                                                (uint32_t *)out, B, result_type, prec, st);
+                     });
 }
 
 inline void HomOR(TLWELvl1 &res, const TLWELvl1 &ca, const TLWELvl1 &cb, const TFHEEvalKey &ek, bool result_type,
                   uint32_t stream_id)
 {
+    (void)stream_id;
     cufhedb_dropin::ensure_ksk(ek, 10);
-    auto &s = cufhedb_dropin::op_slots().get(stream_id);
-    cufhedb_dropin::h2d(s.a, ca, s.st);
-    cufhedb_dropin::h2d(s.c, cb, s.st);
-    cufhedb_dropin::check(cufhedb_hom_or(cufhedb_dropin::engine(), (const uint32_t *)s.a, (const uint32_t *)s.c,
-                                         (uint32_t *)s.b, 1, result_type, CUFHEDB_FP64, s.st));
-    cufhedb_dropin::d2h(res, s.b, s.st);
-    cufhedb_dropin::finish(s.st);
+    const int prec = cufhedb_dropin::precision();
+    detail::two_rows(detail::key(cufhedb_dropin::OP_OR, 0, result_type), res, ca, cb,
+                     [&](const void *a, const void *b, void *out, int B, cudaStream_t st) {
+                         return cufhedb_hom_or(cufhedb_dropin::engine(), (const uint32_t *)a, (const uint32_t *)b,
+                                               (uint32_t *)out, B, result_type, prec, st);
+                     });
 }
 
 inline void LOG_to_ARI(TLWELvl1 &res, const TLWELvl1 &tlwe, const TFHEEvalKey &ek, uint32_t stream_id)
 {
+    (void)stream_id;
     cufhedb_dropin::ensure_ksk(ek, 10);
-    detail::one_row(res, tlwe, stream_id, [&](void *in, void *out, cudaStream_t st) {
-        return cufhedb_log_to_ari(cufhedb_dropin::engine(), (const uint32_t *)in, (uint32_t *)out, 1, CUFHEDB_FP64,
-                                  st);
-    });
+    const int prec = cufhedb_dropin::precision();
+    detail::one_row(detail::key(cufhedb_dropin::OP_LOG2ARI, 0), res, tlwe,
+                    [&](const void *in, void *out, int B, cudaStream_t st) {
+                        return cufhedb_log_to_ari(cufhedb_dropin::engine(), (const uint32_t *)in, (uint32_t *)out,
+                                                  B, prec, st);
+                    });
 }
 
 inline void log_rescale(TLWELvl1 &res, const TLWELvl1 &tlwe, uint32_t scale_bits, const TFHEEvalKey &ek,
                         uint32_t stream_id)
 {
+    (void)stream_id;
     cufhedb_dropin::ensure_ksk(ek, 10);
-    detail::one_row(res, tlwe, stream_id, [&](void *in, void *out, cudaStream_t st) {
-        return cufhedb_log_rescale(cufhedb_dropin::engine(), (const uint32_t *)in, (uint32_t *)out, 1, scale_bits,
-                                   CUFHEDB_FP64, st);
-    });
+    const int prec = cufhedb_dropin::precision();
+    detail::one_row(detail::key(cufhedb_dropin::OP_RESCALE, 0, scale_bits), res, tlwe,
+                    [&](const void *in, void *out, int B, cudaStream_t st) {
+                        return cufhedb_log_rescale(cufhedb_dropin::engine(), (const uint32_t *)in, (uint32_t *)out,
+                                                   B, scale_bits, prec, st);
+                    });
 }
 
 // ---- msb_gpu.cuh ---------------------------------------------------------------
 inline void HomMSB(TLWELvl1 &res, const TLWELvl1 &tlwe, uint32_t plain_bits, const TFHEEvalKey &ek,
                    bool result_type, uint32_t stream_id)
 {
+    (void)stream_id;
     if (plain_bits > 10) throw std::invalid_argument("Plain bits out. ");
     cufhedb_dropin::ensure_ksk(ek, 10);
-    detail::one_row(res, tlwe, stream_id, [&](void *in, void *out, cudaStream_t st) {
-        return cufhedb_hom_msb(cufhedb_dropin::engine(), 1, in, (uint32_t *)out, 1, plain_bits, result_type,
-                               CUFHEDB_FP64, st);
-    });
+    const int prec = cufhedb_dropin::precision();
+    detail::one_row(detail::key(cufhedb_dropin::OP_HOMMSB, 1, plain_bits * 2 + result_type), res, tlwe,
+                    [&](const void *in, void *out, int B, cudaStream_t st) {
+                        return cufhedb_hom_msb(cufhedb_dropin::engine(), 1, in, (uint32_t *)out, B, plain_bits,
+                                               result_type, prec, st);
+                    });
 }
 
 inline void HomMSB(TLWELvl1 &res, const TLWELvl2 &tlwe, uint32_t plain_bits, const TFHEEvalKey &ek,
                    bool result_type, uint32_t stream_id)
 {
+    (void)stream_id;
     if (plain_bits > 33) throw std::invalid_argument("Plain bits out. ");
     cufhedb_dropin::ensure_ksk(ek, 10);
     cufhedb_dropin::ensure_ksk(ek, 20);
     cufhedb_dropin::ensure_ksk(ek, 21);
-    detail::one_row(res, tlwe, stream_id, [&](void *in, void *out, cudaStream_t st) {
-        return cufhedb_hom_msb(cufhedb_dropin::engine(), 2, in, (uint32_t *)out, 1, plain_bits, result_type,
-                               CUFHEDB_FP64, st);
-    });
+    const int prec = cufhedb_dropin::precision();
+    detail::one_row(detail::key(cufhedb_dropin::OP_HOMMSB, 2, plain_bits * 2 + result_type), res, tlwe,
+                    [&](const void *in, void *out, int B, cudaStream_t st) {
+                        return cufhedb_hom_msb(cufhedb_dropin::engine(), 2, in, (uint32_t *)out, B, plain_bits,
+                                               result_type, prec, st);
+                    });
 }
 
 inline void ExtractMSB5(TLWELvl1 &res, const TLWELvl1 &tlwe, const TFHEEvalKey &ek, bool result_type,
@@ -596,18 +822,18 @@ template <typename P>
 inline void compare(int op, TFHEpp::TLWE<P> &c1, TFHEpp::TLWE<P> &c2, TLWELvl1 &res, uint32_t plain_bits,
                     const TFHEEvalKey &ek, bool result_type, uint32_t stream_id)
 {
+    (void)stream_id;
     cufhedb_dropin::ensure_ksk(ek, 10);
     if (level<P>() == 2) {
         cufhedb_dropin::ensure_ksk(ek, 20);
         cufhedb_dropin::ensure_ksk(ek, 21);
     }
-    auto &s = cufhedb_dropin::op_slots().get(stream_id);
-    cufhedb_dropin::h2d(s.a, c1, s.st);
-    cufhedb_dropin::h2d(s.c, c2, s.st);
-    cufhedb_dropin::check(cufhedb_compare(cufhedb_dropin::engine(), op, level<P>(), s.a, s.c, (uint32_t *)s.b, 1,
-                                          plain_bits, result_type, CUFHEDB_FP64, s.st));
-    cufhedb_dropin::d2h(res, s.b, s.st);
-    cufhedb_dropin::finish(s.st);
+    const int prec = cufhedb_dropin::precision();
+    two_rows(key(cufhedb_dropin::OP_COMPARE, (uint64_t)op * 16 + level<P>(), plain_bits * 2 + result_type), res, c1,
+             c2, [&](const void *a, const void *b, void *out, int B, cudaStream_t st) {
+                 return cufhedb_compare(cufhedb_dropin::engine(), op, level<P>(), a, b, (uint32_t *)out, B,
+                                        plain_bits, result_type, prec, st);
+             });
 }
 }  // namespace detail
 
@@ -653,7 +879,7 @@ namespace batch {
 template <typename P>
 void compare(int op, const std::vector<TFHEpp::TLWE<P>> &c1, const std::vector<TFHEpp::TLWE<P>> &c2,
              std::vector<TLWELvl1> &res, uint32_t plain_bits, const TFHEEvalKey &ek, bool result_type,
-             int precision = CUFHEDB_FP64)
+             int precision = cufhedb_dropin::precision())
 {
     if (c1.size() != c2.size()) throw std::invalid_argument("cufhedb: column sizes differ");
     res.resize(c1.size());
@@ -683,7 +909,7 @@ void compare(int op, const std::vector<TFHEpp::TLWE<P>> &c1, const std::vector<T
 }
 
 inline void HomAND(std::vector<TLWELvl1> &res, const std::vector<TLWELvl1> &ca, const std::vector<TLWELvl1> &cb,
-                   const TFHEEvalKey &ek, bool result_type, int precision = CUFHEDB_FP64)
+                   const TFHEEvalKey &ek, bool result_type, int precision = cufhedb_dropin::precision())
 {
     if (ca.size() != cb.size()) throw std::invalid_argument("cufhedb: column sizes differ");
     res.resize(ca.size());

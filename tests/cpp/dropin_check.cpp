@@ -293,6 +293,65 @@ void check_batch_compare(std::mt19937_64 &rng, const TFHESecretKey &sk, const TF
     report(what.c_str(), bad == 0, buf);
 }
 
+// The reference's query programs' row loop (test/HE3_Query/TPCH_Q6.cu:179-193):
+// `omp parallel for num_threads(T)`, every thread calling the one-row
+// operator with its own stream id, each call returning with its row's result.
+// parallel_rows() is that loop's static schedule on T host threads (thread t
+// takes the t-th contiguous block of rows, stream id t).
+// Concurrent calls are coalesced into batched launches; here the rows per
+// second through that unchanged API are set beside cuHEDB::batch::compare on
+// the same rows, and every result of both is decrypted against plaintext.
+template <typename F>
+void parallel_rows(int rows, int threads, F &&f)
+{
+    std::vector<std::thread> th;
+    for (int t = 0; t < threads; t++)
+        th.emplace_back([&, t] {
+            const int lo = (int)((long)rows * t / threads), hi = (int)((long)rows * (t + 1) / threads);
+            for (int i = lo; i < hi; i++) f(i, (uint32_t)t);
+        });
+    for (auto &x : th) x.join();
+}
+
+template <class P>
+void check_row_loop(std::mt19937_64 &rng, const TFHESecretKey &sk, TFHEEvalKey &ek, uint32_t bits, int rows,
+                    int threads)
+{
+    const uint64_t mask = (1ull << bits) - 1;
+    const uint64_t c = rng() & mask;
+    auto cthr = enc_int<P>((typename P::T)c, bits, sk);
+    std::vector<TFHEpp::TLWE<P>> col(rows), thr(rows, cthr);
+    std::vector<uint64_t> x(rows);
+    for (int i = 0; i < rows; i++) {
+        x[i] = rng() & mask;
+        col[i] = enc_int<P>((typename P::T)x[i], bits, sk);
+    }
+    std::vector<TLWELvl1> res(rows);
+    // warm-up: one round of `threads` rows
+    parallel_rows(std::min(threads, rows), threads, [&](int i, uint32_t sid) {
+        cuHEDB::less_than_equal<P>(col[i], thr[i], res[i], bits, ek, LOGIC, sid);
+    });
+    auto t0 = std::chrono::steady_clock::now();
+    parallel_rows(rows, threads, [&](int i, uint32_t sid) {
+        cuHEDB::less_than_equal<P>(col[i], thr[i], res[i], bits, ek, LOGIC, sid);
+    });
+    const double s_rows = seconds_since(t0);
+    int bad = 0;
+    for (int i = 0; i < rows; i++) bad += dec_logic(res[i], sk) != (x[i] <= c);
+    std::vector<TLWELvl1> bres;
+    t0 = std::chrono::steady_clock::now();
+    cuHEDB::batch::compare<P>(3, col, thr, bres, bits, ek, LOGIC);
+    const double s_batch = seconds_since(t0);
+    int bad_batch = 0;
+    for (int i = 0; i < rows; i++) bad_batch += dec_logic(bres[i], sk) != (x[i] <= c);
+    char buf[160];
+    std::snprintf(buf, sizeof buf, "%.0f rows/s one-row calls, %.0f rows/s batch (ratio %.2f)", rows / s_rows,
+                  rows / s_batch, s_rows / s_batch);
+    std::string what = std::string("row loop: ") + std::to_string(threads) + " threads x " + std::to_string(rows) +
+                       " less_than_equal<Lvl" + (P::n == 1024 ? "1" : "2") + "> " + std::to_string(bits) + " bits";
+    report(what.c_str(), bad == 0 && bad_batch == 0, buf);
+}
+
 void check_pbs02(std::mt19937_64 &rng, const TFHESecretKey &sk)
 {
     int bad = 0;
@@ -378,6 +437,8 @@ int main(int argc, char **argv)
         check_batch_compare<Lvl1>(rng, *sk, *ek, 6, 512, CUFHEDB_FP64);
         check_batch_compare<Lvl1>(rng, *sk, *ek, 6, 512, CUFHEDB_SPLIT32);
         check_threads(*sk, *ek);
+        check_row_loop<Lvl1>(rng, *sk, *ek, 6, 16384, 48);
+        check_row_loop<Lvl1>(rng, *sk, *ek, 6, 16384, 1024);
         if (lvl2) {
             check_pbs02(rng, *sk);
             check_compare<Lvl2>(rng, *sk, *ek, 20, 3, 1);
@@ -385,6 +446,8 @@ int main(int argc, char **argv)
             // the noise floor of the lvl2 parameters with randomly drawn keys
             check_compare<Lvl2>(rng, *sk, *ek, 26, 2, 0);
             check_batch_compare<Lvl2>(rng, *sk, *ek, 20, 256, CUFHEDB_FP64);
+            check_row_loop<Lvl2>(rng, *sk, *ek, 20, 4096, 48);
+            check_row_loop<Lvl2>(rng, *sk, *ek, 20, 4096, 1024);
         }
     } catch (const std::exception &e) {
         std::printf("exception: %s\n", e.what());

@@ -1,11 +1,13 @@
-"""Launch-shape choice of the lvl01 PBS (pbs01_choose_w in csrc/pbs_common.cuh),
-checked without a GPU.
+"""Launch-shape choice of the persistent PBS kernels (choose_shape in
+csrc/pbs_common.cuh), checked without a GPU.
 
-Each CTA works through ceil(B / w / SMs) passes of w ciphertexts (w = 7 with a
-producer warp, w = 8 without); the autotuner measures one pass of each shape,
-and the launch picks the shape with the smaller passes x pass time, ties to
-w = 7.  The header function is compiled for the host with nvcc and its
-choices compared with that rule and with hand-worked cases on 148 SMs.
+A kernel runs in one of three shapes, w ciphertexts per CTA (lvl01: 7, 8, 4;
+lvl02: 3, 2, 1).  Each CTA works through ceil(ceil(B / w) / SMs) passes of w
+ciphertexts; the autotuner measures one full pass of each shape, and a launch
+picks the shape with the least passes x pass time, ties to the earlier shape
+in the list.  The header functions are compiled for the host with nvcc and
+their choices compared with that rule for every batch up to 20,000 and with
+hand-worked cases on 148 SMs.
 """
 import os
 import shutil
@@ -16,19 +18,29 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, "cufhedb_b200", "csrc")
 SMS = 148
-PASS = {"untuned": (0.0, 0.0), "split": (9.40, 10.50), "fp64": (14.28, 14.54), "w8_faster": (10.0, 9.0)}
+SHAPES = {1: (7, 8, 4), 2: (3, 2, 1)}
+# pass times (ms) per shape, in list order: the context's untuned default,
+# figures of the order measured on B200, and a case where the wide shape wins
+PASS = {
+    1: {"untuned": (1.0, 1.0, 1.0), "split": (9.40, 10.50, 6.0), "fp64": (14.28, 14.54, 9.0),
+        "w8_faster": (10.0, 9.0, 9.5)},
+    2: {"untuned": (1.0, 1.0, 1.0), "f64": (17.7, 13.5, 8.0)},
+}
 BMAX = 20000
 
 PROG = r"""
 #include "pbs_common.cuh"
 #include <cstdio>
+#include <cstdlib>
 int main(int argc, char **argv)
 {
-    const float pass_ms[2] = {(float)atof(argv[1]), (float)atof(argv[2])};
-    for (int B = 1; B <= %d; ++B) std::printf("%%d\n", cfdb::pbs01_choose_w(B, %d, pass_ms));
+    const int level = atoi(argv[1]);
+    const float pass_ms[3] = {(float)atof(argv[2]), (float)atof(argv[3]), (float)atof(argv[4])};
+    for (int B = 1; B <= %d; ++B)
+        std::printf("%%d\n", level == 1 ? cfdb::pbs01_choose_w(B, %d, pass_ms) : cfdb::pbs02_choose_p(B, %d, pass_ms));
     return 0;
 }
-""" % (BMAX, SMS)
+""" % (BMAX, SMS, SMS)
 
 
 def _nvcc():
@@ -50,35 +62,47 @@ def choices(tmp_path_factory):
                         str(src)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]
     out = {}
-    for name, (p7, p8) in PASS.items():
-        res = subprocess.run([str(exe), repr(p7), repr(p8)], capture_output=True, text=True, timeout=60)
-        out[name] = [int(x) for x in res.stdout.split()]
-        assert len(out[name]) == BMAX
+    for level, cases in PASS.items():
+        for name, t in cases.items():
+            res = subprocess.run([str(exe), str(level), *map(repr, t)], capture_output=True, text=True, timeout=60)
+            out[level, name] = [int(x) for x in res.stdout.split()]
+            assert len(out[level, name]) == BMAX
     return out
 
 
-def _rule(B, p7, p8):
-    cost = lambda w, p: -(-(-(-B // w)) // SMS) * p   # ceil(ceil(B / w) / SMS) passes x pass time
-    return 8 if cost(8, p8) < cost(7, p7) else 7
+def _rule(B, shapes, t):
+    costs = [-(-(-(-B // w)) // SMS) * p for w, p in zip(shapes, t)]   # passes x pass time
+    return shapes[costs.index(min(costs))]                             # first minimum: ties to the earlier
 
 
 def test_choice_follows_the_rule_for_every_batch(choices):
-    for name, (p7, p8) in PASS.items():
-        want = [_rule(B, p7, p8) for B in range(1, BMAX + 1)]
-        got = choices[name]
-        bad = [B for B in range(1, BMAX + 1) if got[B - 1] != want[B - 1]]
-        assert not bad, (name, bad[:10])
+    for level, cases in PASS.items():
+        for name, t in cases.items():
+            want = [_rule(B, SHAPES[level], t) for B in range(1, BMAX + 1)]
+            got = choices[level, name]
+            bad = [B for B in range(1, BMAX + 1) if got[B - 1] != want[B - 1]]
+            assert not bad, (level, name, bad[:10])
 
 
 def test_hand_worked_cases(choices):
-    c = lambda name, B: choices[name][B - 1]
-    assert all(w == 7 for w in choices["untuned"])      # no measurement yet: ties go to 7
-    assert c("split", 1) == 7                            # one pass either way: the lighter one
-    assert c("split", 1024) == 7                         # 147 CTAs of 7: one pass
-    assert c("split", 7 * SMS) == 7                      # 1,036: still one pass of 7
-    assert c("split", 7 * SMS + 1) == 8                  # 1,037: two passes of 7 or one of 8
-    assert c("split", 8 * SMS) == 8                      # 1,184
-    assert c("split", 4736) == 8                         # 5 passes of 7 (47.0) vs 4 of 8 (42.0)
-    assert c("split", 16384) == 8                        # 16 x 9.40 = 150.4 vs 14 x 10.50 = 147.0
-    assert c("fp64", 16384) == 8                         # 16 x 14.28 = 228.5 vs 14 x 14.54 = 203.6
-    assert c("w8_faster", 1024) == 8                     # a faster 8-per-CTA pass wins at equal passes
+    c = lambda level, name, B: choices[level, name][B - 1]
+    # untuned: the fewest passes, ties to the first shape
+    assert all(c(1, "untuned", B) == 7 for B in range(1, 7 * SMS + 1))
+    assert c(1, "untuned", 7 * SMS + 1) == 8                # 2 passes of 7 or 1 of 8
+    assert all(c(2, "untuned", B) == 3 for B in (1, 100, 444, 10000))
+    # lvl01 split, measured
+    assert c(1, "split", 1) == 4                            # one pass either way: the shortest
+    assert c(1, "split", 4 * SMS) == 4                      # 592: one pass of 4
+    assert c(1, "split", 4 * SMS + 1) == 7                  # 2 x 6.0 = 12.0 vs one pass of 7
+    assert c(1, "split", 1024) == 7                         # 147 CTAs of 7: one pass
+    assert c(1, "split", 7 * SMS + 1) == 8                  # 1,037: two passes of 7 or one of 8
+    assert c(1, "split", 8 * SMS) == 8                      # 1,184
+    assert c(1, "split", 4736) == 8                         # 5 passes of 7 (47.0) vs 4 of 8 (42.0)
+    assert c(1, "split", 16384) == 8                        # 16 x 9.40 = 150.4 vs 14 x 10.50 = 147.0
+    assert c(1, "fp64", 16384) == 8                         # 16 x 14.28 = 228.5 vs 14 x 14.54 = 203.6
+    assert c(1, "w8_faster", 1024) == 8                     # a faster 8-per-CTA pass wins at equal passes
+    # lvl02, measured
+    assert c(2, "f64", 48) == 1                             # 48 CTAs of 1: the shortest pass
+    assert c(2, "f64", SMS + 1) == 2                        # 2 x 8.0 = 16.0 vs one pass of 2 (13.5)
+    assert c(2, "f64", 2 * SMS + 1) == 3                    # 297: one pass of 3 (17.7) vs 2 of 2 (27.0)
+    assert c(2, "f64", 16384) == 3                          # 37 x 17.7 = 654.9 vs 56 x 13.5 = 756.0
