@@ -81,6 +81,8 @@ def parse(argv=None):
                    help="run only a queue of this many filter queries, rows log-uniform in [2^8, --queue-max-rows], "
                         "widths uniform in {8, 16, 24, 32}")
     p.add_argument("--queue-max-rows", type=int, default=65536)
+    p.add_argument("--queue-mode", choices=["scheduled", "width_groups"], default="scheduled",
+                   help="native queue scheduler, or one batch per width run back to back")
     p.add_argument("--arc-rows", type=int, default=0,
                    help="run only the ArcEDB comparison measurement over this many rows")
     p.add_argument("--arc-digits", type=int, default=2, help="radix-1024 digits per value for --arc-rows")
@@ -836,9 +838,9 @@ def run_queue_bench(args):
     rng = np.random.default_rng(64)
     lo, hi = np.log(2.0 ** 8), np.log(float(args.queue_max_rows))
     queries = [(int(round(np.exp(rng.uniform(lo, hi)))), int(rng.choice([8, 16, 24, 32]))) for _ in range(args.queue)]
-    r = run_queue(eng, queries, prec)
+    r = run_queue(eng, queries, prec, mode=args.queue_mode)
     print(json.dumps({"workload": f"{args.queue} filter queries x <= c, rows log-uniform in [2^8, {args.queue_max_rows}], "
-                                  "widths uniform in {8, 16, 24, 32}, packed by width",
+                                  "widths uniform in {8, 16, 24, 32}",
                       "precision": args.precision, "autotune_pass_ms": tune, **r}))
     eng.close()
 

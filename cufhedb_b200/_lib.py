@@ -34,6 +34,12 @@ class TestVec(C.Structure):
 
 _vp, _i32, _u32, _u64 = C.c_void_p, C.c_int, C.c_uint32, C.c_uint64
 
+
+class Query(C.Structure):
+    """cufhedb_query: one filter query of a queue (cufhedb_queue_run)"""
+    _fields_ = [("level", C.c_int), ("op", C.c_int), ("plain_bits", C.c_uint32), ("logic", C.c_int),
+                ("rows", C.c_int), ("c1", C.c_void_p), ("c2", C.c_void_p), ("out", C.c_void_p)]
+
 # name -> argtypes (all return int unless listed in _RESTYPE)
 SIGNATURES = {
     "cufhedb_abi_version": [],
@@ -95,6 +101,7 @@ SIGNATURES = {
     "cufhedb_hom_or": [_vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp],
     "cufhedb_hom_msb": [_vp, _i32, _vp, _vp, _i32, _u32, _i32, _i32, _vp],
     "cufhedb_compare": [_vp, _i32, _i32, _vp, _vp, _vp, _i32, _u32, _i32, _i32, _vp],
+    "cufhedb_queue_run": [_vp, _vp, _i32, _i32, _i32, _i32, _vp, _vp],
     "cufhedb_graph_begin": [_vp, _vp],
     "cufhedb_graph_end": [_vp, _vp, C.POINTER(_vp)],
     "cufhedb_graph_launch": [_vp, _vp],

@@ -178,6 +178,9 @@ using namespace cfdb;
 int cufhedb_arc_compare(cufhedb_ctx *ctx, int op, const uint32_t *trlwe, const void *trgsw, uint32_t *out, int B,
                         int D, int precision, cufhedb_stream_t stream)
 {
+    if (!aligned_to(trlwe, 4)) return cfdb::set_error(CUFHEDB_ERR_ARG, "trlwe must be 4-byte aligned");
+    if (!aligned_to(trgsw, 16)) return cfdb::set_error(CUFHEDB_ERR_ARG, "trgsw must be 16-byte aligned");
+    if (!aligned_to(out, 4)) return cfdb::set_error(CUFHEDB_ERR_ARG, "out must be 4-byte aligned");
     if (!ctx) return set_error(CUFHEDB_ERR_ARG, "ctx is null");
     if (op < 0 || op > 3) return set_error(CUFHEDB_ERR_ARG, "unknown ArcEDB comparison");
     if (B < 0 || D < 1) return set_error(CUFHEDB_ERR_ARG, "bad batch or digit count");
@@ -226,6 +229,9 @@ int cufhedb_arc_compare(cufhedb_ctx *ctx, int op, const uint32_t *trlwe, const v
 int cufhedb_polymul_lvl1(cufhedb_ctx *ctx, const uint32_t *a, const double *m_fd, uint32_t *out, int B, int shared,
                          cufhedb_stream_t stream)
 {
+    if (!aligned_to(a, 4)) return cfdb::set_error(CUFHEDB_ERR_ARG, "a must be 4-byte aligned");
+    if (!aligned_to(m_fd, 8)) return cfdb::set_error(CUFHEDB_ERR_ARG, "m_fd must be 8-byte aligned");
+    if (!aligned_to(out, 4)) return cfdb::set_error(CUFHEDB_ERR_ARG, "out must be 4-byte aligned");
     if (!ctx || B < 0) return set_error(CUFHEDB_ERR_ARG, "bad argument");
     if (B == 0) return CUFHEDB_OK;
     if (!a || !m_fd || !out) return set_error(CUFHEDB_ERR_ARG, "null buffer");
@@ -243,6 +249,9 @@ int cufhedb_polymul_lvl1(cufhedb_ctx *ctx, const uint32_t *a, const double *m_fd
 int cufhedb_polymul_lvl2(cufhedb_ctx *ctx, const uint64_t *a, const double *m_fd, uint64_t *out, int B, int shared,
                          cufhedb_stream_t stream)
 {
+    if (!aligned_to(a, 8)) return cfdb::set_error(CUFHEDB_ERR_ARG, "a must be 8-byte aligned");
+    if (!aligned_to(m_fd, 8)) return cfdb::set_error(CUFHEDB_ERR_ARG, "m_fd must be 8-byte aligned");
+    if (!aligned_to(out, 8)) return cfdb::set_error(CUFHEDB_ERR_ARG, "out must be 8-byte aligned");
     if (!ctx || B < 0) return set_error(CUFHEDB_ERR_ARG, "bad argument");
     if (B == 0) return CUFHEDB_OK;
     if (!a || !m_fd || !out) return set_error(CUFHEDB_ERR_ARG, "null buffer");

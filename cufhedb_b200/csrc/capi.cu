@@ -683,6 +683,8 @@ int cufhedb_export_ksk_rows(cufhedb_ctx *ctx, int kind, const uint64_t *rows, in
 int cufhedb_encrypt_lvl1(cufhedb_ctx *ctx, uint64_t seed, uint64_t stream_id, uint64_t idx0, const uint32_t *msg,
                          uint32_t *out, int B, cufhedb_stream_t stream)
 {
+    NEED(aligned_to(msg, 4), "msg must be 4-byte aligned");
+    NEED(aligned_to(out, 4), "out must be 4-byte aligned");
     NEED(ctx && msg && out && B >= 0, "bad argument");
     if (!ctx->have_sk) return fail(CUFHEDB_ERR_NOKEY, "no deterministic key set (call cufhedb_keygen)");
     DeviceGuard g(ctx->device);
@@ -693,6 +695,8 @@ int cufhedb_encrypt_lvl1(cufhedb_ctx *ctx, uint64_t seed, uint64_t stream_id, ui
 int cufhedb_encrypt_lvl2(cufhedb_ctx *ctx, uint64_t seed, uint64_t stream_id, uint64_t idx0, const uint64_t *msg,
                          uint64_t *out, int B, cufhedb_stream_t stream)
 {
+    NEED(aligned_to(msg, 8), "msg must be 8-byte aligned");
+    NEED(aligned_to(out, 8), "out must be 8-byte aligned");
     NEED(ctx && msg && out && B >= 0, "bad argument");
     if (!ctx->have_sk) return fail(CUFHEDB_ERR_NOKEY, "no deterministic key set (call cufhedb_keygen)");
     DeviceGuard g(ctx->device);
@@ -703,6 +707,9 @@ int cufhedb_encrypt_lvl2(cufhedb_ctx *ctx, uint64_t seed, uint64_t stream_id, ui
 int cufhedb_phase_lvl1(cufhedb_ctx *ctx, const uint32_t *ct, const uint32_t *key, uint32_t *phase, int B,
                        cufhedb_stream_t stream)
 {
+    NEED(aligned_to(ct, 4), "ct must be 4-byte aligned");
+    NEED(aligned_to(key, 4), "key must be 4-byte aligned");
+    NEED(aligned_to(phase, 4), "phase must be 4-byte aligned");
     NEED(ctx && ct && phase && B >= 0, "bad argument");
     if (!key && !ctx->have_sk) return fail(CUFHEDB_ERR_NOKEY, "no key given and no deterministic key set");
     DeviceGuard g(ctx->device);
@@ -713,6 +720,9 @@ int cufhedb_phase_lvl1(cufhedb_ctx *ctx, const uint32_t *ct, const uint32_t *key
 int cufhedb_phase_lvl2(cufhedb_ctx *ctx, const uint64_t *ct, const uint64_t *key, uint64_t *phase, int B,
                        cufhedb_stream_t stream)
 {
+    NEED(aligned_to(ct, 8), "ct must be 8-byte aligned");
+    NEED(aligned_to(key, 8), "key must be 8-byte aligned");
+    NEED(aligned_to(phase, 8), "phase must be 8-byte aligned");
     NEED(ctx && ct && phase && B >= 0, "bad argument");
     if (!key && !ctx->have_sk) return fail(CUFHEDB_ERR_NOKEY, "no key given and no deterministic key set");
     DeviceGuard g(ctx->device);
@@ -725,6 +735,9 @@ int cufhedb_phase_lvl2(cufhedb_ctx *ctx, const uint64_t *ct, const uint64_t *key
 int cufhedb_pbs_lvl01(cufhedb_ctx *ctx, const uint32_t *in_lvl0, uint32_t *out_lvl1, int B,
                       const cufhedb_testvec *tv, int precision, cufhedb_stream_t stream)
 {
+    NEED(aligned_to(in_lvl0, 4), "in_lvl0 must be 4-byte aligned");
+    NEED(aligned_to(out_lvl1, 4), "out_lvl1 must be 4-byte aligned");
+    NEED(aligned_to(tv && tv->kind == CUFHEDB_TV_POLY ? tv->poly : nullptr, 4), "poly : nullptr must be 4-byte aligned");
     NEED(ctx != nullptr, "ctx is null");
     NEED(B >= 0, "negative batch");
     if (B == 0) return CUFHEDB_OK;
@@ -956,6 +969,8 @@ int cufhedb_autotune_load(cufhedb_ctx *ctx, const char *path)
 
 int cufhedb_iks(cufhedb_ctx *ctx, int kind, const void *in, uint32_t *out, int B, cufhedb_stream_t stream)
 {
+    NEED(aligned_to(in, kind == 10 ? 4 : 8), "in must be 4-byte (kind 10) or 8-byte (kinds 20, 21) aligned");
+    NEED(aligned_to(out, 4), "out must be 4-byte aligned");
     NEED(ctx != nullptr, "ctx is null");
     const int slot = ksk_slot(kind);
     NEED(slot >= 0, "unknown key-switching kind");
@@ -978,6 +993,9 @@ int cufhedb_iks(cufhedb_ctx *ctx, int kind, const void *in, uint32_t *out, int B
 int cufhedb_gate_lvl1(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint32_t *cb, uint32_t *out, int B,
                       int precision, cufhedb_stream_t stream)
 {
+    NEED(aligned_to(ca, 4), "ca must be 4-byte aligned");
+    NEED(aligned_to(cb, 4), "cb must be 4-byte aligned");
+    NEED(aligned_to(out, 4), "out must be 4-byte aligned");
     NEED(ctx != nullptr, "ctx is null");
     NEED(B >= 0, "negative batch");
     if (B == 0) return CUFHEDB_OK;
@@ -988,6 +1006,8 @@ int cufhedb_gate_lvl1(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint
 
 int cufhedb_twist_ifft_lvl1(cufhedb_ctx *ctx, const uint32_t *in, double *out, int B, cufhedb_stream_t stream)
 {
+    NEED(aligned_to(in, 4), "in must be 4-byte aligned");
+    NEED(aligned_to(out, 8), "out must be 8-byte aligned");
     NEED(ctx && B >= 0, "bad argument");
     if (B == 0) return CUFHEDB_OK;
     NEED(in && out, "null buffer");
@@ -998,6 +1018,8 @@ int cufhedb_twist_ifft_lvl1(cufhedb_ctx *ctx, const uint32_t *in, double *out, i
 
 int cufhedb_twist_fft_lvl1(cufhedb_ctx *ctx, const double *in, uint32_t *out, int B, cufhedb_stream_t stream)
 {
+    NEED(aligned_to(in, 8), "in must be 8-byte aligned");
+    NEED(aligned_to(out, 4), "out must be 4-byte aligned");
     NEED(ctx && B >= 0, "bad argument");
     if (B == 0) return CUFHEDB_OK;
     NEED(in && out, "null buffer");
@@ -1009,6 +1031,8 @@ int cufhedb_twist_fft_lvl1(cufhedb_ctx *ctx, const double *in, uint32_t *out, in
 int cufhedb_trgsw_prepare_lvl1(cufhedb_ctx *ctx, const uint32_t *trgsw, void *out, int B, int precision,
                                cufhedb_stream_t stream)
 {
+    NEED(aligned_to(trgsw, 4), "trgsw must be 4-byte aligned");
+    NEED(aligned_to(out, 16), "out must be 16-byte aligned");
     NEED(ctx && B >= 0, "bad argument");
     if (B == 0) return CUFHEDB_OK;
     NEED(trgsw && out, "null buffer");
@@ -1025,6 +1049,8 @@ int cufhedb_trgsw_prepare_lvl1(cufhedb_ctx *ctx, const uint32_t *trgsw, void *ou
 int cufhedb_trgswfft_prepare_lvl1(cufhedb_ctx *ctx, const double *trgswfft, void *out, int B,
                                   cufhedb_stream_t stream)
 {
+    NEED(aligned_to(trgswfft, 8), "trgswfft must be 8-byte aligned");
+    NEED(aligned_to(out, 16), "out must be 16-byte aligned");
     NEED(ctx && B >= 0, "bad argument");
     if (B == 0) return CUFHEDB_OK;
     NEED(trgswfft && out, "null buffer");
@@ -1036,6 +1062,9 @@ int cufhedb_trgswfft_prepare_lvl1(cufhedb_ctx *ctx, const double *trgswfft, void
 int cufhedb_extprod_lvl1(cufhedb_ctx *ctx, const uint32_t *trlwe, const void *trgsw, uint32_t *out, int B,
                          int shared, int precision, cufhedb_stream_t stream)
 {
+    NEED(aligned_to(trlwe, 4), "trlwe must be 4-byte aligned");
+    NEED(aligned_to(trgsw, 16), "trgsw must be 16-byte aligned");
+    NEED(aligned_to(out, 4), "out must be 4-byte aligned");
     NEED(ctx && B >= 0, "bad argument");
     if (B == 0) return CUFHEDB_OK;
     NEED(trlwe && trgsw && out, "null buffer");
@@ -1071,6 +1100,9 @@ static int pbs02_enqueue(cufhedb_ctx *ctx, const uint32_t *in, uint64_t *out, in
 int cufhedb_pbs_lvl02(cufhedb_ctx *ctx, const uint32_t *in_lvl0, uint64_t *out_lvl2, int B, const cufhedb_testvec *tv,
                       cufhedb_stream_t stream)
 {
+    NEED(aligned_to(in_lvl0, 4), "in_lvl0 must be 4-byte aligned");
+    NEED(aligned_to(out_lvl2, 8), "out_lvl2 must be 8-byte aligned");
+    NEED(aligned_to(tv && tv->kind == CUFHEDB_TV_POLY ? tv->poly : nullptr, 8), "poly : nullptr must be 8-byte aligned");
     NEED(ctx != nullptr, "ctx is null");
     NEED(B >= 0, "negative batch");
     if (B == 0) return CUFHEDB_OK;
@@ -1083,6 +1115,8 @@ int cufhedb_pbs_lvl02(cufhedb_ctx *ctx, const uint32_t *in_lvl0, uint64_t *out_l
 
 int cufhedb_trgsw_prepare_lvl2(cufhedb_ctx *ctx, const uint64_t *trgsw, void *out, int B, cufhedb_stream_t stream)
 {
+    NEED(aligned_to(trgsw, 8), "trgsw must be 8-byte aligned");
+    NEED(aligned_to(out, 16), "out must be 16-byte aligned");
     NEED(ctx && B >= 0, "bad argument");
     if (B == 0) return CUFHEDB_OK;
     NEED(trgsw && out, "null buffer");
@@ -1094,6 +1128,8 @@ int cufhedb_trgsw_prepare_lvl2(cufhedb_ctx *ctx, const uint64_t *trgsw, void *ou
 int cufhedb_trgswfft_prepare_lvl2(cufhedb_ctx *ctx, const double *trgswfft, void *out, int B,
                                   cufhedb_stream_t stream)
 {
+    NEED(aligned_to(trgswfft, 8), "trgswfft must be 8-byte aligned");
+    NEED(aligned_to(out, 16), "out must be 16-byte aligned");
     NEED(ctx && B >= 0, "bad argument");
     if (B == 0) return CUFHEDB_OK;
     NEED(trgswfft && out, "null buffer");
@@ -1105,6 +1141,9 @@ int cufhedb_trgswfft_prepare_lvl2(cufhedb_ctx *ctx, const double *trgswfft, void
 int cufhedb_extprod_lvl2(cufhedb_ctx *ctx, const uint64_t *trlwe, const void *trgsw, uint64_t *out, int B,
                          int shared, cufhedb_stream_t stream)
 {
+    NEED(aligned_to(trlwe, 8), "trlwe must be 8-byte aligned");
+    NEED(aligned_to(trgsw, 16), "trgsw must be 16-byte aligned");
+    NEED(aligned_to(out, 8), "out must be 8-byte aligned");
     NEED(ctx && B >= 0, "bad argument");
     if (B == 0) return CUFHEDB_OK;
     NEED(trlwe && trgsw && out, "null buffer");
@@ -1122,6 +1161,8 @@ int cufhedb_extprod_lvl2(cufhedb_ctx *ctx, const uint64_t *trlwe, const void *tr
 
 int cufhedb_twist_ifft_lvl2(cufhedb_ctx *ctx, const uint64_t *in, double *out, int B, cufhedb_stream_t stream)
 {
+    NEED(aligned_to(in, 8), "in must be 8-byte aligned");
+    NEED(aligned_to(out, 8), "out must be 8-byte aligned");
     NEED(ctx && B >= 0, "bad argument");
     if (B == 0) return CUFHEDB_OK;
     NEED(in && out, "null buffer");
@@ -1132,6 +1173,8 @@ int cufhedb_twist_ifft_lvl2(cufhedb_ctx *ctx, const uint64_t *in, double *out, i
 
 int cufhedb_twist_fft_lvl2(cufhedb_ctx *ctx, const double *in, uint64_t *out, int B, cufhedb_stream_t stream)
 {
+    NEED(aligned_to(in, 8), "in must be 8-byte aligned");
+    NEED(aligned_to(out, 8), "out must be 8-byte aligned");
     NEED(ctx && B >= 0, "bad argument");
     if (B == 0) return CUFHEDB_OK;
     NEED(in && out, "null buffer");

@@ -64,6 +64,11 @@ struct DeviceGuard {
     }
 };
 
+// Device buffers that kernels read or write as w-byte words must start on a
+// w-byte boundary (a misaligned word access is a device fault, which loses the
+// context): every entry point checks its buffers and refuses misaligned ones.
+inline bool aligned_to(const void *p, size_t w) { return ((uintptr_t)p % w) == 0; }
+
 // device address of the allocation-free gate's intermediate on the current
 // device (noalloc.cu); loads that module, so the array is reserved then
 cudaError_t noalloc_scratch_address(uint32_t **out);

@@ -311,6 +311,8 @@ extern "C" {
 CUFHEDB_API int cufhedb_msb_bootstrap(cufhedb_ctx *ctx, int in_level, int out_level, const void *in, void *out,
                                       int B, int logic, int precision, cufhedb_stream_t stream)
 {
+    if (!aligned_to(in, in_level == 1 ? 4 : 8)) return cfdb::set_error(CUFHEDB_ERR_ARG, "in must be 4-byte (lvl1) or 8-byte (lvl2) aligned");
+    if (!aligned_to(out, out_level == 1 ? 4 : 8)) return cfdb::set_error(CUFHEDB_ERR_ARG, "out must be 4-byte (lvl1) or 8-byte (lvl2) aligned");
     Ops o;
     int rc = cfdb::begin_ops(ctx, B, precision, o, stream);
     if (rc || B == 0) return rc;
@@ -325,6 +327,8 @@ CUFHEDB_API int cufhedb_msb_bootstrap(cufhedb_ctx *ctx, int in_level, int out_le
 CUFHEDB_API int cufhedb_ide_bootstrap(cufhedb_ctx *ctx, int in_level, int out_level, const void *in, void *out,
                                       int B, uint32_t scale_bits, int precision, cufhedb_stream_t stream)
 {
+    if (!aligned_to(in, in_level == 1 ? 4 : 8)) return cfdb::set_error(CUFHEDB_ERR_ARG, "in must be 4-byte (lvl1) or 8-byte (lvl2) aligned");
+    if (!aligned_to(out, out_level == 1 ? 4 : 8)) return cfdb::set_error(CUFHEDB_ERR_ARG, "out must be 4-byte (lvl1) or 8-byte (lvl2) aligned");
     Ops o;
     int rc = cfdb::begin_ops(ctx, B, precision, o, stream);
     if (rc || B == 0) return rc;
@@ -341,6 +345,8 @@ CUFHEDB_API int cufhedb_ide_bootstrap(cufhedb_ctx *ctx, int in_level, int out_le
 CUFHEDB_API int cufhedb_log_to_ari(cufhedb_ctx *ctx, const uint32_t *in, uint32_t *out, int B, int precision,
                                    cufhedb_stream_t stream)
 {
+    if (!aligned_to(in, 4)) return cfdb::set_error(CUFHEDB_ERR_ARG, "in must be 4-byte aligned");
+    if (!aligned_to(out, 4)) return cfdb::set_error(CUFHEDB_ERR_ARG, "out must be 4-byte aligned");
     Ops o;
     int rc = cfdb::begin_ops(ctx, B, precision, o, stream);
     if (rc || B == 0) return rc;
@@ -351,6 +357,8 @@ CUFHEDB_API int cufhedb_log_to_ari(cufhedb_ctx *ctx, const uint32_t *in, uint32_
 CUFHEDB_API int cufhedb_log_rescale(cufhedb_ctx *ctx, const uint32_t *in, uint32_t *out, int B, uint32_t scale_bits,
                                     int precision, cufhedb_stream_t stream)
 {
+    if (!aligned_to(in, 4)) return cfdb::set_error(CUFHEDB_ERR_ARG, "in must be 4-byte aligned");
+    if (!aligned_to(out, 4)) return cfdb::set_error(CUFHEDB_ERR_ARG, "out must be 4-byte aligned");
     Ops o;
     int rc = cfdb::begin_ops(ctx, B, precision, o, stream);
     if (rc || B == 0) return rc;
@@ -362,6 +370,9 @@ CUFHEDB_API int cufhedb_log_rescale(cufhedb_ctx *ctx, const uint32_t *in, uint32
 CUFHEDB_API int cufhedb_hom_and(cufhedb_ctx *ctx, const uint32_t *ca, const uint32_t *cb, uint32_t *out, int B,
                                 int logic, int precision, cufhedb_stream_t stream)
 {
+    if (!aligned_to(ca, 4)) return cfdb::set_error(CUFHEDB_ERR_ARG, "ca must be 4-byte aligned");
+    if (!aligned_to(cb, 4)) return cfdb::set_error(CUFHEDB_ERR_ARG, "cb must be 4-byte aligned");
+    if (!aligned_to(out, 4)) return cfdb::set_error(CUFHEDB_ERR_ARG, "out must be 4-byte aligned");
     Ops o;
     int rc = cfdb::begin_ops(ctx, B, precision, o, stream);
     if (rc || B == 0) return rc;
@@ -372,6 +383,9 @@ CUFHEDB_API int cufhedb_hom_and(cufhedb_ctx *ctx, const uint32_t *ca, const uint
 CUFHEDB_API int cufhedb_hom_or(cufhedb_ctx *ctx, const uint32_t *ca, const uint32_t *cb, uint32_t *out, int B,
                                int logic, int precision, cufhedb_stream_t stream)
 {
+    if (!aligned_to(ca, 4)) return cfdb::set_error(CUFHEDB_ERR_ARG, "ca must be 4-byte aligned");
+    if (!aligned_to(cb, 4)) return cfdb::set_error(CUFHEDB_ERR_ARG, "cb must be 4-byte aligned");
+    if (!aligned_to(out, 4)) return cfdb::set_error(CUFHEDB_ERR_ARG, "out must be 4-byte aligned");
     Ops o;
     int rc = cfdb::begin_ops(ctx, B, precision, o, stream);
     if (rc || B == 0) return rc;
@@ -382,6 +396,8 @@ CUFHEDB_API int cufhedb_hom_or(cufhedb_ctx *ctx, const uint32_t *ca, const uint3
 CUFHEDB_API int cufhedb_hom_msb(cufhedb_ctx *ctx, int in_level, const void *in, uint32_t *out_lvl1, int B,
                                 uint32_t plain_bits, int logic, int precision, cufhedb_stream_t stream)
 {
+    if (!aligned_to(in, in_level == 1 ? 4 : 8)) return cfdb::set_error(CUFHEDB_ERR_ARG, "in must be 4-byte (lvl1) or 8-byte (lvl2) aligned");
+    if (!aligned_to(out_lvl1, 4)) return cfdb::set_error(CUFHEDB_ERR_ARG, "out_lvl1 must be 4-byte aligned");
     Ops o;
     int rc = cfdb::begin_ops(ctx, B, precision, o, stream);
     if (rc || B == 0) return rc;
@@ -396,6 +412,9 @@ CUFHEDB_API int cufhedb_compare(cufhedb_ctx *ctx, int op, int level, const void 
                                 uint32_t *out_lvl1, int B, uint32_t plain_bits, int logic, int precision,
                                 cufhedb_stream_t stream)
 {
+    if (!aligned_to(c1, level == 1 ? 4 : 8)) return cfdb::set_error(CUFHEDB_ERR_ARG, "c1 must be 4-byte (lvl1) or 8-byte (lvl2) aligned");
+    if (!aligned_to(c2, level == 1 ? 4 : 8)) return cfdb::set_error(CUFHEDB_ERR_ARG, "c2 must be 4-byte (lvl1) or 8-byte (lvl2) aligned");
+    if (!aligned_to(out_lvl1, 4)) return cfdb::set_error(CUFHEDB_ERR_ARG, "out_lvl1 must be 4-byte aligned");
     Ops o;
     int rc = cfdb::begin_ops(ctx, B, precision, o, stream);
     if (rc || B == 0) return rc;

@@ -344,6 +344,20 @@ class Engine:
         check(self.lib.cufhedb_compare(self.ctx, _lib.COMPARE[op], level, _ptr(c1), _ptr(c2), _ptr(out),
                                        self._rows(c1, level), plain_bits, int(logic), precision, _stream(stream)))
 
+    def queue_run(self, queries, precision: int = _lib.FP64, max_batch_rows: int = 16384, nstreams: int = 2):
+        """Run a queue of filter queries through the native scheduler.
+        queries: list of (op, level, c1_dev, c2_dev, out_dev, plain_bits, logic)
+        with rows taken from out_dev.  Returns (latency_ms per query, total_ms)."""
+        n = len(queries)
+        arr = (_lib.Query * max(n, 1))()
+        for i, (op, level, c1, c2, out, pb, logic) in enumerate(queries):
+            arr[i] = _lib.Query(level, _lib.COMPARE[op] if isinstance(op, str) else op, pb, int(logic),
+                                out.numel() // (N1 + 1), _ptr(c1), _ptr(c2), _ptr(out))
+        lat = (C.c_float * max(n, 1))()
+        total = C.c_float(0.0)
+        check(self.lib.cufhedb_queue_run(self.ctx, arr, n, precision, max_batch_rows, nstreams, lat, C.byref(total)))
+        return [float(x) for x in lat[:n]], float(total.value)
+
     def polymul_lvl1(self, a_dev, m_fd_dev, out_dev, shared: bool = True, stream=None):
         """negacyclic products a_i * m, m in TFHEpp's frequency-domain layout"""
         B = a_dev.numel() // N1

@@ -14,9 +14,11 @@ replayed.
   discount and a 6-bit quantity at lvl1), split into 3 x 2 groups by a
   3-valued flag and a 2-valued status, then SUM(price * (1 - discount)) and
   COUNT per group after decryption.
-* ``run_queue`` -- many filter queries of uneven row counts and widths, packed
-  by width so each batched launch carries the rows of all queries with the
-  same comparison chain.
+* ``run_queue`` -- many filter queries of uneven row counts and widths, run by
+  the engine's native queue scheduler (cufhedb_queue_run: smallest queries
+  first, queries of one comparison chain packed into shared batches, batches
+  on two streams), or, for comparison, as one batch per width run back to
+  back.
 
 Decryption for the checks uses the deterministic key set (``Engine.keygen``).
 """
@@ -194,12 +196,14 @@ def filter_group_aggregate(eng: Engine, rows: int, precision: int, steps: int = 
             "bootstraps_per_row": {"lvl02": 8, "lvl01": 39}}
 
 
-def run_queue(eng: Engine, queries: list, precision: int, seed: int = 0x5EED_B200):
+def run_queue(eng: Engine, queries: list, precision: int, seed: int = 0x5EED_B200, mode: str = "scheduled",
+              max_batch_rows: int = 16384, nstreams: int = 2):
     """Uneven queue of filter queries x <= c.  `queries` is a list of
-    (rows, bits).  Queries of equal width share one comparison chain, so their
-    rows are concatenated and each operator step runs once per width group.
-    Returns per-query latency (the completion time of its width group, from
-    the start of the queue), aggregate rows/s and decrypt errors."""
+    (rows, bits).  mode "scheduled": the native scheduler (cufhedb_queue_run)
+    with each query's own ciphertexts; mode "width_groups": queries of equal
+    width concatenated and each width's chain run once, the widths back to
+    back.  Returns per-query latency (completion from the start of the
+    queue), aggregate rows/s and decrypt errors."""
     import torch
     rng = np.random.default_rng(seed)
     data = []
@@ -207,37 +211,51 @@ def run_queue(eng: Engine, queries: list, precision: int, seed: int = 0x5EED_B20
         x = rng.integers(0, 2 ** bits, rows).astype(np.uint64)
         c = int(rng.integers(0, 2 ** bits))
         data.append((x, c, bits))
-    widths = sorted({b for _, b in queries})
-    groups = {}
-    for w in widths:
-        idx = [i for i, (_, _, b) in enumerate(data) if b == w]
-        xs = np.concatenate([data[i][0] for i in idx])
-        cs = np.concatenate([np.full(data[i][0].size, data[i][1], np.uint64) for i in idx])
-        c1 = encrypt_column(eng, xs, w, seed, 0xC0 + w, 0)
-        c2 = encrypt_column(eng, cs, w, seed, 0xD0 + w, 0)
-        out = torch.empty(xs.size * (N1 + 1), dtype=torch.int32, device="cuda")
-        groups[w] = (idx, xs, cs, c1, c2, out)
-    eng.sync()
-    stream = torch.cuda.current_stream()
-    start = torch.cuda.Event(enable_timing=True)
-    done = {w: torch.cuda.Event(enable_timing=True) for w in widths}
-    start.record(stream)
-    for w in widths:
-        idx, xs, cs, c1, c2, out = groups[w]
-        eng.compare("le", _level(w), c1, c2, out, w, True, precision, stream)
-        done[w].record(stream)
-    eng.sync(stream)
     total_rows = sum(r for r, _ in queries)
     latency = [0.0] * len(queries)
     errors = 0
-    for w in widths:
-        idx, xs, cs, c1, c2, out = groups[w]
-        t = start.elapsed_time(done[w])
-        for i in idx:
-            latency[i] = t
-        errors += int(np.sum(decrypt_bits(eng, out, xs.size) != (xs <= cs).astype(np.int64)))
-    total_ms = max(start.elapsed_time(done[w]) for w in widths)
-    return {"queries": len(queries), "rows": total_rows, "ms": total_ms,
+    if mode == "scheduled":
+        cts = []
+        for qi, (x, c, bits) in enumerate(data):
+            c1 = encrypt_column(eng, x, bits, seed, 0xC0 + bits, 1_000_000 * qi)
+            c2 = encrypt_column(eng, np.full(x.size, c, np.uint64), bits, seed, 0xD0 + bits, 1_000_000 * qi)
+            out = torch.empty(x.size * (N1 + 1), dtype=torch.int32, device="cuda")
+            cts.append(("le", _level(bits), c1, c2, out, bits, True))
+        eng.sync()
+        latency, total_ms = eng.queue_run(cts, precision, max_batch_rows, nstreams)
+        for (x, c, bits), q in zip(data, cts):
+            errors += int(np.sum(decrypt_bits(eng, q[4], x.size) != (x <= c).astype(np.int64)))
+        extra = {"scheduler": {"max_batch_rows": max_batch_rows, "streams": nstreams}}
+    else:
+        widths = sorted({b for _, b in queries})
+        groups = {}
+        for w in widths:
+            idx = [i for i, (_, _, b) in enumerate(data) if b == w]
+            xs = np.concatenate([data[i][0] for i in idx])
+            cs = np.concatenate([np.full(data[i][0].size, data[i][1], np.uint64) for i in idx])
+            c1 = encrypt_column(eng, xs, w, seed, 0xC0 + w, 0)
+            c2 = encrypt_column(eng, cs, w, seed, 0xD0 + w, 0)
+            out = torch.empty(xs.size * (N1 + 1), dtype=torch.int32, device="cuda")
+            groups[w] = (idx, xs, cs, c1, c2, out)
+        eng.sync()
+        stream = torch.cuda.current_stream()
+        start = torch.cuda.Event(enable_timing=True)
+        done = {w: torch.cuda.Event(enable_timing=True) for w in widths}
+        start.record(stream)
+        for w in widths:
+            idx, xs, cs, c1, c2, out = groups[w]
+            eng.compare("le", _level(w), c1, c2, out, w, True, precision, stream)
+            done[w].record(stream)
+        eng.sync(stream)
+        for w in widths:
+            idx, xs, cs, c1, c2, out = groups[w]
+            t = start.elapsed_time(done[w])
+            for i in idx:
+                latency[i] = t
+            errors += int(np.sum(decrypt_bits(eng, out, xs.size) != (xs <= cs).astype(np.int64)))
+        total_ms = max(start.elapsed_time(done[w]) for w in widths)
+        extra = {"width_groups": {int(w): int(groups[w][1].size) for w in widths}}
+    return {"queries": len(queries), "rows": total_rows, "ms": total_ms, "mode": mode,
             "rows_per_s": total_rows / (total_ms / 1000.0), "decrypt_errors": errors,
-            "latency_ms": {"min": min(latency), "median": float(np.median(latency)), "max": max(latency)},
-            "width_groups": {int(w): int(groups[w][1].size) for w in widths}}
+            "latency_ms": {"min": min(latency), "median": float(np.median(latency)), "max": max(latency),
+                           "mean": float(np.mean(latency))}, **extra}

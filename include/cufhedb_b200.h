@@ -260,6 +260,28 @@ CUFHEDB_API int cufhedb_compare(cufhedb_ctx *ctx, int op, int level, const void 
                                 uint32_t *out_lvl1, int B, uint32_t plain_bits, int logic, int precision,
                                 cufhedb_stream_t stream);
 
+/* One filter query of a queue: `rows` comparisons c1[i] op c2[i] of level-
+ * `level` ciphertexts (device memory), results to `out` (rows lvl1 TLWEs). */
+typedef struct {
+    int level;           /* 1 or 2 */
+    int op;              /* as cufhedb_compare: 0 gt, 1 ge, 2 lt, 3 le, 4 eq */
+    uint32_t plain_bits;
+    int logic;
+    int rows;
+    const void *c1, *c2;
+    uint32_t *out;
+} cufhedb_query;
+/* Runs a whole queue of such queries (the reference's query programs run one
+ * query at a time as a row loop of one-row operator calls,
+ * test/HE3_Query/TPCH_Q6.cu:158-209): queries that share a comparison chain
+ * are packed into batches of at most max_batch_rows rows, smallest first; the
+ * batches run in order of cost per completed query on `nstreams` streams
+ * (1..16), so different levels' bootstraps overlap.  latency_ms[i] receives
+ * query i's completion time from the start of the queue and total_ms (may be
+ * NULL) the whole queue's; returns when every result is in place. */
+CUFHEDB_API int cufhedb_queue_run(cufhedb_ctx *ctx, const cufhedb_query *q, int nq, int precision,
+                                  int max_batch_rows, int nstreams, float *latency_ms, float *total_ms);
+
 /* B negacyclic products out_i = a_i * m (the reference's PolyMul_st,
  * src/cuHEDB/fft_gpu/cufft_gpu.cuh:214-226, which multiplies by the
  * polynomial its engine last transformed): TwistFFT(TwistIFFT(a_i) x m) in

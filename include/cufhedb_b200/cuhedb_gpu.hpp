@@ -305,7 +305,13 @@ class Coalescer {
             if (!x.st) check_cuda(cudaStreamCreateWithFlags(&x.st, cudaStreamNonBlocking));
             const size_t n = rows.size();
             const bool two = rows[0].in2 != nullptr;
-            const size_t in_total = n * in_bytes * (two ? 2 : 1), total = in_total + n * out_bytes;
+            // every region starts on a 256-byte boundary: the kernels read and
+            // write 64-bit torus words, and n rows of lvl0 inputs (2,692 bytes
+            // each) end on a 4-byte boundary only
+            auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+            const size_t in2_off = up(n * in_bytes);
+            const size_t out_off = up(in2_off + (two ? n * in_bytes : 0));
+            const size_t total = out_off + n * out_bytes;
             if (x.cap < total) {
                 cudaFreeHost(x.h);
                 x.h = nullptr;
@@ -315,17 +321,16 @@ class Coalescer {
             }
             for (size_t i = 0; i < n; i++) {
                 std::memcpy(x.h + i * in_bytes, rows[i].in1, in_bytes);
-                if (two) std::memcpy(x.h + (n + i) * in_bytes, rows[i].in2, in_bytes);
+                if (two) std::memcpy(x.h + in2_off + i * in_bytes, rows[i].in2, in_bytes);
             }
             unsigned char *d = nullptr;
             check_cuda(cudaMallocAsync((void **)&d, total, x.st));
             int rc = CUFHEDB_OK;
-            cudaError_t e = cudaMemcpyAsync(d, x.h, in_total, cudaMemcpyHostToDevice, x.st);
-            if (e == cudaSuccess)
-                rc = fn(d, two ? d + n * in_bytes : nullptr, d + in_total, (int)n, x.st);
+            cudaError_t e = cudaMemcpyAsync(d, x.h, out_off, cudaMemcpyHostToDevice, x.st);
+            if (e == cudaSuccess) rc = fn(d, two ? d + in2_off : nullptr, d + out_off, (int)n, x.st);
             std::string msg = rc == CUFHEDB_OK ? "" : std::string("cufhedb: ") + cufhedb_last_error();
             if (e == cudaSuccess && rc == CUFHEDB_OK)
-                e = cudaMemcpyAsync(x.h + in_total, d + in_total, n * out_bytes, cudaMemcpyDeviceToHost, x.st);
+                e = cudaMemcpyAsync(x.h + out_off, d + out_off, n * out_bytes, cudaMemcpyDeviceToHost, x.st);
             cudaFreeAsync(d, x.st);
             if (e != cudaSuccess) return std::string("cufhedb (CUDA): ") + cudaGetErrorString(e);
             if (!msg.empty()) {
@@ -333,7 +338,7 @@ class Coalescer {
                 return msg;
             }
             if (cufhedb_sync(ctx, x.st) != CUFHEDB_OK) return std::string("cufhedb: ") + cufhedb_last_error();
-            for (size_t i = 0; i < n; i++) std::memcpy(rows[i].out, x.h + in_total + i * out_bytes, out_bytes);
+            for (size_t i = 0; i < n; i++) std::memcpy(rows[i].out, x.h + out_off + i * out_bytes, out_bytes);
             return "";
         } catch (const std::exception &ex) {
             return ex.what();
@@ -377,13 +382,30 @@ class CuFFT_Torus {
         (void)num_stream;   // streams are created on first use of each stream_id
     }
 
-    // LoadBK (cufft_gpu.cuh:175-184): TFHEpp BootstrappingKeyFFT, host memory
+    // LoadBK (cufft_gpu.cuh:175-184): TFHEpp BootstrappingKeyFFT, host memory.
+    // Then the launch shapes of this level's bootstraps are tuned once: read
+    // from the table file CUFHEDB_AUTOTUNE_FILE names when that was made for
+    // this device and parameter set, else measured (well under a second) and
+    // written there.
     void LoadBK(const std::array<std::array<std::array<std::array<double, P::n>, 2>, (P::k + 1) * P::l>, 672> &bk)
     {
+        cufhedb_ctx *ctx = cufhedb_dropin::engine();
         if constexpr (P::n == 1024)
-            cufhedb_dropin::check(cufhedb_load_bkfft_lvl01(cufhedb_dropin::engine(), &bk[0][0][0][0]));
+            cufhedb_dropin::check(cufhedb_load_bkfft_lvl01(ctx, &bk[0][0][0][0]));
         else
-            cufhedb_dropin::check(cufhedb_load_bkfft_lvl02(cufhedb_dropin::engine(), &bk[0][0][0][0]));
+            cufhedb_dropin::check(cufhedb_load_bkfft_lvl02(ctx, &bk[0][0][0][0]));
+        const char *path = std::getenv("CUFHEDB_AUTOTUNE_FILE");
+        if (path) cufhedb_autotune_load(ctx, path);   // refused when made elsewhere: tuned below
+        float t[3] = {1.0f, 1.0f, 1.0f};
+        cufhedb_autotune_table(ctx, P::n == 1024 ? 1 : 2, CUFHEDB_FP64, nullptr, t);
+        if (!(t[0] == 1.0f && t[1] == 1.0f && t[2] == 1.0f)) return;   // this level is tuned already
+        if constexpr (P::n == 1024) {
+            cufhedb_dropin::check(cufhedb_autotune_pbs01(ctx, CUFHEDB_FP64, nullptr, nullptr));
+            cufhedb_dropin::check(cufhedb_autotune_pbs01(ctx, CUFHEDB_SPLIT32, nullptr, nullptr));
+        } else {
+            cufhedb_dropin::check(cufhedb_autotune_pbs02(ctx, nullptr));
+        }
+        if (path) cufhedb_autotune_save(ctx, path);
     }
 
     void ifft_st(std::array<double, P::n> &res, std::array<typename P::T, P::n> &a, const uint32_t stream_id)

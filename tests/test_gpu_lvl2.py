@@ -168,3 +168,22 @@ def test_pbs02_ragged_multi_pass_batch(engine2, oracle, keys):
     p = ph.cpu().numpy()
     assert np.array_equal((p > 0).astype(int), bits)
     assert np.max(np.abs(np.abs(p.astype(np.float64)) - MU2)) < 2.0 ** 56
+
+
+def test_misaligned_buffers_are_refused(engine2):
+    """A 64-bit torus buffer that does not start on an 8-byte boundary is
+    refused with CUFHEDB_ERR_ARG before anything is enqueued (a misaligned
+    word access would be a device fault)."""
+    import torch
+    from cufhedb_b200 import CufhedbError, testvec_const
+    x = torch.zeros(2 * (N0 + 1), dtype=torch.int32, device="cuda")
+    raw = torch.zeros(2 * (N2 + 1) + 1, dtype=torch.int64, device="cuda")
+    odd = raw.view(torch.int32)[1:1 + 2 * 2 * (N2 + 1)]       # starts 4 bytes into the buffer
+    import ctypes
+    from cufhedb_b200 import _lib
+    tv = testvec_const(1 << 61)
+    rc = engine2.lib.cufhedb_pbs_lvl02(engine2.ctx, x.data_ptr(), odd.data_ptr(), 2, ctypes.byref(tv), None)
+    assert rc == _lib.ERR_ARG and b"8-byte aligned" in _lib.load().cufhedb_last_error()
+    rc = engine2.lib.cufhedb_iks(engine2.ctx, 20, odd.data_ptr(), x.data_ptr(), 1, None)
+    assert rc == _lib.ERR_ARG
+    engine2.sync()

@@ -1,7 +1,8 @@
 """GPU: the query shapes on the batched operator layer -- the filter +
 grouped aggregate (3 range predicates, 3 x 2 groups, SUM and COUNT after
 decryption, DAG replayed as a CUDA graph) and an uneven queue of filter
-queries packed by width -- against plaintext evaluation."""
+queries, run by the native scheduler and as width groups -- against
+plaintext evaluation."""
 from __future__ import annotations
 
 import pytest
@@ -32,7 +33,23 @@ def test_uneven_queue_packed_by_width(eng_q):
     from cufhedb_b200 import SPLIT32
     from cufhedb_b200.queries import run_queue
     queries = [(20, 8), (33, 16), (7, 8), (12, 24), (9, 32), (16, 16)]
-    r = run_queue(eng_q, queries, SPLIT32)
+    r = run_queue(eng_q, queries, SPLIT32, mode="width_groups")
     assert r["decrypt_errors"] == 0, r
     assert r["rows"] == sum(n for n, _ in queries)
     assert r["width_groups"] == {8: 27, 16: 49, 24: 12, 32: 9}
+
+
+@pytest.mark.parametrize("max_batch_rows,nstreams", [(16384, 2), (24, 3), (1, 1)])
+def test_uneven_queue_native_scheduler(eng_q, max_batch_rows, nstreams):
+    """Every query decrypts bit-exact whether the scheduler packs queries into
+    shared batches (gather / scatter through staging), splits them into
+    single-query batches (batch cap below every query) or runs them on one
+    stream; each query has its own latency, no later than the whole queue."""
+    from cufhedb_b200 import SPLIT32
+    from cufhedb_b200.queries import run_queue
+    queries = [(20, 8), (33, 16), (7, 8), (12, 24), (9, 32), (16, 16), (5, 8), (40, 16), (3, 32)]
+    r = run_queue(eng_q, queries, SPLIT32, mode="scheduled", max_batch_rows=max_batch_rows, nstreams=nstreams)
+    assert r["decrypt_errors"] == 0, r
+    assert r["rows"] == sum(n for n, _ in queries)
+    lat = r["latency_ms"]
+    assert 0 < lat["min"] <= lat["median"] <= lat["max"] <= r["ms"] + 1e-3
