@@ -57,7 +57,7 @@ def parse(argv=None):
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--batch", type=int, default=1024)
-    p.add_argument("--precision", choices=["fp64", "split32"], default="split32",
+    p.add_argument("--precision", choices=["fp64", "split32", "split32tc"], default="split32",
                    help="headline path (the other one is timed alongside)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--filter-rows", type=int, default=16384,
@@ -101,6 +101,11 @@ def tensor_peak():
             return float(json.load(fh)["bf16_tflops"]), "measured (MEASURED_PEAKS.json bf16_tflops, burst)"
     except Exception:
         return 1590.0, "fallback (earlier measurement on this pool)"
+
+
+def _prec(name: str) -> int:
+    from cufhedb_b200 import FP64, SPLIT32, SPLIT32_TC
+    return {"fp64": FP64, "split32": SPLIT32, "split32tc": SPLIT32_TC}[name]
 
 
 def dist_env():
@@ -463,11 +468,11 @@ def run_ours(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
-    from cufhedb_b200 import FP64, GEN_ALL, GEN_BK01, GEN_KSK10, SPLIT32, Engine, _lib, testvec_const
+    from cufhedb_b200 import FP64, GEN_ALL, GEN_BK01, GEN_KSK10, SPLIT32, SPLIT32_TC, Engine, _lib, testvec_const
 
     head = args.precision
-    other = "fp64" if head == "split32" else "split32"
-    PREC = {"fp64": FP64, "split32": SPLIT32}
+    other = "fp64" if head != "fp64" else "split32"
+    PREC = {"fp64": FP64, "split32": SPLIT32, "split32tc": SPLIT32_TC}
     B = args.batch
     single = world == 1
     eng = Engine(local)
@@ -496,7 +501,8 @@ def run_ours(args):
     # ---- launch-shape autotuning (untimed): one full pass of every shape ----------
     tuned = eng.autotune(levels=(1, 2) if (single and args.filter_rows) else (1,))
     tune = {f"pbs01_{name}": {"pass_ms_by_shape": tuned[f"pbs01_{name}"],
-                              "ciphertexts_per_cta": eng.launch_shape(1, PREC[name], B)} for name in (head, other)}
+                              "ciphertexts_per_cta": eng.launch_shape(1, PREC[name], B)}
+            for name in ("split32", "fp64", "split32tc")}
     if single and args.filter_rows:
         tune["pbs02"] = {"pass_ms_by_shape": tuned["pbs02"],
                          "ciphertexts_per_cta_filter": eng.launch_shape(2, FP64, args.filter_rows)}
@@ -529,6 +535,11 @@ def run_ours(args):
         res[name]["pbs_ms"] = statistics.median(
             _timed(lambda: eng.pbs_lvl01(lvl0, out, tv, prec, stream), 5, flush, stream))
     iks_ms = statistics.median(_timed(lambda: eng.iks(10, ca, lvl0, stream), 5, flush, stream))
+    # the split path with its first transform step on the tensor cores, kernel alone
+    tc_name = "split32tc" if head != "split32tc" else "split32"
+    tc_ms = statistics.median(_timed(lambda: eng.pbs_lvl01(lvl0, out, tv, PREC[tc_name], stream), 5, flush, stream))
+    eng.gate_lvl1("NAND", ca, cb, out, PREC[tc_name], stream)
+    tc_errors, _, _ = _gate_errors(eng, out, want, stream)
 
     # ---- end to end through the C ABI with host buffers: pinned H2D + gate + D2H --
     ca_h = ca.cpu().pin_memory()
@@ -613,6 +624,11 @@ def run_ours(args):
             "split_over_fp64": (value / v_other) if head == "split32" else (v_other / value),
             "split_over_fp64_kernel": (res["fp64"]["pbs_ms"] / res["split32"]["pbs_ms"]),
             "pbs_kernel_ms": res[head]["pbs_ms"], "iks_kernel_ms": iks_ms,
+            tc_name: {"pbs_kernel_ms": tc_ms, "pbs_per_s_kernel": B / (tc_ms / 1000.0),
+                      "decrypt_errors_one_step": int(tc_errors),
+                      "shape": eng.launch_shape(1, PREC[tc_name], B),
+                      "what": "split32 with the first step of every digit transform on the tensor cores "
+                              "(tcgen05 MMA, FP16 two-limb constants, FP32 accumulation in tensor memory)"},
             "autotune": tune,
             "roofline": roof(head),
             "gpu_launches": 2 * args.steps,
@@ -647,8 +663,8 @@ def run_ours(args):
 
 
 def run_filter_only(args):
-    from cufhedb_b200 import FP64, GEN_ALL, SPLIT32, Engine
-    prec = FP64 if args.precision == "fp64" else SPLIT32
+    from cufhedb_b200 import GEN_ALL, Engine
+    prec = _prec(args.precision)
     eng = Engine(0)
     eng.keygen(SEED, GEN_ALL)
     rows = args.filter_rows or 16384
@@ -743,8 +759,8 @@ def run_extprod(args):
 def run_profile_pbs(args):
     """--steps launches of the PBS kernel alone, no key-switching key."""
     import torch
-    from cufhedb_b200 import FP64, GEN_BK01, GEN_BK02, SPLIT32, Engine, testvec_const
-    prec = FP64 if args.precision == "fp64" else SPLIT32
+    from cufhedb_b200 import FP64, GEN_BK01, GEN_BK02, SPLIT32, SPLIT32_TC, Engine, testvec_const
+    prec = {"fp64": FP64, "split32": SPLIT32, "split32tc": SPLIT32_TC}[args.precision]
     eng = Engine(0)
     eng.keygen(SEED, GEN_BK01 if args.level == 1 else GEN_BK02)
     g = torch.Generator(device="cuda").manual_seed(99)
@@ -818,10 +834,9 @@ def _engine_all_keys_tuned():
 
 
 def run_agg(args):
-    from cufhedb_b200 import FP64, SPLIT32
     from cufhedb_b200.queries import filter_group_aggregate
     eng, tune = _engine_all_keys_tuned()
-    prec = FP64 if args.precision == "fp64" else SPLIT32
+    prec = _prec(args.precision)
     r = filter_group_aggregate(eng, args.agg_rows, prec, steps=max(1, min(args.steps, 3)))
     print(json.dumps({"workload": "filter (date range at lvl2, discount range, quantity bound) + 3 x 2 groups, "
                                   "SUM(price * (1 - discount)) and COUNT after decryption; DAG replayed as a CUDA graph",
@@ -831,10 +846,9 @@ def run_agg(args):
 
 def run_queue_bench(args):
     import numpy as np
-    from cufhedb_b200 import FP64, SPLIT32
     from cufhedb_b200.queries import run_queue
     eng, tune = _engine_all_keys_tuned()
-    prec = FP64 if args.precision == "fp64" else SPLIT32
+    prec = _prec(args.precision)
     rng = np.random.default_rng(64)
     lo, hi = np.log(2.0 ** 8), np.log(float(args.queue_max_rows))
     queries = [(int(round(np.exp(rng.uniform(lo, hi)))), int(rng.choice([8, 16, 24, 32]))) for _ in range(args.queue)]

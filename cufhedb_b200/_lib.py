@@ -13,7 +13,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libcufhedb_b200.so")
 
 OK, ERR_ARG, ERR_NOKEY, ERR_CUDA, ERR_OOM, ERR_DEVICE, ERR_UNSUPPORTED = range(7)
-FP64, SPLIT32 = 0, 1
+FP64, SPLIT32, SPLIT32_TC = 0, 1, 2
 KSK10, KSK20, KSK21 = 10, 20, 21
 GEN_BK01, GEN_BK02, GEN_KSK10, GEN_KSK20, GEN_KSK21, GEN_ALL = 1, 2, 4, 8, 16, 31
 TV_CONST, TV_STAIRCASE, TV_POLY = 0, 1, 2

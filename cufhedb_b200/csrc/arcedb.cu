@@ -186,7 +186,8 @@ int cufhedb_arc_compare(cufhedb_ctx *ctx, int op, const uint32_t *trlwe, const v
     if (B < 0 || D < 1) return set_error(CUFHEDB_ERR_ARG, "bad batch or digit count");
     if (B == 0) return CUFHEDB_OK;
     if (!trlwe || !trgsw || !out) return set_error(CUFHEDB_ERR_ARG, "null buffer");
-    if (precision != CUFHEDB_FP64 && precision != CUFHEDB_SPLIT32) return set_error(CUFHEDB_ERR_ARG, "unsupported precision");
+    if (precision != CUFHEDB_FP64 && precision != CUFHEDB_SPLIT32 &&
+        precision != CUFHEDB_SPLIT32_TC) return set_error(CUFHEDB_ERR_ARG, "unsupported precision");
     if (D > 1 && !ctx->ksk[0]) return set_error(CUFHEDB_ERR_NOKEY, "lvl10 key-switching key not loaded");
     if (D > 1 && !ctx->bk01) return set_error(CUFHEDB_ERR_NOKEY, "lvl01 bootstrapping key not loaded");
     DeviceGuard guard(ctx->device);

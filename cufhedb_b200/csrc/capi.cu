@@ -16,6 +16,7 @@
 #include "keys.cuh"
 #include "lvl2.cuh"
 #include "pbs_common.cuh"
+#include "tc_stage1.cuh"
 
 using namespace cfdb;
 
@@ -103,6 +104,7 @@ void build_tables_f(const Fft512Tables &D, Fft512TablesF &F)
         P.w32[j] = make_float2((float)D.w32[j].x, (float)D.w32[j].y);
         P.w32p[j] = Q.w32p[j] = dup(D.w32[j].x, D.w32[j].y);
     }
+    build_stage1_b(F.tc_b[0], F.tc_b[1]);
 }
 
 struct GateSpec {
@@ -140,28 +142,39 @@ int check_tv(const cufhedb_testvec *tv, int N)
     return CUFHEDB_OK;
 }
 
+bool valid_precision(int p) { return p == CUFHEDB_FP64 || p == CUFHEDB_SPLIT32 || p == CUFHEDB_SPLIT32_TC; }
+
+// the lvl01 PBS kernel of a precision, in the launch shape the context's
+// table picks for the batch (key, tables and kernel set in `a` here)
+int launch_pbs01_any(cufhedb_ctx *ctx, Pbs01Args &a, int precision, cudaStream_t st)
+{
+    const int w = pbs01_choose_w(a.B, ctx->num_sms, ctx->pbs01_pass_ms[precision]);
+    if (precision == CUFHEDB_FP64) {
+        a.bk = ctx->bk01;
+        a.tables = ctx->tab512;
+        CK(launch_pbs01_f64(a, ctx->num_sms, w, st));
+        return CUFHEDB_OK;
+    }
+    if (!ctx->bk01_split) return fail(CUFHEDB_ERR_NOKEY, "split-precision lvl01 key not prepared");
+    a.bk = reinterpret_cast<const double2 *>(ctx->bk01_split);
+    a.tables = ctx->tab512f;
+    if (precision == CUFHEDB_SPLIT32_TC) CK(launch_pbs01_split_tc(a, ctx->num_sms, w, st));
+    else CK(launch_pbs01_split(a, ctx->num_sms, w, st));
+    return CUFHEDB_OK;
+}
+
 int pbs01_enqueue(cufhedb_ctx *ctx, const uint32_t *in, uint32_t *out, int B, const cufhedb_testvec *tv,
                   int precision, cudaStream_t st)
 {
     if (!ctx->bk01) return fail(CUFHEDB_ERR_NOKEY, "lvl01 bootstrapping key not loaded");
-    if (precision != CUFHEDB_FP64 && precision != CUFHEDB_SPLIT32) return fail(CUFHEDB_ERR_ARG, "unsupported precision");
+    if (!valid_precision(precision)) return fail(CUFHEDB_ERR_ARG, "unsupported precision");
     Pbs01Args a{};
     a.in = in;
     a.out = out;
     a.B = B;
     a.tv = to_tv(tv);
     a.err = ctx->err;
-    if (precision == CUFHEDB_FP64) {
-        a.bk = ctx->bk01;
-        a.tables = ctx->tab512;
-        CK(launch_pbs01_f64(a, ctx->num_sms, pbs01_choose_w(B, ctx->num_sms, ctx->pbs01_pass_ms[0]), st));
-    } else {
-        if (!ctx->bk01_split) return fail(CUFHEDB_ERR_NOKEY, "split-precision lvl01 key not prepared");
-        a.bk = reinterpret_cast<const double2 *>(ctx->bk01_split);
-        a.tables = ctx->tab512f;
-        CK(launch_pbs01_split(a, ctx->num_sms, pbs01_choose_w(B, ctx->num_sms, ctx->pbs01_pass_ms[1]), st));
-    }
-    return CUFHEDB_OK;
+    return launch_pbs01_any(ctx, a, precision, st);
 }
 
 int gate_enqueue(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint32_t *cb, uint32_t *out, int B,
@@ -205,7 +218,7 @@ int pbs01_run(cufhedb_ctx *ctx, const uint32_t *in, uint32_t *out, int B, const 
 {
     if (B <= 0) return CUFHEDB_OK;
     if (!ctx->bk01) return fail(CUFHEDB_ERR_NOKEY, "lvl01 bootstrapping key not loaded");
-    if (precision != CUFHEDB_FP64 && precision != CUFHEDB_SPLIT32) return fail(CUFHEDB_ERR_ARG, "unsupported precision");
+    if (!valid_precision(precision)) return fail(CUFHEDB_ERR_ARG, "unsupported precision");
     Pbs01Args a{};
     a.in = in;
     a.out = out;
@@ -213,17 +226,7 @@ int pbs01_run(cufhedb_ctx *ctx, const uint32_t *in, uint32_t *out, int B, const 
     a.tv = tv;
     a.out_b_add = b_add;
     a.err = ctx->err;
-    if (precision == CUFHEDB_FP64) {
-        a.bk = ctx->bk01;
-        a.tables = ctx->tab512;
-        CK(launch_pbs01_f64(a, ctx->num_sms, pbs01_choose_w(B, ctx->num_sms, ctx->pbs01_pass_ms[0]), st));
-    } else {
-        if (!ctx->bk01_split) return fail(CUFHEDB_ERR_NOKEY, "split-precision lvl01 key not prepared");
-        a.bk = reinterpret_cast<const double2 *>(ctx->bk01_split);
-        a.tables = ctx->tab512f;
-        CK(launch_pbs01_split(a, ctx->num_sms, pbs01_choose_w(B, ctx->num_sms, ctx->pbs01_pass_ms[1]), st));
-    }
-    return CUFHEDB_OK;
+    return launch_pbs01_any(ctx, a, precision, st);
 }
 
 int pbs02_run(cufhedb_ctx *ctx, const uint32_t *in, uint64_t *out, int B, const TestVec &tv, uint64_t b_add,
@@ -790,7 +793,8 @@ static int autotune_level(cufhedb_ctx *ctx, int level, int precision, float out_
                     } else {
                         a.bk = reinterpret_cast<const double2 *>(ctx->bk01_split);
                         a.tables = ctx->tab512f;
-                        e = launch_pbs01_split(a, ctx->num_sms, w, st);
+                        e = precision == CUFHEDB_SPLIT32_TC ? launch_pbs01_split_tc(a, ctx->num_sms, w, st)
+                                                            : launch_pbs01_split(a, ctx->num_sms, w, st);
                     }
                 } else {
                     const cufhedb_testvec tv{CUFHEDB_TV_CONST, 0, 1ull << 61, nullptr};
@@ -826,9 +830,9 @@ static int autotune_level(cufhedb_ctx *ctx, int level, int precision, float out_
 int cufhedb_autotune_pbs01(cufhedb_ctx *ctx, int precision, float *ms_w7, float *ms_w8)
 {
     NEED(ctx != nullptr, "ctx is null");
-    NEED(precision == CUFHEDB_FP64 || precision == CUFHEDB_SPLIT32, "unsupported precision");
+    NEED(valid_precision(precision), "unsupported precision");
     if (!ctx->bk01) return fail(CUFHEDB_ERR_NOKEY, "lvl01 bootstrapping key not loaded");
-    if (precision == CUFHEDB_SPLIT32 && !ctx->bk01_split)
+    if (precision != CUFHEDB_FP64 && !ctx->bk01_split)
         return fail(CUFHEDB_ERR_NOKEY, "split-precision lvl01 key not prepared");
     DeviceGuard g(ctx->device);
     float ms[NSHAPES];
@@ -857,8 +861,7 @@ int cufhedb_autotune_pbs02(cufhedb_ctx *ctx, float *ms)
 
 static float *shape_table(cufhedb_ctx *ctx, int level, int precision)
 {
-    if (level == 1 && (precision == CUFHEDB_FP64 || precision == CUFHEDB_SPLIT32))
-        return ctx->pbs01_pass_ms[precision];
+    if (level == 1 && valid_precision(precision)) return ctx->pbs01_pass_ms[precision];
     if (level == 2 && precision == CUFHEDB_FP64) return ctx->pbs02_pass_ms;
     return nullptr;
 }
@@ -913,8 +916,8 @@ int cufhedb_autotune_save(cufhedb_ctx *ctx, const char *path)
     if (!f) return fail(CUFHEDB_ERR_ARG, std::string("cannot write ") + path);
     std::fprintf(f, "cufhedb_b200 autotune 1\ndevice %s sms %d params %016llx\n", device_tag(ctx->device).c_str(),
                  ctx->num_sms, (unsigned long long)param_hash());
-    const char *names[2] = {"fp64", "split32"};
-    for (int p = 0; p < 2; ++p) {
+    const char *names[3] = {"fp64", "split32", "split32tc"};
+    for (int p = 0; p < 3; ++p) {
         std::fprintf(f, "pbs01 %s", names[p]);
         for (int i = 0; i < NSHAPES; ++i) std::fprintf(f, " %d %.6f", PBS01_SHAPES[i], ctx->pbs01_pass_ms[p][i]);
         std::fprintf(f, "\n");
@@ -938,14 +941,17 @@ int cufhedb_autotune_load(cufhedb_ctx *ctx, const char *path)
                           &hash) == 4 &&
               version == 1;
     const bool same = ok && device_tag(ctx->device) == dev && sms == ctx->num_sms && hash == param_hash();
-    float t01[2][NSHAPES], t02[NSHAPES];
+    float t01[3][NSHAPES], t02[NSHAPES];
     int seen = 0;
     while (same && std::fscanf(f, "%15s %15s", kind, prec) == 2) {
         float *dst = nullptr;
         const int *shapes = nullptr;
-        if (!std::strcmp(kind, "pbs01") && !std::strcmp(prec, "fp64")) dst = t01[0], shapes = PBS01_SHAPES;
-        else if (!std::strcmp(kind, "pbs01") && !std::strcmp(prec, "split32")) dst = t01[1], shapes = PBS01_SHAPES;
-        else if (!std::strcmp(kind, "pbs02") && !std::strcmp(prec, "fp64")) dst = t02, shapes = PBS02_SHAPES;
+        int bit = 0;
+        if (!std::strcmp(kind, "pbs01") && !std::strcmp(prec, "fp64")) dst = t01[0], shapes = PBS01_SHAPES, bit = 1;
+        else if (!std::strcmp(kind, "pbs01") && !std::strcmp(prec, "split32")) dst = t01[1], shapes = PBS01_SHAPES, bit = 2;
+        else if (!std::strcmp(kind, "pbs01") && !std::strcmp(prec, "split32tc"))
+            dst = t01[2], shapes = PBS01_SHAPES, bit = 4;
+        else if (!std::strcmp(kind, "pbs02") && !std::strcmp(prec, "fp64")) dst = t02, shapes = PBS02_SHAPES, bit = 8;
         if (!dst) {
             ok = false;
             break;
@@ -954,14 +960,13 @@ int cufhedb_autotune_load(cufhedb_ctx *ctx, const char *path)
             int w = 0;
             ok = std::fscanf(f, "%d %f", &w, &dst[i]) == 2 && w == shapes[i] && dst[i] > 0.0f;
         }
-        seen |= dst == t02 ? 4 : dst == t01[0] ? 1 : 2;
+        seen |= bit;
     }
     std::fclose(f);
     if (!same) return fail(CUFHEDB_ERR_ARG, "autotune table is for another device, SM count or parameter set");
-    if (!ok || seen != 7) return fail(CUFHEDB_ERR_ARG, "malformed autotune table");
+    if (!ok || seen != 15) return fail(CUFHEDB_ERR_ARG, "malformed autotune table");
     for (int i = 0; i < NSHAPES; ++i) {
-        ctx->pbs01_pass_ms[0][i] = t01[0][i];
-        ctx->pbs01_pass_ms[1][i] = t01[1][i];
+        for (int p = 0; p < 3; ++p) ctx->pbs01_pass_ms[p][i] = t01[p][i];
         ctx->pbs02_pass_ms[i] = t02[i];
     }
     return CUFHEDB_OK;
@@ -1036,7 +1041,7 @@ int cufhedb_trgsw_prepare_lvl1(cufhedb_ctx *ctx, const uint32_t *trgsw, void *ou
     NEED(ctx && B >= 0, "bad argument");
     if (B == 0) return CUFHEDB_OK;
     NEED(trgsw && out, "null buffer");
-    NEED(precision == CUFHEDB_FP64 || precision == CUFHEDB_SPLIT32, "unsupported precision");
+    NEED(valid_precision(precision), "unsupported precision");
     DeviceGuard g(ctx->device);
     const int rows = B * 2 * L1;
     if (precision == CUFHEDB_FP64)
@@ -1068,7 +1073,7 @@ int cufhedb_extprod_lvl1(cufhedb_ctx *ctx, const uint32_t *trlwe, const void *tr
     NEED(ctx && B >= 0, "bad argument");
     if (B == 0) return CUFHEDB_OK;
     NEED(trlwe && trgsw && out, "null buffer");
-    NEED(precision == CUFHEDB_FP64 || precision == CUFHEDB_SPLIT32, "unsupported precision");
+    NEED(valid_precision(precision), "unsupported precision");
     DeviceGuard g(ctx->device);
     ExtProdArgs a{};
     a.trlwe = trlwe;

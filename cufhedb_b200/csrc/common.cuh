@@ -36,6 +36,7 @@ enum : int {
     DEV_TIMEOUT_FULL = 1,    // consumer gave up waiting for a key chunk
     DEV_TIMEOUT_EMPTY = 2,   // producer gave up waiting for a free ring slot
     DEV_TIMEOUT_DRAIN = 3,   // producer gave up waiting for its last copies
+    DEV_TIMEOUT_MMA = 4,     // a warp gave up waiting for its tensor-core product
 };
 
 // bounded waits: polls of mbarrier.try_wait (each poll may suspend in hardware

@@ -29,8 +29,9 @@ struct cufhedb_ctx {
     std::mutex io_mu;
     bool have_sk = false;
     // measured time of one full pass of each launch shape (PBS01_SHAPES per
-    // precision FP64 / split, PBS02_SHAPES); all equal until the autotuner runs
-    float pbs01_pass_ms[2][NSHAPES] = {{1.0f, 1.0f, 1.0f}, {1.0f, 1.0f, 1.0f}};
+    // precision FP64 / split / split with the tensor-core stage, PBS02_SHAPES);
+    // all equal until the autotuner runs
+    float pbs01_pass_ms[3][NSHAPES] = {{1.0f, 1.0f, 1.0f}, {1.0f, 1.0f, 1.0f}, {1.0f, 1.0f, 1.0f}};
     float pbs02_pass_ms[NSHAPES] = {1.0f, 1.0f, 1.0f};
     uint32_t *s0_d = nullptr, *s1_d = nullptr;
     uint64_t *s2_d = nullptr;

@@ -30,10 +30,12 @@ struct Fft512TablesFold {
     float4 w32p[16];
 };
 // both sets, as the context keeps them in global memory; a kernel copies the
-// set it uses into shared memory
+// set it uses into shared memory.  tc_b: the two FP16 limbs of the constant
+// matrix of the tensor-core stage 1 (tc_stage1.cuh), hi then lo.
 struct Fft512TablesF {
     Fft512TablesPlain plain;
     Fft512TablesFold fold;
+    uint16_t tc_b[2][32 * 32];
 };
 static_assert(sizeof(Fft512TablesPlain) % 16 == 0 && sizeof(Fft512TablesFold) % 16 == 0, "16-byte copies");
 
@@ -191,9 +193,17 @@ __device__ __forceinline__ float2 cw64(float2 a, int m2)
 // is applied with the stage-1 twiddles (tw512w, q2 = 0 included), the radix-2
 // twiddles come from constants.  Same output as ffft512_fwd on fully twisted
 // inputs.
+__device__ __forceinline__ void ffft512_fwd_tw_rest(float2 v[16], float2 *xp, const Fft512TablesFold &T, int lane);
 __device__ __forceinline__ void ffft512_fwd_tw(float2 v[16], float2 *xp, const Fft512TablesFold &T, int lane)
 {
     fdft16<1>(v);
+    ffft512_fwd_tw_rest(v, xp, T, lane);
+}
+
+// everything after the first 16-point DFT: v[q2] = X[q2] of this lane (the
+// tensor-core path computes X on the tensor cores, tc_stage1.cuh)
+__device__ __forceinline__ void ffft512_fwd_tw_rest(float2 v[16], float2 *xp, const Fft512TablesFold &T, int lane)
+{
 #pragma unroll
     for (int q2 = 0; q2 < 16; ++q2) v[q2] = fcmul(v[q2], T.tw512w[q2 * 32 + lane]);
     __syncwarp();

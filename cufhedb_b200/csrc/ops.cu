@@ -291,7 +291,8 @@ int begin_ops(cufhedb_ctx *ctx, int B, int precision, Ops &o, cufhedb_stream_t s
 {
     if (!ctx) return set_error(CUFHEDB_ERR_ARG, "ctx is null");
     if (B < 0) return set_error(CUFHEDB_ERR_ARG, "negative batch");
-    if (precision != CUFHEDB_FP64 && precision != CUFHEDB_SPLIT32)
+    if (precision != CUFHEDB_FP64 && precision != CUFHEDB_SPLIT32 &&
+        precision != CUFHEDB_SPLIT32_TC)
         return set_error(CUFHEDB_ERR_ARG, "unsupported precision");
     if (o.guard.set(ctx->device) != cudaSuccess) return set_error(CUFHEDB_ERR_CUDA, "cudaSetDevice failed");
     o.c = ctx;

@@ -23,6 +23,7 @@
 #include "fft_f32.cuh"
 #include "pbs_common.cuh"
 #include "ring.cuh"
+#include "tc_stage1.cuh"
 
 #include <type_traits>
 
@@ -38,6 +39,13 @@ struct Pbs01SplitSmem {
     static constexpr int ACC_BYTES = 2 * N1 * 4;
     static constexpr int ABAR_BYTES = ((N0 * 2) + 127) / 128 * 128;
     static constexpr int PER_WARP = XP_BYTES + ACC_BYTES + ABAR_BYTES;
+    // tensor-core stage 1 only: the two FP16 limbs of B, one mbarrier per
+    // warp, the tensor-memory base address
+    static constexpr int TC_OFF = (WARP_OFF + W * PER_WARP + 1023) / 1024 * 1024;
+    static constexpr int TC_B_BYTES = 2 * TC_B_HALVES * 2;
+    static constexpr int TC_BAR_OFF = TC_OFF + TC_B_BYTES;
+    static constexpr int TC_SLOT_OFF = TC_BAR_OFF + 8 * 16;
+    static constexpr int TOTAL_TC = TC_SLOT_OFF + 16;
     static constexpr int TOTAL = WARP_OFF + W * PER_WARP;
 };
 
@@ -112,9 +120,79 @@ __device__ __forceinline__ CP pmul_first(unsigned long long vr, unsigned long lo
     return CP{f2(nvi, ki, m2(vr, kr)), f2(vi, kr, m2(vr, ki))};
 }
 
+// Tensor-core stage 1 of one warp (tc_stage1.cuh): its tensor-memory
+// columns (A double-buffered, 16 columns each, then D, 32 columns), its
+// mbarrier and phase, and the shared-memory descriptors of B's limbs.
+// (addresses are recomputed from the block's shared memory and the warp
+// index at each use instead of held in registers: the kernel runs at the
+// 255-register limit)
+template <class L>
+struct TcStage {
+    unsigned char *smem;
+    uint32_t phase;     // completed products of this warp
+
+    __device__ __forceinline__ uint32_t tlane(int warp) const
+    {
+        const uint32_t base = *reinterpret_cast<const volatile uint32_t *>(smem + L::TC_SLOT_OFF);
+        return base + 64u * warp + ((32u * (warp & 3)) << 16);
+    }
+    __device__ __forceinline__ uint64_t *bar(int warp) const
+    {
+        return reinterpret_cast<uint64_t *>(smem + L::TC_BAR_OFF) + warp;
+    }
+    // A <- the digit-d row of every lane, into buffer buf
+    __device__ __forceinline__ void put(const uint32_t w[32], int d, int buf, int warp)
+    {
+        uint32_t a[16];
+        tc_a_row(a, w, d);
+        tmem_st16(tlane(warp) + 16 * buf, a);
+        tc_fence_before();
+        __syncwarp();
+    }
+    // D = A(buf) (Bhi + Blo), issued by lane 0, completing on the warp's mbarrier
+    __device__ __forceinline__ void issue(int buf, int warp, int lane)
+    {
+        if (lane == 0) {
+            tc_fence_after();
+            const uint32_t tcol = tlane(warp) & 0xFFFFu;   // lane field 0: the MMA spans all 128 lanes
+            const uint32_t a = tcol + 16 * buf, d = tcol + 32;
+            const uint32_t b = smem_u32(smem + L::TC_OFF), limb = TC_B_HALVES * 2, kstep = 2 * TC_B_LBO;
+            umma_ts(d, a, tc_smem_desc(b, TC_B_LBO, TC_B_SBO), 0);
+            umma_ts(d, a + 8, tc_smem_desc(b + kstep, TC_B_LBO, TC_B_SBO), 1);
+            umma_ts(d, a, tc_smem_desc(b + limb, TC_B_LBO, TC_B_SBO), 1);
+            umma_ts(d, a + 8, tc_smem_desc(b + limb + kstep, TC_B_LBO, TC_B_SBO), 1);
+            umma_commit(bar(warp));
+        }
+        __syncwarp();
+    }
+    // waits for the warp's last product and reads its row: v[q] = X[q]
+    __device__ __forceinline__ void take(float2 v[16], int warp, int *err)
+    {
+        if (!mbar_wait(bar(warp), phase & 1)) report_error(err, DEV_TIMEOUT_MMA);
+        ++phase;
+        tc_fence_after();
+        uint32_t r[32];
+        tmem_ld32(tlane(warp) + 32, r);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = make_float2(__uint_as_float(r[q]), __uint_as_float(r[16 + q]));
+        tc_fence_before();
+        __syncwarp();
+    }
+};
+
+// tensor-memory columns of a block: 64 per consumer warp, rounded up to a
+// power of two (the allocation unit)
+template <int W>
+constexpr uint32_t tc_cols()
+{
+    return W * 64 <= 256 ? 256u : 512u;
+}
+
 // W consumer warps, plus a producer warp when PRODUCER (ring.cuh has both
-// feeds; the launch picks per shape, see launch_pbs01_split)
-template <int W, int S, bool PRODUCER>
+// feeds; the launch picks per shape, see launch_pbs01_split).  TC: the first
+// step of every digit transform runs on the tensor cores (tc_stage1.cuh), the
+// rest as in the CUDA-core path.
+template <int W, int S, bool PRODUCER, bool TC>
 __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_kernel(Pbs01Args a)
 {
     // the folded tables (fft_f32.cuh): the twist and untwist ride on the
@@ -130,14 +208,33 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
               (uint32_t)CHUNKS, (uint32_t)groups_of_block(ngroups, blockIdx.x, gridDim.x) * CHUNKS};
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) ring.init_by_thread0();
+    uint64_t *tc_bars = reinterpret_cast<uint64_t *>(smem + L::TC_BAR_OFF);
+    uint32_t *tc_slot = reinterpret_cast<uint32_t *>(smem + L::TC_SLOT_OFF);
+    if (threadIdx.x == 0) {
+        ring.init_by_thread0();
+        if constexpr (TC) {
+            for (int k = 0; k < W; ++k) mbar_init(&tc_bars[k], 1);
+            fence_barrier_init();
+        }
+    }
+    if constexpr (TC) {
+        if (warp == 0) tmem_alloc(tc_slot, tc_cols<W>());
+    }
     {
         const Fft512TablesF *all = reinterpret_cast<const Fft512TablesF *>(a.tables);
         const float4 *src = reinterpret_cast<const float4 *>(&all->fold);
         float4 *dst = reinterpret_cast<float4 *>(T);
         for (int i = threadIdx.x; i < (int)(sizeof(TT) / 16); i += blockDim.x) dst[i] = src[i];
+        if constexpr (TC) {
+            const float4 *bs = reinterpret_cast<const float4 *>(&all->tc_b[0][0]);
+            float4 *bd = reinterpret_cast<float4 *>(smem + L::TC_OFF);
+            for (int i = threadIdx.x; i < L::TC_B_BYTES / 16; i += blockDim.x) bd[i] = bs[i];
+            fence_proxy_async_smem();   // B is read by the tensor cores (async proxy)
+        }
     }
+    if constexpr (TC) tc_fence_before();
     __syncthreads();
+    if constexpr (TC) tc_fence_after();
     if constexpr (PRODUCER) {
         if (warp == W) {
             ring.run_producer(lane, a.err);
@@ -146,6 +243,8 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
     } else {
         if (threadIdx.x == 0) ring.prologue_by_thread0();
     }
+
+    TcStage<L> tc{smem, 0u};
 
     unsigned char *wb = smem + L::WARP_OFF + warp * L::PER_WARP;
     unsigned long long *xp = reinterpret_cast<unsigned long long *>(wb);
@@ -173,14 +272,38 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
             const bool active = ab != 0;
             CP f0[16], f1[16];
             uint32_t w[32];
+            if constexpr (TC) {
+                // the product of digit polynomial 0 is in flight before the loop
+                if (active) {
+                    digit_words1(w, acc, ab, lane);
+                    tc.put(w, 0, 0, warp);
+                    tc.issue(0, warp, lane);
+                }
+            }
 #pragma unroll 1
             for (int r = 0; r < 2 * L1; ++r, ++c) {
-                if (active && r % L1 == 0) digit_words1(w, acc + (r / L1) * N1, ab, lane);
+                float2 v[16];
+                if constexpr (TC) {
+                    // stage the next digit polynomial while this one's product
+                    // runs, take this one's, then start the next
+                    if (active) {
+                        if (r + 1 < 2 * L1) {
+                            if ((r + 1) % L1 == 0) digit_words1(w, acc + N1, ab, lane);
+                            tc.put(w, (r + 1) % L1, (r + 1) & 1, warp);
+                        }
+                        tc.take(v, warp, a.err);
+                        if (r + 1 < 2 * L1) tc.issue((r + 1) & 1, warp, lane);
+                    }
+                } else {
+                    if (active && r % L1 == 0) digit_words1(w, acc + (r / L1) * N1, ab, lane);
+                }
                 const float4 *bkc = reinterpret_cast<const float4 *>(ring.acquire(c, a.err));
                 if (active) {
-                    float2 v[16];
-                    digits_from_words_f(v, w, r % L1);
-                    ffft512_fwd_tw(v, reinterpret_cast<float2 *>(xp), *T, lane);
+                    if constexpr (!TC) {
+                        digits_from_words_f(v, w, r % L1);
+                        fdft16<1>(v);
+                    }
+                    ffft512_fwd_tw_rest(v, reinterpret_cast<float2 *>(xp), *T, lane);
                     if (r == 0) {
 #pragma unroll
                         for (int s = 0; s < 16; ++s) {
@@ -216,6 +339,15 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
         }
         __syncwarp();
     }
+    if constexpr (TC) {
+        // every product of every warp was waited for; then the columns are freed
+        tc_fence_before();
+        asm volatile("bar.sync 1, %0;" ::"r"(W * 32) : "memory");
+        if (warp == 0) {
+            tc_fence_after();
+            tmem_dealloc(*tc_slot, tc_cols<W>());
+        }
+    }
     if constexpr (!PRODUCER) {
         __syncthreads();
         if (threadIdx.x == 0) ring.drain_by_thread0(a.err);
@@ -230,45 +362,65 @@ constexpr int PBS01S_S = W == 8 ? 6 : 7;
 template <int W>
 using SplitLayout = Pbs01SplitSmem<W, PBS01S_S<W>, (int)sizeof(Fft512TablesFold)>;
 
+template <int W, bool TC>
+constexpr int split_smem_bytes()
+{
+    return TC ? SplitLayout<W>::TOTAL_TC : SplitLayout<W>::TOTAL;
+}
+
 // 7 and 4 ciphertexts per CTA run with a producer warp (8 or 5 warps), 8 per
 // CTA without one (8 warps): at most 2 warps per SM sub-partition (up to 255
 // registers); 4 per CTA leaves one consumer warp per sub-partition
 template <int W>
 constexpr bool PBS01S_PROD = W != 8;
 
-template <int W>
+template <int W, bool TC>
 static cudaError_t launch_pbs01_split_t(const Pbs01Args &a, int grid, cudaStream_t st)
 {
     constexpr bool PROD = PBS01S_PROD<W>;
-    using L = SplitLayout<W>;
-    static_assert(L::TOTAL <= 227 * 1024, "shared memory budget");
-    pbs01_split_kernel<W, PBS01S_S<W>, PROD><<<grid, (W + (PROD ? 1 : 0)) * 32, L::TOTAL, st>>>(a);
+    static_assert(split_smem_bytes<W, TC>() <= 227 * 1024, "shared memory budget");
+    pbs01_split_kernel<W, PBS01S_S<W>, PROD, TC>
+        <<<grid, (W + (PROD ? 1 : 0)) * 32, split_smem_bytes<W, TC>(), st>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t launch_pbs01_split(const Pbs01Args &a, int num_sms, int w, cudaStream_t st)
+template <bool TC>
+static cudaError_t launch_split_any(const Pbs01Args &a, int num_sms, int w, cudaStream_t st)
 {
     if (a.B <= 0) return cudaSuccess;
     const int groups = (a.B + w - 1) / w;
     const int grid = groups < num_sms ? groups : num_sms;
-    if (w == 7) return launch_pbs01_split_t<7>(a, grid, st);
-    if (w == 8) return launch_pbs01_split_t<8>(a, grid, st);
-    if (w == 4) return launch_pbs01_split_t<4>(a, grid, st);
+    if (w == 7) return launch_pbs01_split_t<7, TC>(a, grid, st);
+    if (w == 8) return launch_pbs01_split_t<8, TC>(a, grid, st);
+    if (w == 4) return launch_pbs01_split_t<4, TC>(a, grid, st);
     return cudaErrorInvalidValue;
 }
 
-template <int W>
+cudaError_t launch_pbs01_split(const Pbs01Args &a, int num_sms, int w, cudaStream_t st)
+{
+    return launch_split_any<false>(a, num_sms, w, st);
+}
+
+cudaError_t launch_pbs01_split_tc(const Pbs01Args &a, int num_sms, int w, cudaStream_t st)
+{
+    return launch_split_any<true>(a, num_sms, w, st);
+}
+
+template <int W, bool TC>
 static cudaError_t init_pbs01_split_t()
 {
-    return cudaFuncSetAttribute(pbs01_split_kernel<W, PBS01S_S<W>, PBS01S_PROD<W>>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, SplitLayout<W>::TOTAL);
+    return cudaFuncSetAttribute(pbs01_split_kernel<W, PBS01S_S<W>, PBS01S_PROD<W>, TC>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, split_smem_bytes<W, TC>());
 }
 
 cudaError_t init_pbs01_split()
 {
-    cudaError_t e = init_pbs01_split_t<7>();
-    if (e == cudaSuccess) e = init_pbs01_split_t<8>();
-    if (e == cudaSuccess) e = init_pbs01_split_t<4>();
+    cudaError_t e = init_pbs01_split_t<7, false>();
+    if (e == cudaSuccess) e = init_pbs01_split_t<8, false>();
+    if (e == cudaSuccess) e = init_pbs01_split_t<4, false>();
+    if (e == cudaSuccess) e = init_pbs01_split_t<7, true>();
+    if (e == cudaSuccess) e = init_pbs01_split_t<8, true>();
+    if (e == cudaSuccess) e = init_pbs01_split_t<4, true>();
     return e;
 }
 

@@ -72,6 +72,8 @@ struct Pbs01Args {
 cudaError_t launch_pbs01_f64(const Pbs01Args &a, int num_sms, int w, cudaStream_t st);
 // bk: split-precision key (float4 hi/lo chunk layout), tables: Fft512TablesF
 cudaError_t launch_pbs01_split(const Pbs01Args &a, int num_sms, int w, cudaStream_t st);
+// the same with the first step of every digit transform on the tensor cores
+cudaError_t launch_pbs01_split_tc(const Pbs01Args &a, int num_sms, int w, cudaStream_t st);
 
 // Launch shapes of the persistent PBS kernels, as ciphertexts per CTA: lvl01
 // 7 (with a producer warp on the split path), 8 and 4 (one warp per SM

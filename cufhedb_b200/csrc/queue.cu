@@ -68,7 +68,8 @@ extern "C" CUFHEDB_API int cufhedb_queue_run(cufhedb_ctx *ctx, const cufhedb_que
     if (nq < 0 || (nq > 0 && (!q || !latency_ms))) return set_error(CUFHEDB_ERR_ARG, "bad query list");
     if (max_batch_rows < 1 || nstreams < 1 || nstreams > 16)
         return set_error(CUFHEDB_ERR_ARG, "max_batch_rows >= 1 and 1 <= nstreams <= 16");
-    if (precision != CUFHEDB_FP64 && precision != CUFHEDB_SPLIT32)
+    if (precision != CUFHEDB_FP64 && precision != CUFHEDB_SPLIT32 &&
+        precision != CUFHEDB_SPLIT32_TC)
         return set_error(CUFHEDB_ERR_ARG, "unsupported precision");
     for (int i = 0; i < nq; ++i) {
         const cufhedb_query &x = q[i];

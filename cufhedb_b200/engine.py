@@ -189,18 +189,21 @@ class Engine:
         """the persisted launch-shape table: loaded from `path` when it was made
         for this device and parameter set, else measured for every loaded key
         (lvl01 on both precisions, lvl02) and saved to `path`.  Returns
-        {"loaded": bool, "pbs01_fp64": {...}, "pbs01_split32": {...}, "pbs02": {...}}"""
+        {"loaded": bool, "pbs01_fp64": {...}, "pbs01_split32": {...}, "pbs01_split32tc": {...},
+        "pbs02": {...}}"""
         loaded = bool(path) and self.autotune_load(path)
         if not loaded:
             if 1 in levels:
                 self.autotune_pbs01(_lib.FP64)
                 self.autotune_pbs01(_lib.SPLIT32)
+                self.autotune_pbs01(_lib.SPLIT32_TC)
             if 2 in levels:
                 self.autotune_pbs02()
             if path:
                 self.autotune_save(path)
         return {"loaded": loaded, "pbs01_fp64": self.autotune_table(1, _lib.FP64),
-                "pbs01_split32": self.autotune_table(1, _lib.SPLIT32), "pbs02": self.autotune_table(2, _lib.FP64)}
+                "pbs01_split32": self.autotune_table(1, _lib.SPLIT32),
+                "pbs01_split32tc": self.autotune_table(1, _lib.SPLIT32_TC), "pbs02": self.autotune_table(2, _lib.FP64)}
 
     def phase_lvl1(self, ct_dev, phase_dev, key_dev=None, stream=None):
         """decryption phases b - <a, s1> of lvl1 TLWEs (key: device words, or the key set's)"""

@@ -61,8 +61,10 @@ enum cufhedb_status {
 };
 
 enum cufhedb_precision {
-    CUFHEDB_FP64 = 0,   /* FP64 FFT and FP64 frequency-domain products */
-    CUFHEDB_SPLIT32 = 1 /* FP32 transforms, two-limb key, exact top-limb rounding */
+    CUFHEDB_FP64 = 0,      /* FP64 FFT and FP64 frequency-domain products */
+    CUFHEDB_SPLIT32 = 1,   /* FP32 transforms, two-limb key, exact top-limb rounding */
+    CUFHEDB_SPLIT32_TC = 2 /* SPLIT32 with the first step of every digit transform on the tensor
+                              cores (tcgen05, FP16 two-limb constants, FP32 accumulation) */
 };
 
 enum cufhedb_ksk_kind { CUFHEDB_KSK10 = 10, CUFHEDB_KSK20 = 20, CUFHEDB_KSK21 = 21 };

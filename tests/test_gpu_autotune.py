@@ -30,11 +30,12 @@ def eng2():
 
 def _force(eng, tmp_path, level, precision, shape):
     """load a table in which `shape` has the only short pass for this level"""
-    from cufhedb_b200 import FP64, SPLIT32
+    from cufhedb_b200 import FP64, SPLIT32, SPLIT32_TC
     path = str(tmp_path / "real.tbl")
     eng.autotune_save(path)
     lines = open(path).read().splitlines()
-    key = {1: {FP64: "pbs01 fp64", SPLIT32: "pbs01 split32"}, 2: {FP64: "pbs02 fp64"}}[level][precision]
+    key = {1: {FP64: "pbs01 fp64 ", SPLIT32: "pbs01 split32 ", SPLIT32_TC: "pbs01 split32tc "},
+           2: {FP64: "pbs02 fp64 "}}[level][precision]
     for i, ln in enumerate(lines):
         if ln.startswith(key):
             f = ln.split()
@@ -47,12 +48,12 @@ def _force(eng, tmp_path, level, precision, shape):
     return path
 
 
-@pytest.mark.parametrize("precision", ["split32", "fp64"])
+@pytest.mark.parametrize("precision", ["split32", "fp64", "split32tc"])
 @pytest.mark.parametrize("shape", [7, 8, 4])
 def test_every_lvl01_shape_bootstraps_correctly(eng2, tmp_path, precision, shape):
     import torch
-    from cufhedb_b200 import FP64, SPLIT32
-    prec = SPLIT32 if precision == "split32" else FP64
+    from cufhedb_b200 import FP64, SPLIT32, SPLIT32_TC
+    prec = {"split32": SPLIT32, "fp64": FP64, "split32tc": SPLIT32_TC}[precision]
     real = _force(eng2, tmp_path, 1, prec, shape)
     try:
         B = 2 * shape * eng2.num_sms + 5          # two full passes and a ragged third
@@ -103,7 +104,7 @@ def test_table_persists_and_is_refused_elsewhere(eng2, tmp_path):
     path = str(tmp_path / "tuned.tbl")
     t = eng2.autotune(path)
     assert not t["loaded"]
-    for name in ("pbs01_fp64", "pbs01_split32", "pbs02"):
+    for name in ("pbs01_fp64", "pbs01_split32", "pbs01_split32tc", "pbs02"):
         assert all(ms > 0 for ms in t[name].values()), t
     fresh = Engine(0)
     fresh.keygen(SEED, GEN_BK01)

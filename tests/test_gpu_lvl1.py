@@ -211,7 +211,8 @@ def test_api_errors(engine):
     engine.sync()
 
 
-def test_split32_pbs_decrypts_with_fp64_noise_level(engine, oracle, keys):
+@pytest.mark.parametrize("path", ["split32", "split32tc"])
+def test_split32_pbs_decrypts_with_fp64_noise_level(engine, oracle, keys, path):
     """Split-precision FP32 path: every output decrypts, and its output noise
     (phase minus the encoded +-mu) has the variance of the FP64 path's.  The
     two paths' outputs are not compared with each other: a few-unit difference
@@ -219,7 +220,8 @@ def test_split32_pbs_decrypts_with_fp64_noise_level(engine, oracle, keys):
     two correct runs carry independent rounding noise.  With 1,029 samples per
     path the variance ratio of two equal-variance noises lies within
     [0.88, 1.13] at 95 %; the bound 1.25 leaves room for that spread."""
-    from cufhedb_b200 import FP64, SPLIT32, testvec_const
+    from cufhedb_b200 import FP64, SPLIT32, SPLIT32_TC, testvec_const
+    SPLIT = SPLIT32 if path == "split32" else SPLIT32_TC
     s0, s1, _ = keys
     B = 7 * 147
     bits = np.random.default_rng(31).integers(0, 2, B)
@@ -227,7 +229,7 @@ def test_split32_pbs_decrypts_with_fp64_noise_level(engine, oracle, keys):
     xd = dev(x)
     o64, o32 = empty_dev(B * (N1 + 1)), empty_dev(B * (N1 + 1))
     engine.pbs_lvl01(xd, o64, testvec_const(MU), FP64)
-    engine.pbs_lvl01(xd, o32, testvec_const(MU), SPLIT32)
+    engine.pbs_lvl01(xd, o32, testvec_const(MU), SPLIT)
     engine.sync()
     s1u = s1.astype(np.uint64)
 

@@ -1,5 +1,6 @@
 """GPU parity against the reference's own CPU implementation on the same keys
-and inputs, for both lvl01 precisions (FP64 and split32):
+and inputs, for every lvl01 path (FP64, split32, and split32 with the
+first transform step on the tensor cores):
 
 * GateBootstrappingTLWE2TLWEFFT<lvl01param> (TFHEpp src/gatebootstrapping.cpp:
   14-23) over whole batches that land on each lvl01 launch shape (1,024
@@ -62,11 +63,19 @@ def eng_all():
     eng.close()
 
 
-@pytest.mark.parametrize("precision", ["split32", "fp64"])
+PRECISIONS = ["split32", "fp64", "split32tc"]
+
+
+def _prec(name):
+    from cufhedb_b200 import FP64, SPLIT32, SPLIT32_TC
+    return {"split32": SPLIT32, "fp64": FP64, "split32tc": SPLIT32_TC}[name]
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
 def test_pbs01_matches_reference_on_both_launch_shapes(engine, oracle, ref_keyed, keys, precision):
     import torch
-    from cufhedb_b200 import FP64, SPLIT32, testvec_const
-    prec = SPLIT32 if precision == "split32" else FP64
+    from cufhedb_b200 import testvec_const
+    prec = _prec(precision)
     s0, s1, _ = keys
     tv = np.full(N1, MU, np.uint32)
     for B, stream_id in ((1024, 0xA1), (8 * engine.num_sms, 0xA2)):
@@ -84,10 +93,9 @@ def test_pbs01_matches_reference_on_both_launch_shapes(engine, oracle, ref_keyed
         assert np.max(d) < 2 ** 25, (B, int(np.max(d)))
 
 
-@pytest.mark.parametrize("precision", ["split32", "fp64"])
+@pytest.mark.parametrize("precision", PRECISIONS)
 def test_homnand_matches_reference_batch(eng_all, oracle, ref_all, keys, precision):
-    from cufhedb_b200 import FP64, SPLIT32
-    prec = SPLIT32 if precision == "split32" else FP64
+    prec = _prec(precision)
     _, s1, _ = keys
     B = 96
     rng = np.random.default_rng(0xA3)
