@@ -74,6 +74,8 @@ def parse(argv=None):
                    help="run only the PBS kernel on `--batch` random lvl0 inputs (bootstrapping key only, "
                         "a few hundred MB on the device): the small case for ncu captures")
     p.add_argument("--level", type=int, choices=[1, 2], default=1, help="PBS level for --profile-pbs")
+    p.add_argument("--agg-leg-rows", type=int, default=65536,
+                   help="rows of the filter + grouped aggregate query timed at N=1 beside the gate steps (0: skip)")
     p.add_argument("--agg-rows", type=int, default=0,
                    help="run only the filter + grouped aggregate query (3 range predicates, 6 groups) over this "
                         "many rows, its operator DAG captured as one CUDA graph")
@@ -587,6 +589,12 @@ def run_ours(args):
                     "sample": f"first {nrows} rows of the same ciphertexts, HEDB less_than_equal<Lvl2> "
                               "(oracle/_ref) on all host threads"}
             del finputs
+        if args.filter_rows and args.agg_leg_rows:
+            from cufhedb_b200.queries import filter_group_aggregate
+            extra["aggregate"] = {
+                "workload": "filter (date range at lvl2, discount range, quantity bound) + 3 x 2 groups, "
+                            "SUM(price * (1 - discount)) and COUNT after decryption; DAG replayed as a CUDA graph",
+                "precision": head, **filter_group_aggregate(eng, args.agg_leg_rows, PREC[head], steps=1)}
         if args.error_bootstraps:
             extra["error_rate"] = error_rate(eng, args.error_bootstraps, stream)
         if cref is not None and args.noise_samples:

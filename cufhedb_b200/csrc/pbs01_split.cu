@@ -140,18 +140,20 @@ struct TcStage {
     {
         return reinterpret_cast<uint64_t *>(smem + L::TC_BAR_OFF) + warp;
     }
-    // A <- the digit-d row of every lane, into buffer buf
+    // A <- the digit-d row of every lane, into buffer buf (in flight until
+    // issue(), which waits for it)
     __device__ __forceinline__ void put(const uint32_t w[32], int d, int buf, int warp)
     {
         uint32_t a[16];
         tc_a_row(a, w, d);
         tmem_st16(tlane(warp) + 16 * buf, a);
-        tc_fence_before();
-        __syncwarp();
     }
     // D = A(buf) (Bhi + Blo), issued by lane 0, completing on the warp's mbarrier
     __device__ __forceinline__ void issue(int buf, int warp, int lane)
     {
+        tmem_wait_st();
+        tc_fence_before();
+        __syncwarp();
         if (lane == 0) {
             tc_fence_after();
             const uint32_t tcol = tlane(warp) & 0xFFFFu;   // lane field 0: the MMA spans all 128 lanes
@@ -288,8 +290,11 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
                     // runs, take this one's, then start the next
                     if (active) {
                         if (r + 1 < 2 * L1) {
-                            if ((r + 1) % L1 == 0) digit_words1(w, acc + N1, ab, lane);
-                            tc.put(w, (r + 1) % L1, (r + 1) & 1, warp);
+                            // the words are recomputed for each digit polynomial
+                            // (not carried across the transform: register room)
+                            uint32_t wn[32];
+                            digit_words1(wn, acc + ((r + 1) / L1) * N1, ab, lane);
+                            tc.put(wn, (r + 1) % L1, (r + 1) & 1, warp);
                         }
                         tc.take(v, warp, a.err);
                         if (r + 1 < 2 * L1) tc.issue((r + 1) & 1, warp, lane);

@@ -94,7 +94,8 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// this lane's 16 32-bit columns at taddr (lane field = the warp's sub-partition)
+// this lane's 16 32-bit columns at taddr (lane field = the warp's
+// sub-partition); tmem_wait_st() before anything reads them
 __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t v[16])
 {
     asm volatile(
@@ -103,8 +104,8 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t v[16])
         "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]),
         "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
         : "memory");
-    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t v[32])
 {
