@@ -517,6 +517,78 @@ int cufhedb_load_keyfile(cufhedb_ctx *ctx, const char *path, uint32_t *sk_out)
     return CUFHEDB_OK;
 }
 
+// ---- TFHEpp cereal key archives ---------------------------------------------
+// The reference's key files (src/HEDB/utils/serialize.cpp:7-60,
+// src/ARCEDB/utils/serialize.cpp) are cereal PortableBinary archives of
+// EvalKey::serialize_<key>(ar) = ar(params, unique_ptr<key>)
+// (thirdparty/TFHEpp/include/cloudkey.hpp:149-228): one endianness byte (1 =
+// little endian), the parameter block, the pointer's valid byte (1), then the
+// key's std::arrays of arithmetic values as one raw block, little endian, in
+// TFHEpp's in-memory layout.  The key is therefore the file's last
+// sizeof(key) bytes; the checks below pin the bytes around it.
+static size_t cereal_key_bytes(int kind)
+{
+    switch (kind) {
+    case CUFHEDB_CEREAL_BKFFT01: return BK01_WORDS * sizeof(double);
+    case CUFHEDB_CEREAL_BKFFT02: return BK02_WORDS * sizeof(double);
+    case CUFHEDB_CEREAL_KSK10: return ksk_words(10) * 4;
+    case CUFHEDB_CEREAL_KSK20: return ksk_words(20) * 4;
+    case CUFHEDB_CEREAL_KSK21: return ksk_words(21) * 4;
+    default: return 0;
+    }
+}
+
+int cufhedb_cereal_key_payload(const char *path, int kind, uint64_t *offset, uint64_t *bytes)
+{
+    NEED(path && offset && bytes, "null argument");
+    const size_t n = cereal_key_bytes(kind);
+    NEED(n > 0, "unknown cereal key kind");
+    FileCloser fc{fopen(path, "rb")};
+    if (!fc.f) return fail(CUFHEDB_ERR_ARG, std::string("cannot open ") + path);
+    if (fseeko(fc.f, 0, SEEK_END) != 0) return fail(CUFHEDB_ERR_ARG, "cannot size the archive");
+    const off_t size = ftello(fc.f);
+    if (size < (off_t)(n + 2)) return fail(CUFHEDB_ERR_ARG, "archive smaller than the key it should hold");
+    unsigned char endian = 0, valid = 0;
+    rewind(fc.f);
+    if (fread(&endian, 1, 1, fc.f) != 1) return fail(CUFHEDB_ERR_ARG, "short read");
+    if (fseeko(fc.f, size - (off_t)n - 1, SEEK_SET) != 0 || fread(&valid, 1, 1, fc.f) != 1)
+        return fail(CUFHEDB_ERR_ARG, "short read");
+    if (endian != 1) return fail(CUFHEDB_ERR_ARG, "not a little-endian cereal portable binary archive");
+    if (valid != 1) return fail(CUFHEDB_ERR_ARG, "the archive's key pointer is empty or of another key type");
+    *offset = (uint64_t)(size - (off_t)n);
+    *bytes = n;
+    return CUFHEDB_OK;
+}
+
+int cufhedb_load_cereal_key(cufhedb_ctx *ctx, const char *path, int kind)
+{
+    NEED(ctx != nullptr, "ctx is null");
+    uint64_t off = 0, n = 0;
+    int rc = cufhedb_cereal_key_payload(path, kind, &off, &n);
+    if (rc) return rc;
+    FileCloser fc{fopen(path, "rb")};
+    if (!fc.f || fseeko(fc.f, (off_t)off, SEEK_SET) != 0) return fail(CUFHEDB_ERR_ARG, "cannot seek in the archive");
+    if (kind == CUFHEDB_CEREAL_BKFFT01 || kind == CUFHEDB_CEREAL_BKFFT02) {
+        std::vector<double> bk(n / sizeof(double));
+        if (fread(bk.data(), 1, n, fc.f) != n) return fail(CUFHEDB_ERR_ARG, "short read (bootstrapping key)");
+        return kind == CUFHEDB_CEREAL_BKFFT01 ? cufhedb_load_bkfft_lvl01(ctx, bk.data())
+                                              : cufhedb_load_bkfft_lvl02(ctx, bk.data());
+    }
+    const int ksk = kind == CUFHEDB_CEREAL_KSK10 ? 10 : kind == CUFHEDB_CEREAL_KSK20 ? 20 : 21;
+    const int slot = ksk_slot(ksk);
+    DeviceGuard g(ctx->device);
+    rc = ensure_alloc((void **)&ctx->ksk[slot], n);
+    if (rc) return rc;
+    PinnedBuf buf;
+    CK(cudaMallocHost(&buf.p, KF_CHUNK));
+    for (size_t o = 0; o < n; o += KF_CHUNK) {
+        const size_t m = std::min(KF_CHUNK, (size_t)n - o);
+        if (fread(buf.p, 1, m, fc.f) != m) return fail(CUFHEDB_ERR_ARG, "short read (key-switching key)");
+        CK(cudaMemcpy(reinterpret_cast<char *>(ctx->ksk[slot]) + o, buf.p, m, cudaMemcpyHostToDevice));
+    }
+    return CUFHEDB_OK;
+}
+
 int cufhedb_save_keyfile(cufhedb_ctx *ctx, const char *path, const uint32_t *sk)
 {
     NEED(ctx && path, "null argument");

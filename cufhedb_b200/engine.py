@@ -116,6 +116,12 @@ class Engine:
         skp = None if sk is None else _ptr(np.ascontiguousarray(sk, np.uint32))
         check(self.lib.cufhedb_save_keyfile(self.ctx, path.encode(), skp))
 
+    CEREAL = {"bkfft01": 1, "bkfft02": 2, "ksk10": 10, "ksk20": 20, "ksk21": 21}
+
+    def load_cereal_key(self, path: str, kind: str):
+        """a key from a TFHEpp cereal archive (the reference's serialize.cpp files)"""
+        check(self.lib.cufhedb_load_cereal_key(self.ctx, path.encode(), self.CEREAL[kind]))
+
     def export_bk_lvl01(self) -> np.ndarray:
         out = np.zeros(BK01_SHAPE, np.uint32)
         check(self.lib.cufhedb_export_bk_lvl01(self.ctx, _ptr(out)))

@@ -153,6 +153,23 @@ CUFHEDB_API int cufhedb_secret_keys(uint64_t seed, uint32_t *s0, uint32_t *s1, u
  * deterministic key set's lvl1 key when sk is NULL, or zeros. */
 CUFHEDB_API int cufhedb_load_keyfile(cufhedb_ctx *ctx, const char *path, uint32_t *sk_out);
 CUFHEDB_API int cufhedb_save_keyfile(cufhedb_ctx *ctx, const char *path, const uint32_t *sk);
+/* TFHEpp cereal key archives, as the reference's key tools write them
+ * (src/HEDB/utils/serialize.cpp:7-60: cereal::PortableBinaryOutputArchive of
+ * EvalKey::serialize_bkfftlvl01 / _bkfftlvl02 / _iksklvl10 / _iksklvl20 /
+ * _iksklvl21, thirdparty/TFHEpp/include/cloudkey.hpp:149-228).  payload:
+ * host-only, locates and checks the key inside the archive (the last
+ * sizeof(key) bytes, after the parameter block and the pointer's valid byte);
+ * load: reads it into the context like cufhedb_load_bkfft_lvl01/02 /
+ * cufhedb_load_ksk (key-switching keys streamed in 64 MB pieces). */
+enum cufhedb_cereal_kind {
+    CUFHEDB_CEREAL_BKFFT01 = 1,
+    CUFHEDB_CEREAL_BKFFT02 = 2,
+    CUFHEDB_CEREAL_KSK10 = 10,
+    CUFHEDB_CEREAL_KSK20 = 20,
+    CUFHEDB_CEREAL_KSK21 = 21
+};
+CUFHEDB_API int cufhedb_cereal_key_payload(const char *path, int kind, uint64_t *offset, uint64_t *bytes);
+CUFHEDB_API int cufhedb_load_cereal_key(cufhedb_ctx *ctx, const char *path, int kind);
 /* deterministic lvl1 TLWE encryptions of B messages (device arrays), counter
  * blocks idx0.. of generator stream `stream_id` (test/benchmark inputs) */
 CUFHEDB_API int cufhedb_encrypt_lvl1(cufhedb_ctx *ctx, uint64_t seed, uint64_t stream_id, uint64_t idx0, const uint32_t *msg,

@@ -368,6 +368,7 @@ class RefTFHEpp:
         _sig(L, "tref_compare_lvl2", [vp, _u32p, _u64p, _u64p, i32, u32, i32])
         _sig(L, "tref_homand", [vp, _u32p, _u32p, _u32p, i32])
         _sig(L, "tref_compare_lvl1_batch", [vp, _u32p, _u32p, _u32p, i32, i32, u32, i32, i32])
+        _sig(L, "tref_save_cereal", [vp, i32, C.c_char_p], i32)
         _sig(L, "tref_compare_lvl2_batch", [vp, _u32p, _u64p, _u64p, i32, i32, u32, i32, i32])
         _sig(L, "tref_arc_digit_lvl1", [_u32p, i32, _u32p, _f64p])
         _sig(L, "tref_arc_compare_batch", [vp, _u32p, i32, _u32p, _f64p, i32, i32, i32])
@@ -512,6 +513,15 @@ class RefTFHEpp:
                                            np.ascontiguousarray(c2, np.uint64), n, op, plain_bits, int(logic),
                                            nthreads)
         return out
+
+    CEREAL = {"bkfft01": 1, "bkfft02": 2, "ksk10": 10, "ksk20": 20, "ksk21": 21}
+
+    def save_cereal(self, kind, path):
+        """the context's key as the reference's key tools archive it (cereal
+        PortableBinary, EvalKey::serialize_<key>)"""
+        rc = self.L.tref_save_cereal(self.ctx, self.CEREAL[kind], path.encode())
+        if rc != 0:
+            raise RuntimeError(f"tref_save_cereal({kind}) failed")
 
     def homand(self, ca, cb, logic=True):
         out = np.zeros(N1 + 1, np.uint32)

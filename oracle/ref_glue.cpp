@@ -10,6 +10,7 @@
 
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <thread>
 #include <vector>
 #include <atomic>
@@ -138,6 +139,27 @@ size_t tref_ksk_bytes(int kind)
     if (kind == 10) return sizeof(KeySwitchingKey<lvl10param>);
     if (kind == 20) return sizeof(KeySwitchingKey<lvl20param>);
     if (kind == 21) return sizeof(KeySwitchingKey<lvl21param>);
+    return 0;
+}
+
+// Writes one key of the context as the reference's key tools do
+// (src/HEDB/utils/serialize.cpp:7-60): a cereal PortableBinary archive of
+// EvalKey::serialize_<key> (thirdparty/TFHEpp/include/cloudkey.hpp:149-228).
+// kind: 1 bkfftlvl01, 2 bkfftlvl02, 10 iksklvl10, 20 iksklvl20, 21 iksklvl21.
+// Returns 0, or -1 for an unknown kind or an unset key.
+int tref_save_cereal(void *p, int kind, const char *path)
+{
+    RefCtx *c = static_cast<RefCtx *>(p);
+    std::ofstream ofs{path, std::ios::binary};
+    cereal::PortableBinaryOutputArchive ar(ofs);
+    switch (kind) {
+    case 1: if (!c->ek.bkfftlvl01) return -1; c->ek.serialize_bkfftlvl01(ar); break;
+    case 2: if (!c->ek.bkfftlvl02) return -1; c->ek.serialize_bkfftlvl02(ar); break;
+    case 10: if (!c->ek.iksklvl10) return -1; c->ek.serialize_iksklvl10(ar); break;
+    case 20: if (!c->ek.iksklvl20) return -1; c->ek.serialize_iksklvl20(ar); break;
+    case 21: if (!c->ek.iksklvl21) return -1; c->ek.serialize_iksklvl21(ar); break;
+    default: return -1;
+    }
     return 0;
 }
 

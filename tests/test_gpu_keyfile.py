@@ -56,3 +56,34 @@ def test_keyfile_rejects_wrong_size(tmp_path):
         e.load_keyfile(str(path))
     assert err.value.code == 1
     e.close()
+
+
+def test_cereal_archives_load_into_a_context(ref_keyed, oracle, keys, bk01, tmp_path):
+    """The reference's cereal key archives (src/HEDB/utils/serialize.cpp) load
+    into a fresh context: the lvl01 bootstrapping key recovers the integer key
+    exactly, and with the lvl10 key-switching key from its archive the
+    context's gates decrypt."""
+    import torch
+    from cufhedb_b200 import Engine
+    from oracle.oracle import N1, NS_LVL1
+    s0, s1, _ = keys
+    p_bk = str(tmp_path / "bkfftlvl01.key")
+    ref_keyed.save_cereal("bkfft01", p_bk)
+    ptr, _ = ref_keyed.ksk_view(10)
+    oracle.ksk_full_into(10, SEED, keys, ptr)
+    p_ks = str(tmp_path / "iksklvl10.key")
+    ref_keyed.save_cereal("ksk10", p_ks)
+    eng = Engine(0)
+    eng.load_cereal_key(p_bk, "bkfft01")
+    eng.load_cereal_key(p_ks, "ksk10")
+    os.unlink(p_ks)
+    assert np.array_equal(eng.export_bk_lvl01(), bk01)
+    B = 32
+    rng = np.random.default_rng(8)
+    a, b = rng.integers(0, 2, B), rng.integers(0, 2, B)
+    enc = lambda bits, base: np.stack([oracle.tlwe32((1 << 29) if t else (-(1 << 29)) & 0xFFFFFFFF, s1, NS_LVL1,
+                                                     SEED, 0xE1, base + i) for i, t in enumerate(bits)])
+    out = eng.gate_lvl1_host("NAND", enc(a, 0), enc(b, B))
+    ph = [(int(oracle.phase32(o, s1)) + 2 ** 31) % 2 ** 32 - 2 ** 31 for o in out]
+    assert np.array_equal((np.array(ph) > 0).astype(int), 1 - (a & b))
+    eng.close()
