@@ -103,6 +103,9 @@ SIGNATURES = {
     "cufhedb_compare": [_vp, _i32, _i32, _vp, _vp, _vp, _i32, _u32, _i32, _i32, _vp],
     "cufhedb_queue_run": [_vp, _vp, _i32, _i32, _i32, _i32, _vp, _vp],
     "cufhedb_cereal_key_payload": [C.c_char_p, _i32, _vp, _vp],
+    "cufhedb_compare_host": [_vp, _i32, _i32, _vp, _vp, _vp, _i32, _u32, _i32, _i32],
+    "cufhedb_gate_lvl1_host_multi": [_vp, _i32, _i32, _vp, _vp, _vp, _i32, _i32],
+    "cufhedb_compare_host_multi": [_vp, _i32, _i32, _i32, _vp, _vp, _vp, _i32, _u32, _i32, _i32],
     "cufhedb_load_cereal_key": [_vp, C.c_char_p, _i32],
     "cufhedb_graph_begin": [_vp, _vp],
     "cufhedb_graph_end": [_vp, _vp, C.POINTER(_vp)],

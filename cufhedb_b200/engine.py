@@ -423,3 +423,49 @@ class Engine:
         check(self.lib.cufhedb_gate_lvl1_host(self.ctx, _lib.GATES[gate], _ptr(ca), _ptr(cb), _ptr(out),
                                               ca.shape[0], precision))
         return out
+
+
+def _ctx_array(engines):
+    arr = (C.c_void_p * len(engines))()
+    for i, e in enumerate(engines):
+        arr[i] = e.ctx
+    return arr
+
+
+def compare_host(engine: Engine, op: str, level: int, c1: np.ndarray, c2: np.ndarray, plain_bits: int,
+                 logic: bool = True, precision: int = _lib.FP64) -> np.ndarray:
+    """cufhedb_compare on host arrays (B x (N+1) words of `level`); returns B lvl1 TLWEs"""
+    dt = np.uint32 if level == 1 else np.uint64
+    width = (N1 if level == 1 else N2) + 1
+    c1 = np.ascontiguousarray(c1, dt).reshape(-1, width)
+    c2 = np.ascontiguousarray(c2, dt).reshape(-1, width)
+    out = np.zeros((c1.shape[0], N1 + 1), np.uint32)
+    check(engine.lib.cufhedb_compare_host(engine.ctx, _lib.COMPARE[op], level, _ptr(c1), _ptr(c2), _ptr(out),
+                                          c1.shape[0], plain_bits, int(logic), precision))
+    return out
+
+
+def gate_lvl1_host_multi(engines, gate: str, ca: np.ndarray, cb: np.ndarray, precision: int = _lib.FP64):
+    """HomGate over host arrays, rows sharded over the engines' contexts
+    (one per GPU), one host thread each"""
+    ca = np.ascontiguousarray(ca, np.uint32).reshape(-1, N1 + 1)
+    cb = np.ascontiguousarray(cb, np.uint32).reshape(-1, N1 + 1)
+    out = np.zeros_like(ca)
+    lib = engines[0].lib
+    check(lib.cufhedb_gate_lvl1_host_multi(_ctx_array(engines), len(engines), _lib.GATES[gate], _ptr(ca), _ptr(cb),
+                                           _ptr(out), ca.shape[0], precision))
+    return out
+
+
+def compare_host_multi(engines, op: str, level: int, c1: np.ndarray, c2: np.ndarray, plain_bits: int,
+                       logic: bool = True, precision: int = _lib.FP64) -> np.ndarray:
+    """compare_host with the rows sharded over the engines' contexts"""
+    dt = np.uint32 if level == 1 else np.uint64
+    width = (N1 if level == 1 else N2) + 1
+    c1 = np.ascontiguousarray(c1, dt).reshape(-1, width)
+    c2 = np.ascontiguousarray(c2, dt).reshape(-1, width)
+    out = np.zeros((c1.shape[0], N1 + 1), np.uint32)
+    lib = engines[0].lib
+    check(lib.cufhedb_compare_host_multi(_ctx_array(engines), len(engines), _lib.COMPARE[op], level, _ptr(c1),
+                                         _ptr(c2), _ptr(out), c1.shape[0], plain_bits, int(logic), precision))
+    return out

@@ -345,6 +345,22 @@ CUFHEDB_API int cufhedb_extprod_lvl1_host(cufhedb_ctx *ctx, const uint32_t *trlw
 CUFHEDB_API int cufhedb_gate_lvl1_host(cufhedb_ctx *ctx, int gate, const uint32_t *ca, const uint32_t *cb, uint32_t *out, int B,
                            int precision);
 
+/* cufhedb_compare on host buffers (c1, c2: B ciphertexts of `level`; out: B
+ * lvl1 TLWEs), synchronous like the other *_host calls */
+CUFHEDB_API int cufhedb_compare_host(cufhedb_ctx *ctx, int op, int level, const void *c1, const void *c2,
+                                     uint32_t *out_lvl1, int B, uint32_t plain_bits, int logic, int precision);
+/* Row sharding over several contexts (one per GPU; the reference binds device
+ * 0 only, src/cuHEDB/gatebootstrap_gpu.cuh:11-15): the B rows split into
+ * nctx contiguous slices, each run by its own host thread through that
+ * context's host-buffer call; results land in `out` in row order.  Every
+ * context needs the keys the operator uses.  No data crosses between
+ * devices. */
+CUFHEDB_API int cufhedb_gate_lvl1_host_multi(cufhedb_ctx *const *ctxs, int nctx, int gate, const uint32_t *ca,
+                                             const uint32_t *cb, uint32_t *out, int B, int precision);
+CUFHEDB_API int cufhedb_compare_host_multi(cufhedb_ctx *const *ctxs, int nctx, int op, int level, const void *c1,
+                                           const void *c2, uint32_t *out_lvl1, int B, uint32_t plain_bits, int logic,
+                                           int precision);
+
 /* Self-test of the kernels' bounded waits (no counterpart in the reference,
  * which has none): one block waits `polls` times (1 .. 2^20) for a key-ring
  * chunk that is never issued, gives up, records the failure and returns.
