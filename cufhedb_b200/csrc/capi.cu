@@ -54,12 +54,28 @@ constexpr size_t BK01_WORDS = BK01_ROWS * 2 * N1;
 constexpr size_t BK02_ROWS = (size_t)N0 * 2 * L2;   // TRGSW rows of the lvl02 key
 constexpr size_t BK02_WORDS = BK02_ROWS * 2 * N2;
 
-size_t ksk_words(int kind)
+// key-switching keys: rows (i, j, digit value) of a TLWE each; TFHEpp's
+// layout (and the files') packs rows of row_words; the device layout pads
+// every row to ksk_pitch(row_words) words
+size_t ksk_rows(int kind)
 {
-    if (kind == 10) return (size_t)1024 * 2 * 1023 * (N0 + 1);
-    if (kind == 20) return (size_t)2048 * 2 * 1023 * (N0 + 1);
-    if (kind == 21) return (size_t)2048 * 10 * 7 * (N1 + 1);
+    if (kind == 10) return (size_t)1024 * 2 * 1023;
+    if (kind == 20) return (size_t)2048 * 2 * 1023;
+    if (kind == 21) return (size_t)2048 * 10 * 7;
     return 0;
+}
+size_t ksk_row_words(int kind) { return kind == 21 ? N1 + 1 : N0 + 1; }
+size_t ksk_words(int kind) { return ksk_rows(kind) * ksk_row_words(kind); }
+size_t ksk_dev_bytes(int kind) { return ksk_rows(kind) * ksk_pitch((int)ksk_row_words(kind)) * sizeof(uint32_t); }
+
+// rows [r0, r0 + n) from the packed host layout into the device layout, pad
+// words zeroed
+cudaError_t ksk_rows_to_device(uint32_t *dev, int kind, size_t r0, const void *host, size_t n)
+{
+    const size_t rw = ksk_row_words(kind), pw = (size_t)ksk_pitch((int)rw);
+    cudaError_t e = cudaMemcpy2D(dev + r0 * pw, pw * 4, host, rw * 4, rw * 4, n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset2D(dev + r0 * pw + rw, pw * 4, 0, (pw - rw) * 4, n);
+    return e;
 }
 
 int ksk_slot(int kind) { return kind == 10 ? 0 : kind == 20 ? 1 : kind == 21 ? 2 : -1; }
@@ -454,10 +470,9 @@ int cufhedb_load_ksk(cufhedb_ctx *ctx, int kind, const uint32_t *ksk)
     const int slot = ksk_slot(kind);
     NEED(slot >= 0, "unknown key-switching key kind");
     DeviceGuard g(ctx->device);
-    const size_t bytes = ksk_words(kind) * sizeof(uint32_t);
-    int rc = ensure_alloc((void **)&ctx->ksk[slot], bytes);
+    int rc = ensure_alloc((void **)&ctx->ksk[slot], ksk_dev_bytes(kind));
     if (rc) return rc;
-    CK(cudaMemcpy(ctx->ksk[slot], ksk, bytes, cudaMemcpyHostToDevice));
+    CK(ksk_rows_to_device(ctx->ksk[slot], kind, 0, ksk, ksk_rows(kind)));
     return CUFHEDB_OK;
 }
 
@@ -484,6 +499,21 @@ struct PinnedBuf {
     ~PinnedBuf() { cudaFreeHost(p); }
 };
 
+// a whole key-switching key from a file (packed rows) into the device layout,
+// through a pinned staging buffer of whole rows
+int ksk_from_file(uint32_t *dev, int kind, FILE *f)
+{
+    const size_t rb = ksk_row_words(kind) * 4, rows = ksk_rows(kind), per = KF_CHUNK / rb;
+    PinnedBuf buf;
+    CK(cudaMallocHost(&buf.p, per * rb));
+    for (size_t r0 = 0; r0 < rows; r0 += per) {
+        const size_t m = std::min(per, rows - r0);
+        if (fread(buf.p, 1, m * rb, f) != m * rb) return fail(CUFHEDB_ERR_ARG, "short read (key-switching key)");
+        CK(ksk_rows_to_device(dev, kind, r0, buf.p, m));
+    }
+    return CUFHEDB_OK;
+}
+
 }  // namespace
 
 int cufhedb_load_keyfile(cufhedb_ctx *ctx, const char *path, uint32_t *sk_out)
@@ -504,15 +534,10 @@ int cufhedb_load_keyfile(cufhedb_ctx *ctx, const char *path, uint32_t *sk_out)
     int rc = cufhedb_load_bkfft_lvl01(ctx, bk.data());
     if (rc) return rc;
     DeviceGuard g(ctx->device);
-    rc = ensure_alloc((void **)&ctx->ksk[0], KF_KSK_BYTES);
+    rc = ensure_alloc((void **)&ctx->ksk[0], ksk_dev_bytes(10));
     if (rc) return rc;
-    PinnedBuf buf;
-    CK(cudaMallocHost(&buf.p, KF_CHUNK));
-    for (size_t off = 0; off < KF_KSK_BYTES; off += KF_CHUNK) {
-        const size_t n = std::min(KF_CHUNK, KF_KSK_BYTES - off);
-        if (fread(buf.p, 1, n, fc.f) != n) return fail(CUFHEDB_ERR_ARG, "short read (key-switching key)");
-        CK(cudaMemcpy(reinterpret_cast<char *>(ctx->ksk[0]) + off, buf.p, n, cudaMemcpyHostToDevice));
-    }
+    rc = ksk_from_file(ctx->ksk[0], 10, fc.f);
+    if (rc) return rc;
     if (sk_out) std::memcpy(sk_out, sk.data(), KF_SK_BYTES);
     return CUFHEDB_OK;
 }
@@ -577,16 +602,9 @@ int cufhedb_load_cereal_key(cufhedb_ctx *ctx, const char *path, int kind)
     const int ksk = kind == CUFHEDB_CEREAL_KSK10 ? 10 : kind == CUFHEDB_CEREAL_KSK20 ? 20 : 21;
     const int slot = ksk_slot(ksk);
     DeviceGuard g(ctx->device);
-    rc = ensure_alloc((void **)&ctx->ksk[slot], n);
+    rc = ensure_alloc((void **)&ctx->ksk[slot], ksk_dev_bytes(ksk));
     if (rc) return rc;
-    PinnedBuf buf;
-    CK(cudaMallocHost(&buf.p, KF_CHUNK));
-    for (size_t o = 0; o < n; o += KF_CHUNK) {
-        const size_t m = std::min(KF_CHUNK, (size_t)n - o);
-        if (fread(buf.p, 1, m, fc.f) != m) return fail(CUFHEDB_ERR_ARG, "short read (key-switching key)");
-        CK(cudaMemcpy(reinterpret_cast<char *>(ctx->ksk[slot]) + o, buf.p, m, cudaMemcpyHostToDevice));
-    }
-    return CUFHEDB_OK;
+    return ksk_from_file(ctx->ksk[slot], ksk, fc.f);
 }
 
 int cufhedb_save_keyfile(cufhedb_ctx *ctx, const char *path, const uint32_t *sk)
@@ -610,12 +628,15 @@ int cufhedb_save_keyfile(cufhedb_ctx *ctx, const char *path, const uint32_t *sk)
     if (!fc.f) return fail(CUFHEDB_ERR_ARG, std::string("cannot create key file ") + path);
     if (fwrite(skw.data(), 1, KF_SK_BYTES, fc.f) != KF_SK_BYTES || fwrite(bk.data(), 1, KF_BK_BYTES, fc.f) != KF_BK_BYTES)
         return fail(CUFHEDB_ERR_ARG, "short write");
+    const size_t rw = ksk_row_words(10), pw = (size_t)ksk_pitch((int)rw), rows = ksk_rows(10),
+                 per = KF_CHUNK / (rw * 4);
     PinnedBuf buf;
-    CK(cudaMallocHost(&buf.p, KF_CHUNK));
-    for (size_t off = 0; off < KF_KSK_BYTES; off += KF_CHUNK) {
-        const size_t n = std::min(KF_CHUNK, KF_KSK_BYTES - off);
-        CK(cudaMemcpy(buf.p, reinterpret_cast<const char *>(ctx->ksk[0]) + off, n, cudaMemcpyDeviceToHost));
-        if (fwrite(buf.p, 1, n, fc.f) != n) return fail(CUFHEDB_ERR_ARG, "short write (key-switching key)");
+    CK(cudaMallocHost(&buf.p, per * rw * 4));
+    for (size_t r0 = 0; r0 < rows; r0 += per) {
+        const size_t m = std::min(per, rows - r0);
+        CK(cudaMemcpy2D(buf.p, rw * 4, ctx->ksk[0] + r0 * pw, pw * 4, rw * 4, m, cudaMemcpyDeviceToHost));
+        if (fwrite(buf.p, 1, m * rw * 4, fc.f) != m * rw * 4)
+            return fail(CUFHEDB_ERR_ARG, "short write (key-switching key)");
     }
     if (fflush(fc.f) != 0) return fail(CUFHEDB_ERR_ARG, "flush failed");
     return CUFHEDB_OK;
@@ -682,7 +703,7 @@ int cufhedb_keygen(cufhedb_ctx *ctx, uint64_t seed, unsigned flags)
     const unsigned kflags[3] = {CUFHEDB_GEN_KSK10, CUFHEDB_GEN_KSK20, CUFHEDB_GEN_KSK21};
     for (int t = 0; t < 3; ++t) {
         if (!(flags & kflags[t])) continue;
-        rc = ensure_alloc((void **)&ctx->ksk[t], ksk_words(kinds[t]) * sizeof(uint32_t));
+        rc = ensure_alloc((void **)&ctx->ksk[t], ksk_dev_bytes(kinds[t]));
         if (rc) return rc;
         const void *dom = kinds[t] == 10 ? (const void *)ctx->s1_d : (const void *)ctx->s2_d;
         const uint32_t *tgt = kinds[t] == 21 ? ctx->s1_d : ctx->s0_d;
@@ -746,11 +767,11 @@ int cufhedb_export_ksk_rows(cufhedb_ctx *ctx, int kind, const uint64_t *rows, in
     NEED(slot >= 0, "unknown key-switching key kind");
     if (!ctx->ksk[slot]) return fail(CUFHEDB_ERR_NOKEY, "key-switching key not loaded");
     DeviceGuard g(ctx->device);
-    const size_t width = kind == 21 ? N1 + 1 : N0 + 1;
-    const size_t nrows = ksk_words(kind) / width;
+    const size_t width = ksk_row_words(kind), pitch = (size_t)ksk_pitch((int)width);
+    const size_t nrows = ksk_rows(kind);
     for (int r = 0; r < n; ++r) {
         NEED(rows[r] < nrows, "row index out of range");
-        CK(cudaMemcpy(out + r * width, ctx->ksk[slot] + rows[r] * width, width * 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(out + r * width, ctx->ksk[slot] + rows[r] * pitch, width * 4, cudaMemcpyDeviceToHost));
     }
     return CUFHEDB_OK;
 }

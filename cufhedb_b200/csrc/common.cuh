@@ -18,6 +18,10 @@ constexpr int N2 = 2048, L2 = 4, BGBIT2 = 9;
 constexpr int KS10_BASEBIT = 10, KS10_T = 2;
 constexpr int KS20_BASEBIT = 10, KS20_T = 2;
 constexpr int KS21_BASEBIT = 3, KS21_T = 10;
+// Key-switching key rows live in HBM with their words padded to a multiple of
+// four (16 bytes: lvl0 rows 673 -> 676 words, lvl1 rows 1025 -> 1028), the
+// pad words zero, so that the gather reads each row with 16-byte loads.
+__host__ __device__ constexpr int ksk_pitch(int row_words) { return (row_words + 3) & ~3; }
 
 // gadget decomposition constants (thirdparty/TFHEpp/src/trgsw.cpp:9-39)
 constexpr uint32_t DEC1_OFFSET = (32u << 26) + (32u << 20) + (32u << 14);   // sum Bg/2 * 2^(32-i*Bgbit)

@@ -6,7 +6,8 @@
 //     a_ij = ((a_i + prec_offset) >> (w - (j+1) basebit)) & (2^basebit - 1)
 //     if a_ij != 0: res -= ksk[i][j][a_ij - 1]
 // The reference runs this on the host for every GPU bootstrap
-// (src/cuHEDB/gatebootstrap_gpu.cuh:42,133).  Here it is an HBM-bound gather:
+// (src/cuHEDB/gatebootstrap_gpu.cuh:42,133).  Here it is an HBM-bound gather
+// over key rows padded to 16-byte multiples (ksk_pitch), read as uint4:
 // one CTA per ciphertext walks the input coefficients in chunks of NT; each
 // chunk's digits are decoded into a shared list of selected key rows (in key
 // order), then
@@ -20,36 +21,63 @@ namespace cfdb {
 
 namespace {
 
-template <int NOUT, int NT>
-__device__ __forceinline__ void gather_rows(const uint32_t *__restrict__ ksk, const uint32_t *rowid, int nrows,
-                                            uint32_t *acc)
+// a 16-byte read-only load, issued where it stands (volatile: the U loads of
+// a group are all in flight before the first subtraction)
+__device__ __forceinline__ uint4 ldg_v4(const uint4 *p)
 {
-    constexpr int PER = (NOUT + NT - 1) / NT;
-    constexpr int U = 4;
+    uint4 v;
+    asm volatile("ld.global.nc.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p));
+    return v;
+}
+
+// a -= x, placed after the group's loads (volatile, like them)
+__device__ __forceinline__ void sub_v4(uint4 &a, const uint4 &x)
+{
+    asm volatile("sub.u32 %0, %0, %4;\n\tsub.u32 %1, %1, %5;\n\tsub.u32 %2, %2, %6;\n\tsub.u32 %3, %3, %7;"
+                 : "+r"(a.x), "+r"(a.y), "+r"(a.z), "+r"(a.w)
+                 : "r"(x.x), "r"(x.y), "r"(x.z), "r"(x.w));
+}
+
+// acc[p] -= row[t + p NT] (16-byte words of the padded rows) over the listed
+// rows, U rows' loads in flight per thread
+template <int NP4, int NT>
+__device__ __forceinline__ void gather_rows(const uint4 *__restrict__ ksk, const uint32_t *rowid, int nrows,
+                                            uint4 *acc)
+{
+    constexpr int PER = (NP4 + NT - 1) / NT;
+    constexpr int U = 8;
     const int t = threadIdx.x;
     int r = 0;
     for (; r + U <= nrows; r += U) {
-        uint32_t v[U][PER];
+        uint4 v[U][PER];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const uint32_t *row = ksk + (size_t)rowid[r + u] * NOUT;
+            const uint4 *row = ksk + (size_t)rowid[r + u] * NP4;
 #pragma unroll
             for (int p = 0; p < PER; ++p) {
                 const int k = t + p * NT;
-                v[u][p] = (k < NOUT) ? __ldg(row + k) : 0u;
+                v[u][p] = (k < NP4) ? ldg_v4(row + k) : make_uint4(0u, 0u, 0u, 0u);
             }
         }
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
-            for (int p = 0; p < PER; ++p) acc[p] -= v[u][p];
+            for (int p = 0; p < PER; ++p) sub_v4(acc[p], v[u][p]);
     }
     for (; r < nrows; ++r) {
-        const uint32_t *row = ksk + (size_t)rowid[r] * NOUT;
+        const uint4 *row = ksk + (size_t)rowid[r] * NP4;
 #pragma unroll
         for (int p = 0; p < PER; ++p) {
             const int k = t + p * NT;
-            if (k < NOUT) acc[p] -= __ldg(row + k);
+            if (k < NP4) {
+                const uint4 x = ldg_v4(row + k);
+                acc[p].x -= x.x;
+                acc[p].y -= x.y;
+                acc[p].z -= x.z;
+                acc[p].w -= x.w;
+            }
         }
     }
 }
@@ -79,12 +107,13 @@ __global__ void __launch_bounds__(NT) iks_kernel(IksArgs a)
     constexpr int W = WIDE ? 64 : 32;
     constexpr uint64_t prec = 1ull << (W - (1 + BASEBIT * TT));
     constexpr uint32_t mask = (1u << BASEBIT) - 1;
-    constexpr int PER = (NOUT + NT - 1) / NT;
+    constexpr int NP4 = ksk_pitch(NOUT) / 4;
+    constexpr int PER = (NP4 + NT - 1) / NT;
     const int ct = blockIdx.x;
     const size_t base = (size_t)ct * (NIN + 1);
-    uint32_t acc[PER];
+    uint4 acc[PER];
 #pragma unroll
-    for (int p = 0; p < PER; ++p) acc[p] = 0;
+    for (int p = 0; p < PER; ++p) acc[p] = make_uint4(0u, 0u, 0u, 0u);
 
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int i0 = 0; i0 < NIN; i0 += NT) {
@@ -121,7 +150,7 @@ __global__ void __launch_bounds__(NT) iks_kernel(IksArgs a)
         for (int j = 0; j < TT; ++j)
             if (j < n) rowid[pos + j] = ids[j];
         __syncthreads();
-        gather_rows<NOUT, NT>(a.ksk, rowid, total, acc);
+        gather_rows<NP4, NT>(reinterpret_cast<const uint4 *>(a.ksk), rowid, total, acc);
         __syncthreads();
     }
 
@@ -131,9 +160,13 @@ __global__ void __launch_bounds__(NT) iks_kernel(IksArgs a)
     uint32_t *o = a.out + (size_t)ct * NOUT;
 #pragma unroll
     for (int p = 0; p < PER; ++p) {
-        const int k = threadIdx.x + p * NT;
-        if (k < NOUT - 1) o[k] = acc[p];
-        else if (k == NOUT - 1) o[k] = acc[p] + bnew;
+        const int k0 = 4 * (threadIdx.x + p * NT);
+        const uint32_t v[4] = {acc[p].x, acc[p].y, acc[p].z, acc[p].w};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            if (k0 + c < NOUT - 1) o[k0 + c] = v[c];
+            else if (k0 + c == NOUT - 1) o[k0 + c] = v[c] + bnew;
+        }
     }
 }
 
@@ -142,12 +175,14 @@ __global__ void __launch_bounds__(NT) iks_kernel(IksArgs a)
 cudaError_t launch_iks(const IksArgs &a, int kind, cudaStream_t st)
 {
     if (a.B <= 0) return cudaSuccess;
+    // one 16-byte word of a padded row per thread: 169 of 192 (lvl0 rows),
+    // 257 of 288 (lvl1 rows)
     if (kind == 10)
-        iks_kernel<256, false, N1, KS10_BASEBIT, KS10_T, N0 + 1><<<a.B, 256, 0, st>>>(a);
+        iks_kernel<192, false, N1, KS10_BASEBIT, KS10_T, N0 + 1><<<a.B, 192, 0, st>>>(a);
     else if (kind == 20)
-        iks_kernel<256, true, N2, KS20_BASEBIT, KS20_T, N0 + 1><<<a.B, 256, 0, st>>>(a);
+        iks_kernel<192, true, N2, KS20_BASEBIT, KS20_T, N0 + 1><<<a.B, 192, 0, st>>>(a);
     else if (kind == 21)
-        iks_kernel<352, true, N2, KS21_BASEBIT, KS21_T, N1 + 1><<<a.B, 352, 0, st>>>(a);
+        iks_kernel<288, true, N2, KS21_BASEBIT, KS21_T, N1 + 1><<<a.B, 288, 0, st>>>(a);
     else
         return cudaErrorInvalidValue;
     return cudaGetLastError();

@@ -14,7 +14,7 @@ struct IksArgs {
     uint32_t offset;     // added to b of the 32-bit input (gate / MSB offsets)
     uint64_t offset64;   // added to b of the 64-bit input before rescaling
     uint32_t *out;
-    const uint32_t *ksk;
+    const uint32_t *ksk;   // rows of ksk_pitch(out width) words, 16-byte aligned
     int B;
 };
 

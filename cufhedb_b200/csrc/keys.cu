@@ -73,7 +73,8 @@ __global__ void ksk_rows_kernel(uint32_t *out, uint64_t nrows, int n, int t, int
                                     : reinterpret_cast<const uint32_t *>(key_dom)[i];
     const uint32_t m = (uint32_t)(kd * (uint64_t)(k + 1) * (1ull << (32 - (j + 1) * basebit)));
     const uint64_t base = row * CB_TLWE32;
-    uint32_t *o = out + row * (uint64_t)(n + 1);
+    uint32_t *o = out + row * (uint64_t)ksk_pitch(n + 1);
+    for (int x = n + 1 + lane; x < ksk_pitch(n + 1); x += 32) o[x] = 0u;   // row padding
     uint32_t part = 0;
     for (int x = lane; x < n; x += 32) {
         const uint32_t av = (uint32_t)draw_k(skey, base + x);

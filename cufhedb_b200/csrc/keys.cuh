@@ -20,6 +20,7 @@ uint64_t stream_key(uint64_t seed, uint64_t stream);
 uint64_t host_draw(uint64_t seed, uint64_t stream, uint64_t ctr);
 void host_secret_keys(uint64_t seed, uint32_t *s0, uint32_t *s1, uint64_t *s2);
 
+// rows of ksk_pitch(width) words (common.cuh), pad words zero
 cudaError_t gen_ksk(uint32_t *out, int kind, uint64_t seed, const void *key_dom_d, const uint32_t *key_tgt_d,
                     cudaStream_t st);
 cudaError_t gen_bk01(uint32_t *out, uint64_t seed, const uint32_t *s0_d, const int *s1pos_d, int ns1,

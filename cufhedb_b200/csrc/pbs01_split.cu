@@ -120,74 +120,87 @@ __device__ __forceinline__ CP pmul_first(unsigned long long vr, unsigned long lo
     return CP{f2(nvi, ki, m2(vr, kr)), f2(vi, kr, m2(vr, ki))};
 }
 
-// Tensor-core stage 1 of one warp (tc_stage1.cuh): its tensor-memory
-// columns (A double-buffered, 16 columns each, then D, 32 columns), its
-// mbarrier and phase, and the shared-memory descriptors of B's limbs.
-// (addresses are recomputed from the block's shared memory and the warp
-// index at each use instead of held in registers: the kernel runs at the
-// 255-register limit)
-template <class L>
+// Tensor-core stage 1 (tc_stage1.cuh), shared by the warps of a group of
+// four (warps 0-3 and 4-7; a producer warp takes no part): each warp writes
+// its 32 A rows into its own sub-partition's lanes of the group's A columns,
+// the group meets at a named barrier, one lane of the group's first warp
+// issues the M = 128 MMAs for all four and commits them to the group's
+// mbarrier for that buffer, and every warp of the group waits on it.  Per
+// group: A double-buffered (16 columns each), D double-buffered (32 columns
+// each).  Every warp takes part in every step, active or not (a warp whose
+// rotation is 0 for this CMux writes no rows and reads no result), so the
+// barriers and the buffer reuse stay in step.  Addresses are recomputed from
+// the block's shared memory and the warp index at each use (the kernel runs
+// at the 255-register limit).
+constexpr uint32_t TC_GROUP_COLS = 96;
+
+template <class L, int W>
 struct TcStage {
     unsigned char *smem;
-    uint32_t phase;     // completed products of this warp
+    uint32_t phase;     // per buffer (bits 0, 1): parity of its next completion
 
-    __device__ __forceinline__ uint32_t tlane(int warp) const
+    __device__ __forceinline__ static int group(int warp) { return warp >> 2; }
+    __device__ __forceinline__ uint32_t tbase() const
     {
-        const uint32_t base = *reinterpret_cast<const volatile uint32_t *>(smem + L::TC_SLOT_OFF);
-        return base + 64u * warp + ((32u * (warp & 3)) << 16);
+        return *reinterpret_cast<const volatile uint32_t *>(smem + L::TC_SLOT_OFF);
     }
-    __device__ __forceinline__ uint64_t *bar(int warp) const
+    __device__ __forceinline__ uint64_t *bar(int warp, int buf) const
     {
-        return reinterpret_cast<uint64_t *>(smem + L::TC_BAR_OFF) + warp;
+        return reinterpret_cast<uint64_t *>(smem + L::TC_BAR_OFF) + 2 * group(warp) + buf;
     }
-    // A <- the digit-d row of every lane, into buffer buf (in flight until
-    // issue(), which waits for it)
-    __device__ __forceinline__ void put(const uint32_t w[32], int d, int buf, int warp)
+    // A(buf) <- the digit-d row of this lane (only when active)
+    __device__ __forceinline__ void put(const uint32_t *w, bool active, int d, int buf, int warp)
     {
-        uint32_t a[16];
-        tc_a_row(a, w, d);
-        tmem_st16(tlane(warp) + 16 * buf, a);
+        if (active) {
+            uint32_t a[16];
+            tc_a_row(a, w, d);
+            tmem_st16(tbase() + TC_GROUP_COLS * group(warp) + ((32u * (warp & 3)) << 16) + 16 * buf, a);
+            tmem_wait_st();
+        }
     }
-    // D = A(buf) (Bhi + Blo), issued by lane 0, completing on the warp's mbarrier
+    // the group meets, then its first warp issues D(buf) = A(buf) (Bhi + Blo)
     __device__ __forceinline__ void issue(int buf, int warp, int lane)
     {
-        tmem_wait_st();
         tc_fence_before();
-        __syncwarp();
-        if (lane == 0) {
+        if (group(warp) == 0) asm volatile("bar.sync 2, %0;" ::"n"(32 * (W < 4 ? W : 4)) : "memory");
+        else asm volatile("bar.sync 3, %0;" ::"n"(32 * (W > 4 ? W - 4 : 1)) : "memory");
+        if ((warp & 3) == 0 && lane == 0) {
             tc_fence_after();
-            const uint32_t tcol = tlane(warp) & 0xFFFFu;   // lane field 0: the MMA spans all 128 lanes
-            const uint32_t a = tcol + 16 * buf, d = tcol + 32;
+            const uint32_t gcol = tbase() + TC_GROUP_COLS * group(warp);
+            const uint32_t a = gcol + 16 * buf, dcol = gcol + 32 + 32 * buf;
             const uint32_t b = smem_u32(smem + L::TC_OFF), limb = TC_B_HALVES * 2, kstep = 2 * TC_B_LBO;
-            umma_ts(d, a, tc_smem_desc(b, TC_B_LBO, TC_B_SBO), 0);
-            umma_ts(d, a + 8, tc_smem_desc(b + kstep, TC_B_LBO, TC_B_SBO), 1);
-            umma_ts(d, a, tc_smem_desc(b + limb, TC_B_LBO, TC_B_SBO), 1);
-            umma_ts(d, a + 8, tc_smem_desc(b + limb + kstep, TC_B_LBO, TC_B_SBO), 1);
-            umma_commit(bar(warp));
+            umma_ts(dcol, a, tc_smem_desc(b, TC_B_LBO, TC_B_SBO), 0);
+            umma_ts(dcol, a + 8, tc_smem_desc(b + kstep, TC_B_LBO, TC_B_SBO), 1);
+            umma_ts(dcol, a, tc_smem_desc(b + limb, TC_B_LBO, TC_B_SBO), 1);
+            umma_ts(dcol, a + 8, tc_smem_desc(b + limb + kstep, TC_B_LBO, TC_B_SBO), 1);
+            umma_commit(bar(warp, buf));
         }
         __syncwarp();
     }
-    // waits for the warp's last product and reads its row: v[q] = X[q]
-    __device__ __forceinline__ void take(float2 v[16], int warp, int *err)
+    // waits for the group's product in buffer buf and (when active) reads
+    // this lane's row: v[q] = X[q]
+    __device__ __forceinline__ void take(float2 v[16], bool active, int buf, int warp, int *err)
     {
-        if (!mbar_wait(bar(warp), phase & 1)) report_error(err, DEV_TIMEOUT_MMA);
-        ++phase;
-        tc_fence_after();
-        uint32_t r[32];
-        tmem_ld32(tlane(warp) + 32, r);
+        if (!mbar_wait(bar(warp, buf), (phase >> buf) & 1)) report_error(err, DEV_TIMEOUT_MMA);
+        phase ^= 1u << buf;
+        if (active) {
+            tc_fence_after();
+            uint32_t r[32];
+            tmem_ld32(tbase() + TC_GROUP_COLS * group(warp) + ((32u * (warp & 3)) << 16) + 32 + 32 * buf, r);
 #pragma unroll
-        for (int q = 0; q < 16; ++q) v[q] = make_float2(__uint_as_float(r[q]), __uint_as_float(r[16 + q]));
+            for (int q = 0; q < 16; ++q) v[q] = make_float2(__uint_as_float(r[q]), __uint_as_float(r[16 + q]));
+        }
         tc_fence_before();
         __syncwarp();
     }
 };
 
-// tensor-memory columns of a block: 64 per consumer warp, rounded up to a
-// power of two (the allocation unit)
+// tensor-memory columns of a block: TC_GROUP_COLS per group of four consumer
+// warps, rounded up to a power of two (the allocation unit)
 template <int W>
 constexpr uint32_t tc_cols()
 {
-    return W * 64 <= 256 ? 256u : 512u;
+    return ((W + 3) / 4) * TC_GROUP_COLS <= 128 ? 128u : 256u;
 }
 
 // W consumer warps, plus a producer warp when PRODUCER (ring.cuh has both
@@ -215,7 +228,7 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
     if (threadIdx.x == 0) {
         ring.init_by_thread0();
         if constexpr (TC) {
-            for (int k = 0; k < W; ++k) mbar_init(&tc_bars[k], 1);
+            for (int k = 0; k < 4; ++k) mbar_init(&tc_bars[k], 1);   // 2 groups x 2 buffers
             fence_barrier_init();
         }
     }
@@ -246,7 +259,7 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
         if (threadIdx.x == 0) ring.prologue_by_thread0();
     }
 
-    TcStage<L> tc{smem, 0u};
+    TcStage<L, W> tc{smem, 0u};
 
     unsigned char *wb = smem + L::WARP_OFF + warp * L::PER_WARP;
     unsigned long long *xp = reinterpret_cast<unsigned long long *>(wb);
@@ -276,29 +289,26 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
             uint32_t w[32];
             if constexpr (TC) {
                 // the product of digit polynomial 0 is in flight before the loop
-                if (active) {
-                    digit_words1(w, acc, ab, lane);
-                    tc.put(w, 0, 0, warp);
-                    tc.issue(0, warp, lane);
-                }
+                if (active) digit_words1(w, acc, ab, lane);
+                tc.put(w, active, 0, 0, warp);
+                tc.issue(0, warp, lane);
             }
 #pragma unroll 1
             for (int r = 0; r < 2 * L1; ++r, ++c) {
                 float2 v[16];
                 if constexpr (TC) {
-                    // stage the next digit polynomial while this one's product
-                    // runs, take this one's, then start the next
-                    if (active) {
-                        if (r + 1 < 2 * L1) {
-                            // the words are recomputed for each digit polynomial
-                            // (not carried across the transform: register room)
-                            uint32_t wn[32];
-                            digit_words1(wn, acc + ((r + 1) / L1) * N1, ab, lane);
-                            tc.put(wn, (r + 1) % L1, (r + 1) & 1, warp);
-                        }
-                        tc.take(v, warp, a.err);
-                        if (r + 1 < 2 * L1) tc.issue((r + 1) & 1, warp, lane);
+                    // stage the next digit polynomial, take this one's product,
+                    // then start the next one's, which runs while this one is
+                    // transformed
+                    if (r + 1 < 2 * L1 && active) {
+                        // the words are recomputed for each digit polynomial
+                        // (not carried across the transform: register room)
+                        uint32_t wn[32];
+                        digit_words1(wn, acc + ((r + 1) / L1) * N1, ab, lane);
+                        tc.put(wn, true, (r + 1) % L1, (r + 1) & 1, warp);
                     }
+                    tc.take(v, active, r & 1, warp, a.err);
+                    if (r + 1 < 2 * L1) tc.issue((r + 1) & 1, warp, lane);
                 } else {
                     if (active && r % L1 == 0) digit_words1(w, acc + (r / L1) * N1, ab, lane);
                 }

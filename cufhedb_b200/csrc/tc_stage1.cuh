@@ -19,13 +19,14 @@
 // the products of the exact digits with the limbs are exact in FP32, so D
 // carries FP32 accumulation rounding only, as the CUDA-core stage does.
 //
-// Each warp has its own tensor-memory columns: A (16 columns: 32 FP16 per row,
-// two per 32-bit column) double-buffered, and D (32 FP32 columns).  A warp
-// writes its 32 rows into the 32 lanes of its sub-partition (tcgen05.st),
-// one of its lanes issues the M = 128 MMA (A from tensor memory, B from
-// shared memory) and commits it to the warp's mbarrier; the rows of the other
-// three sub-partitions in its columns are never read.  No warp waits for
-// another.
+// The consumer warps work in groups of four (one per sub-partition).  A group
+// has its own tensor-memory columns: A (16 columns: 32 FP16 per row, two per
+// 32-bit column) and D (32 FP32 columns), both double-buffered.  Each warp
+// writes its 32 rows into the 32 lanes of its sub-partition (tcgen05.st), the
+// group meets at a named barrier, one lane of its first warp issues the
+// M = 128 MMAs (A from tensor memory, B from shared memory) for all four
+// warps and commits them to the group's mbarrier, and each warp reads its own
+// 32 rows of D back (tcgen05.ld).
 #pragma once
 #include <cuda_fp16.h>
 

@@ -149,6 +149,37 @@ def test_iks_from_lvl2_bit_exact(engine2, oracle, keys, kind):
         assert np.array_equal(oracle.iks(kind, x, SEED, keys), o)
 
 
+def test_host_ksk21_loads_into_the_padded_device_layout(engine2, oracle, keys):
+    """A whole lvl21 key-switching key handed over as a host array in TFHEpp's
+    packed row layout (cufhedb_load_ksk) lands in the device layout (rows
+    padded to 16-byte multiples): the rows read back equal the host rows and
+    the key switch of the loaded key equals the one of the generated key."""
+    import torch
+    from cufhedb_b200 import Engine
+    _, _, s2 = keys
+    rows, width = 2048 * 10 * 7, N1 + 1
+    host = np.zeros(rows * width, np.uint32)
+    oracle.ksk_full_into(21, SEED, keys, host.ctypes.data)
+    eng = Engine(0)
+    eng.load_ksk(21, host)
+    q = np.array([0, 1, 2, 3, 70_001, rows - 1], np.uint64)
+    got = eng.export_ksk_rows(21, q)
+    host = host.reshape(rows, width)
+    for r, row in zip(q, got):
+        assert np.array_equal(host[int(r)], row)
+    del host
+    B = 5
+    xs = np.stack([oracle.tlwe64((i % 8) << 61, s2, NS_LVL2, SEED, 0x43, i) for i in range(B)])
+    o1 = torch.empty(B * width, dtype=torch.int32, device="cuda")
+    o2 = torch.empty_like(o1)
+    engine2.iks(21, _dev(xs), o1)
+    eng.iks(21, _dev(xs), o2)
+    engine2.sync()
+    eng.sync()
+    assert torch.equal(o1, o2)
+    eng.close()
+
+
 def test_pbs02_ragged_multi_pass_batch(engine2, oracle, keys):
     """Two full passes of three ciphertexts per SM plus a ragged remainder of
     two: every output decrypts to its input bit at +-mu."""
