@@ -127,8 +127,11 @@ CUFHEDB_API int cufhedb_load_bk_lvl01(cufhedb_ctx *ctx, const uint32_t *bk);
  * BootstrappingKeyFFT<lvl02param> (cufftlvl2.LoadBK), host memory */
 CUFHEDB_API int cufhedb_load_bk_lvl02(cufhedb_ctx *ctx, const uint64_t *bk);
 CUFHEDB_API int cufhedb_load_bkfft_lvl02(cufhedb_ctx *ctx, const double *bkfft);
-/* KeySwitchingKey<lvl10/20/21param>, host memory; kind is cufhedb_ksk_kind.
- * Replaces the host-resident key TFHEpp::IdentityKeySwitch reads (EvalKey::iksklvl*). */
+/* KeySwitchingKey<lvl10/20/21param>, host memory in TFHEpp's packed layout
+ * (rows of n+1 words); kind is cufhedb_ksk_kind.  On the device every row is
+ * padded to a multiple of 16 bytes (673 -> 676, 1025 -> 1028 words; the
+ * export and save functions below return the packed layout).  Replaces the
+ * host-resident key TFHEpp::IdentityKeySwitch reads (EvalKey::iksklvl*). */
 CUFHEDB_API int cufhedb_load_ksk(cufhedb_ctx *ctx, int kind, const uint32_t *ksk);
 /* Deterministic key set from `seed`, generated on the device (restates
  * TFHEpp bkgen / ikskgen, thirdparty/TFHEpp/src/cloudkey.cpp:7-69, with a
@@ -147,7 +150,8 @@ CUFHEDB_API int cufhedb_secret_keys(uint64_t seed, uint32_t *s0, uint32_t *s1, u
  * (test/HE3_Query/fastR.h:6-74): the lvl1 secret key (1024 x uint32), TFHEpp's
  * BootstrappingKeyFFT<lvl01param> (672 x 6 x 2 x 1024 doubles) and
  * KeySwitchingKey<lvl10param> (1024 x 2 x 1023 x 673 uint32), in that order,
- * 5.71 GB.  load: uploads both keys (the key-switching key in 64 MB pieces)
+ * 5.71 GB.  load: uploads both keys (the key-switching key in pieces of whole
+ * rows, about 64 MB each)
  * and copies the secret key to sk_out when it is not NULL; save: writes this
  * context's lvl01 and lvl10 keys, with `sk` (1024 words), or the
  * deterministic key set's lvl1 key when sk is NULL, or zeros. */
@@ -160,7 +164,7 @@ CUFHEDB_API int cufhedb_save_keyfile(cufhedb_ctx *ctx, const char *path, const u
  * host-only, locates and checks the key inside the archive (the last
  * sizeof(key) bytes, after the parameter block and the pointer's valid byte);
  * load: reads it into the context like cufhedb_load_bkfft_lvl01/02 /
- * cufhedb_load_ksk (key-switching keys streamed in 64 MB pieces). */
+ * cufhedb_load_ksk (key-switching keys streamed in pieces of whole rows). */
 enum cufhedb_cereal_kind {
     CUFHEDB_CEREAL_BKFFT01 = 1,
     CUFHEDB_CEREAL_BKFFT02 = 2,
