@@ -151,9 +151,9 @@ __device__ __forceinline__ C cx_w32(C a, int j)
 
 // ---- tables ---------------------------------------------------------------------
 // Each thread's twiddles are powers of one step, so the tables hold the
-// steps and the transforms form the powers by a recurrence (FP64: seven
-// steps add a few ulp, far inside the transform's error; the shared-memory
-// reads they replace were a fifth of the kernel's traffic):
+// steps and the transforms form the powers by repeated multiplication (FP64:
+// seven products add a few ulp, far inside the transform's error; the
+// shared-memory reads they replace were a fifth of the kernel's traffic):
 //   twA0[t] = w^t, twAs[t] = W_M^t     stage A twiddle w^t W_M^{t k} = twA0 twAs^k, k < 8
 //   twB1[a] = W_T^a                    stage B twiddle W_T^{a q1} = twB1^q1, q1 < 8
 // (stage C's twiddles W_16^r, r < 8, are compile-time constants)
@@ -183,34 +183,14 @@ inline void build_fft8x_tables(Fft8xTables<double2, T> &tab)
     for (int a = 0; a < L; ++a) tab.twB1[a] = cis(a, T);
 }
 
-// The powers of a unit step e^{i theta} follow the three-term recurrence
-//   p_{k+1} = 2 cos(theta) p_k - p_{k-1}
-// (two FMAs per power instead of a complex product), with p_0 = base and
-// p_1 = base * step; over seven steps its rounding stays within a few ulp.
-template <typename C>
-__device__ __forceinline__ C fft8x_next_power(C p, C pm, double c2)
-{
-    C r;
-    r.x = fma(c2, p.x, -pm.x);
-    r.y = fma(c2, p.y, -pm.y);
-    return r;
-}
-
 // v[0..7] *= base * step^k (S = +1) or conj(base * step^k) (S = -1)
 template <int S, typename C>
 __device__ __forceinline__ void fft8x_twiddle_powers(C v[8], C base, C step)
 {
-    const double c2 = step.x + step.x;
-    C pm = base, p = cx_mul(base, step);
-    v[0] = S > 0 ? cx_mul(v[0], base) : cx_mulc(v[0], base);
 #pragma unroll
-    for (int k = 1; k < 8; ++k) {
-        if (k > 1) {
-            const C pn = fft8x_next_power(p, pm, c2);
-            pm = p;
-            p = pn;
-        }
-        v[k] = S > 0 ? cx_mul(v[k], p) : cx_mulc(v[k], p);
+    for (int k = 0; k < 8; ++k) {
+        if (k > 0) base = cx_mul(base, step);
+        v[k] = S > 0 ? cx_mul(v[k], base) : cx_mulc(v[k], base);
     }
 }
 
@@ -218,17 +198,10 @@ __device__ __forceinline__ void fft8x_twiddle_powers(C v[8], C base, C step)
 template <int S, typename C>
 __device__ __forceinline__ void fft8x_step_powers(C v[8], C step)
 {
-    const double c2 = step.x + step.x;
-    C pm, p = step;
-    pm.x = 1.0;
-    pm.y = 0.0;
+    C p = step;
 #pragma unroll
     for (int k = 1; k < 8; ++k) {
-        if (k > 1) {
-            const C pn = fft8x_next_power(p, pm, c2);
-            pm = p;
-            p = pn;
-        }
+        if (k > 1) p = cx_mul(p, step);
         v[k] = S > 0 ? cx_mul(v[k], p) : cx_mulc(v[k], p);
     }
 }
