@@ -102,6 +102,7 @@ SIGNATURES = {
     "cufhedb_hom_msb": [_vp, _i32, _vp, _vp, _i32, _u32, _i32, _i32, _vp],
     "cufhedb_compare": [_vp, _i32, _i32, _vp, _vp, _vp, _i32, _u32, _i32, _i32, _vp],
     "cufhedb_queue_run": [_vp, _vp, _i32, _i32, _i32, _i32, _vp, _vp],
+    "cufhedb_queue_plan": [_vp, _i32, C.c_double, C.c_double, _i32, _i32, _vp, _vp, _vp],
     "cufhedb_cereal_key_payload": [C.c_char_p, _i32, _vp, _vp],
     "cufhedb_compare_host": [_vp, _i32, _i32, _vp, _vp, _vp, _i32, _u32, _i32, _i32],
     "cufhedb_gate_lvl1_host_multi": [_vp, _i32, _i32, _vp, _vp, _vp, _i32, _i32],

@@ -58,39 +58,12 @@ struct Batch {
     double cost = 0.0;
 };
 
-}  // namespace
-
-extern "C" CUFHEDB_API int cufhedb_queue_run(cufhedb_ctx *ctx, const cufhedb_query *q, int nq, int precision,
-                                             int max_batch_rows, int nstreams, float *latency_ms, float *total_ms)
+// Steps 1-3 of the scheduler (host only): the batches in run order and the
+// stream each is queued on.  t01 / t02: per-ciphertext pass time of lvl01 /
+// lvl02 bootstraps.
+void plan_queue(const cufhedb_query *q, int nq, double t01, double t02, int max_batch_rows, int nstreams,
+                std::vector<Batch> &batches, std::vector<int> &stream_of)
 {
-    using namespace cfdb;
-    if (!ctx) return set_error(CUFHEDB_ERR_ARG, "ctx is null");
-    if (nq < 0 || (nq > 0 && (!q || !latency_ms))) return set_error(CUFHEDB_ERR_ARG, "bad query list");
-    if (max_batch_rows < 1 || nstreams < 1 || nstreams > 16)
-        return set_error(CUFHEDB_ERR_ARG, "max_batch_rows >= 1 and 1 <= nstreams <= 16");
-    if (precision != CUFHEDB_FP64 && precision != CUFHEDB_SPLIT32 &&
-        precision != CUFHEDB_SPLIT32_TC)
-        return set_error(CUFHEDB_ERR_ARG, "unsupported precision");
-    for (int i = 0; i < nq; ++i) {
-        const cufhedb_query &x = q[i];
-        if ((x.level != 1 && x.level != 2) || x.op < 0 || x.op > 4 || x.rows < 0 || x.plain_bits < 1 ||
-            (x.rows > 0 && (!x.c1 || !x.c2 || !x.out)) || !aligned_to(x.c1, x.level == 1 ? 4 : 8) ||
-            !aligned_to(x.c2, x.level == 1 ? 4 : 8) || !aligned_to(x.out, 4))
-            return set_error(CUFHEDB_ERR_ARG, ("bad query " + std::to_string(i)).c_str());
-    }
-    if (total_ms) *total_ms = 0.0f;
-    if (nq == 0) return CUFHEDB_OK;
-    DeviceGuard guard;
-    if (guard.set(ctx->device) != cudaSuccess) return set_error(CUFHEDB_ERR_CUDA, "cudaSetDevice failed");
-
-    // per-ciphertext time of a full pass of the fastest shape, per level
-    auto per_ct = [&](const float *t, const int *shapes) {
-        double best = 1e30;
-        for (int i = 0; i < NSHAPES; ++i) best = std::min(best, (double)t[i] / (shapes[i] * ctx->num_sms));
-        return best;
-    };
-    const double t01 = per_ct(ctx->pbs01_pass_ms[precision], PBS01_SHAPES);
-    const double t02 = per_ct(ctx->pbs02_pass_ms, PBS02_SHAPES);
     std::vector<double> cost(nq);
     for (int i = 0; i < nq; ++i) {
         const ChainCost c = chain_cost(q[i]);
@@ -105,7 +78,7 @@ extern "C" CUFHEDB_API int cufhedb_queue_run(cufhedb_ctx *ctx, const cufhedb_que
         return q[a].level == q[b].level && q[a].op == q[b].op && q[a].plain_bits == q[b].plain_bits &&
                (q[a].logic != 0) == (q[b].logic != 0);
     };
-    std::vector<Batch> batches;
+    batches.clear();
     std::vector<int> open_of(nq, -1);   // open batch index per chain, keyed by its first query
     std::vector<int> chain_head;
     for (int i : order) {
@@ -130,6 +103,81 @@ extern "C" CUFHEDB_API int cufhedb_queue_run(cufhedb_ctx *ctx, const cufhedb_que
         return a.cost / a.members.size() < b.cost / b.members.size();
     });
 
+    // each batch on the stream with the least estimated work queued
+    std::vector<double> busy(nstreams, 0.0);
+    stream_of.assign(batches.size(), 0);
+    for (size_t bi = 0; bi < batches.size(); ++bi) {
+        const int s = (int)(std::min_element(busy.begin(), busy.end()) - busy.begin());
+        busy[s] += batches[bi].cost;
+        stream_of[bi] = s;
+    }
+}
+
+bool query_shape_ok(const cufhedb_query &x)
+{
+    return (x.level == 1 || x.level == 2) && x.op >= 0 && x.op <= 4 && x.rows >= 0 && x.plain_bits >= 1;
+}
+
+}  // namespace
+
+extern "C" CUFHEDB_API int cufhedb_queue_plan(const cufhedb_query *q, int nq, double t01_ms, double t02_ms,
+                                              int max_batch_rows, int nstreams, int *batch_of,
+                                              int *stream_of_batch, int *nbatches)
+{
+    using namespace cfdb;
+    if (nq < 0 || (nq > 0 && (!q || !batch_of || !stream_of_batch)) || !nbatches)
+        return set_error(CUFHEDB_ERR_ARG, "bad query list");
+    if (max_batch_rows < 1 || nstreams < 1 || nstreams > 16)
+        return set_error(CUFHEDB_ERR_ARG, "max_batch_rows >= 1 and 1 <= nstreams <= 16");
+    if (!(t01_ms > 0.0) || !(t02_ms > 0.0)) return set_error(CUFHEDB_ERR_ARG, "pass times must be positive");
+    for (int i = 0; i < nq; ++i)
+        if (!query_shape_ok(q[i])) return set_error(CUFHEDB_ERR_ARG, ("bad query " + std::to_string(i)).c_str());
+    std::vector<Batch> batches;
+    std::vector<int> stream_of;
+    plan_queue(q, nq, t01_ms, t02_ms, max_batch_rows, nstreams, batches, stream_of);
+    for (size_t b = 0; b < batches.size(); ++b) {
+        for (int m : batches[b].members) batch_of[m] = (int)b;
+        stream_of_batch[b] = stream_of[b];
+    }
+    *nbatches = (int)batches.size();
+    return CUFHEDB_OK;
+}
+
+extern "C" CUFHEDB_API int cufhedb_queue_run(cufhedb_ctx *ctx, const cufhedb_query *q, int nq, int precision,
+                                             int max_batch_rows, int nstreams, float *latency_ms, float *total_ms)
+{
+    using namespace cfdb;
+    if (!ctx) return set_error(CUFHEDB_ERR_ARG, "ctx is null");
+    if (nq < 0 || (nq > 0 && (!q || !latency_ms))) return set_error(CUFHEDB_ERR_ARG, "bad query list");
+    if (max_batch_rows < 1 || nstreams < 1 || nstreams > 16)
+        return set_error(CUFHEDB_ERR_ARG, "max_batch_rows >= 1 and 1 <= nstreams <= 16");
+    if (precision != CUFHEDB_FP64 && precision != CUFHEDB_SPLIT32 &&
+        precision != CUFHEDB_SPLIT32_TC)
+        return set_error(CUFHEDB_ERR_ARG, "unsupported precision");
+    for (int i = 0; i < nq; ++i) {
+        const cufhedb_query &x = q[i];
+        if (!query_shape_ok(x) || (x.rows > 0 && (!x.c1 || !x.c2 || !x.out)) ||
+            !aligned_to(x.c1, x.level == 1 ? 4 : 8) || !aligned_to(x.c2, x.level == 1 ? 4 : 8) ||
+            !aligned_to(x.out, 4))
+            return set_error(CUFHEDB_ERR_ARG, ("bad query " + std::to_string(i)).c_str());
+    }
+    if (total_ms) *total_ms = 0.0f;
+    if (nq == 0) return CUFHEDB_OK;
+    DeviceGuard guard;
+    if (guard.set(ctx->device) != cudaSuccess) return set_error(CUFHEDB_ERR_CUDA, "cudaSetDevice failed");
+
+    // per-ciphertext time of a full pass of the fastest shape, per level
+    auto per_ct = [&](const float *t, const int *shapes) {
+        double best = 1e30;
+        for (int i = 0; i < NSHAPES; ++i) best = std::min(best, (double)t[i] / (shapes[i] * ctx->num_sms));
+        return best;
+    };
+    const double t01 = per_ct(ctx->pbs01_pass_ms[precision], PBS01_SHAPES);
+    const double t02 = per_ct(ctx->pbs02_pass_ms, PBS02_SHAPES);
+    std::vector<Batch> batches;
+    std::vector<int> stream_of;
+    plan_queue(q, nq, t01, t02, max_batch_rows, nstreams, batches, stream_of);
+
     std::vector<cudaStream_t> streams(nstreams, nullptr);
     std::vector<cudaEvent_t> done(batches.size(), nullptr);
     cudaEvent_t start = nullptr;
@@ -141,12 +189,9 @@ extern "C" CUFHEDB_API int cufhedb_queue_run(cufhedb_ctx *ctx, const cufhedb_que
     for (int s = 1; s < nstreams && e == cudaSuccess; ++s) e = cudaStreamWaitEvent(streams[s], start, 0);
     if (e != cudaSuccess) rc = cuda_error(e, "queue set-up");
 
-    std::vector<double> busy(nstreams, 0.0);   // estimated work queued per stream
     for (size_t bi = 0; bi < batches.size() && rc == CUFHEDB_OK; ++bi) {
         const Batch &B = batches[bi];
-        const int s = (int)(std::min_element(busy.begin(), busy.end()) - busy.begin());
-        busy[s] += B.cost;
-        cudaStream_t st = streams[s];
+        cudaStream_t st = streams[stream_of[bi]];
         const cufhedb_query &h = q[B.members[0]];
         const size_t in_w = (size_t)(h.level == 1 ? N1 + 1 : N2 + 1) * (h.level == 1 ? 4 : 8);   // bytes per row
         const size_t out_w = (size_t)(N1 + 1) * 4;

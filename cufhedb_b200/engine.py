@@ -432,6 +432,24 @@ def _ctx_array(engines):
     return arr
 
 
+def queue_plan(queries, t01_ms: float, t02_ms: float, max_batch_rows: int = 16384, nstreams: int = 2):
+    """The native queue scheduler's plan (host only, no device): queries is a
+    list of (op, level, rows, plain_bits, logic); returns (batch of each
+    query, stream of each batch), batches numbered in run order."""
+    lib = _lib.load()
+    n = len(queries)
+    arr = (_lib.Query * max(n, 1))()
+    for i, (op, level, rows, pb, logic) in enumerate(queries):
+        arr[i] = _lib.Query(level, _lib.COMPARE[op] if isinstance(op, str) else op, pb, int(logic), rows,
+                            None, None, None)
+    batch_of = (C.c_int * max(n, 1))()
+    stream_of = (C.c_int * max(n, 1))()
+    nb = C.c_int(0)
+    check(lib.cufhedb_queue_plan(arr, n, float(t01_ms), float(t02_ms), max_batch_rows, nstreams, batch_of,
+                                 stream_of, C.byref(nb)))
+    return [int(x) for x in batch_of[:n]], [int(x) for x in stream_of[:nb.value]]
+
+
 def compare_host(engine: Engine, op: str, level: int, c1: np.ndarray, c2: np.ndarray, plain_bits: int,
                  logic: bool = True, precision: int = _lib.FP64) -> np.ndarray:
     """cufhedb_compare on host arrays (B x (N+1) words of `level`); returns B lvl1 TLWEs"""

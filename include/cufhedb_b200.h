@@ -304,6 +304,15 @@ typedef struct {
  * NULL) the whole queue's; returns when every result is in place. */
 CUFHEDB_API int cufhedb_queue_run(cufhedb_ctx *ctx, const cufhedb_query *q, int nq, int precision,
                                   int max_batch_rows, int nstreams, float *latency_ms, float *total_ms);
+/* The plan cufhedb_queue_run follows, host only (no device, no context):
+ * t01_ms / t02_ms are the per-ciphertext times of lvl01 / lvl02 bootstraps
+ * (queue_run takes them from the context's launch-shape table).  Batches are
+ * numbered in run order; batch_of[i] (nq entries) receives query i's batch,
+ * stream_of_batch[b] (up to nq entries) the stream batch b is queued on, and
+ * *nbatches their count.  The query pointers are not read. */
+CUFHEDB_API int cufhedb_queue_plan(const cufhedb_query *q, int nq, double t01_ms, double t02_ms,
+                                   int max_batch_rows, int nstreams, int *batch_of, int *stream_of_batch,
+                                   int *nbatches);
 
 /* B negacyclic products out_i = a_i * m (the reference's PolyMul_st,
  * src/cuHEDB/fft_gpu/cufft_gpu.cuh:214-226, which multiplies by the
