@@ -301,10 +301,11 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
                     // then start the next one's, which runs while this one is
                     // transformed
                     if (r + 1 < 2 * L1 && active) {
-                        // the words of the second polynomial replace the
-                        // first's when its first digit is staged
-                        if ((r + 1) % L1 == 0) digit_words1(w, acc + N1, ab, lane);
-                        tc.put(w, true, (r + 1) % L1, (r + 1) & 1, warp);
+                        // the words are recomputed for each digit polynomial
+                        // (not carried across the transform: register room)
+                        uint32_t wn[32];
+                        digit_words1(wn, acc + ((r + 1) / L1) * N1, ab, lane);
+                        tc.put(wn, true, (r + 1) % L1, (r + 1) & 1, warp);
                     }
                     tc.take(v, active, r & 1, warp, a.err);
                     if (r + 1 < 2 * L1) tc.issue((r + 1) & 1, warp, lane);
