@@ -166,7 +166,8 @@ inline int &precision_setting()
 {
     static int p = [] {
         const char *e = std::getenv("CUFHEDB_PRECISION");
-        return (e && std::string(e) == "fp64") ? (int)CUFHEDB_FP64 : (int)CUFHEDB_SPLIT32;
+        const std::string v = e ? e : "";
+        return v == "fp64" ? (int)CUFHEDB_FP64 : v == "split32tc" ? (int)CUFHEDB_SPLIT32_TC : (int)CUFHEDB_SPLIT32;
     }();
     return p;
 }
