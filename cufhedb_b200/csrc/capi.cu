@@ -357,6 +357,18 @@ int cufhedb_ctx_create(cufhedb_ctx **out, int device)
     if (e == cudaSuccess) e = init_pbs01_split();
     if (e == cudaSuccess) e = init_pbs02_f64();
     if (e == cudaSuccess) e = noalloc_scratch_address(&ctx->noalloc_scratch);
+    if (e == cudaSuccess) {
+        // The entry points take their scratch from the device's stream-ordered
+        // pool (cudaMallocAsync).  With the pool's default release threshold
+        // of 0 every synchronisation hands its memory back to the driver, so
+        // a synchronous call (the host-buffer entry points, the drop-in
+        // header's batches) would map its scratch afresh each time; the pool
+        // keeps what it has instead.
+        cudaMemPool_t pool = nullptr;
+        uint64_t keep = UINT64_MAX;
+        e = cudaDeviceGetDefaultMemPool(&pool, device);
+        if (e == cudaSuccess) e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     if (e != cudaSuccess) {
         cufhedb_ctx_destroy(ctx);
         return cuda_fail(e, "context set-up");

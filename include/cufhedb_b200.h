@@ -111,7 +111,11 @@ enum cufhedb_gate {
 CUFHEDB_API int cufhedb_abi_version(void);
 CUFHEDB_API const char *cufhedb_last_error(void);
 /* replaces the CuFFT_Torus constructor (src/cuHEDB/fft_gpu/cufft_gpu.cuh:135-163):
- * binds a device, builds the twiddle tables; keys are loaded separately */
+ * binds a device, builds the twiddle tables; keys are loaded separately.
+ * Entry points take transient scratch from the device's default stream-ordered
+ * memory pool; this call sets that pool's release threshold to its maximum,
+ * so memory freed into it stays mapped across synchronisations (a process-
+ * wide attribute of the default pool; nothing outlasts the process). */
 CUFHEDB_API int cufhedb_ctx_create(cufhedb_ctx **out, int device);
 CUFHEDB_API int cufhedb_ctx_destroy(cufhedb_ctx *ctx);
 CUFHEDB_API int cufhedb_ctx_num_sms(const cufhedb_ctx *ctx);
