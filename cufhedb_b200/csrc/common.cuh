@@ -127,6 +127,13 @@ __device__ __forceinline__ void bulk_g2s(void *smem_dst, const void *gsrc, uint3
 
 // signed Bg-bit field d (0 = most significant) of x: two plain shifts, the
 // field moved to the top and sign-extended back down
+// asks L2 to fetch [gsrc, gsrc + bytes) ahead of its use (no data returned;
+// gsrc 16-byte aligned, bytes a multiple of 16)
+__device__ __forceinline__ void bulk_prefetch_l2(const void *gsrc, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(gsrc), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ int digit_field1(uint32_t x, int d)
 {
     return (int)(x << (BGBIT1 * d)) >> (32 - BGBIT1);

@@ -7,13 +7,29 @@
 // transformed back per output polynomial.  One warp per product; the TRGSW
 // rows (one per TRGSW or one shared by the batch) are read straight from HBM
 // in the per-lane chunk layout the PBS kernels use, so every load is a
-// coalesced 16-byte access and each TRGSW byte is read once.
+// coalesced 16-byte access and each TRGSW byte is read once.  A warp's loads
+// of TRGSW row r come after the transform of digit polynomial r, so lane 0
+// asks L2 for the rows two ahead (a bulk prefetch) and the loads find them
+// there instead of waiting on HBM.
+
 #include "extprod.cuh"
 #include "fft_f32.cuh"
 
 namespace cfdb {
 
 namespace {
+
+// 16 KB per TRGSW row (1,024 complex FP64, or 1,024 (hi, lo) FP32 pairs)
+constexpr uint32_t TRGSW_ROW_BYTES = 16384;
+
+// rows r and r + 1 of this warp's own TRGSW into L2 (nothing to do when the
+// batch shares one TRGSW: it stays in L2 anyway)
+__device__ __forceinline__ void prefetch_rows(const void *g, int r, int n, const ExtProdArgs &a, int lane)
+{
+    if (a.shared || lane != 0) return;
+    for (int k = r; k < r + n && k < 2 * L1; ++k)
+        bulk_prefetch_l2(reinterpret_cast<const unsigned char *>(g) + (size_t)k * TRGSW_ROW_BYTES, TRGSW_ROW_BYTES);
+}
 
 __device__ __forceinline__ void digits_f64(double2 v[16], const uint32_t *poly, int d, int lane, const Fft512Tables &T)
 {
@@ -50,9 +66,11 @@ __global__ void __launch_bounds__(128) extprod1_f64_kernel(ExtProdArgs a)
     const uint32_t *in = a.trlwe + (size_t)p * 2 * N1;
     const double2 *g = reinterpret_cast<const double2 *>(a.trgsw) + (a.shared ? 0 : (size_t)p * 6 * 1024);
     double2 f0[16], f1[16];
+    prefetch_rows(g, 0, 2, a, lane);
 #pragma unroll 1
     for (int r = 0; r < 2 * L1; ++r) {
         double2 v[16];
+        prefetch_rows(g, r + 2, 1, a, lane);
         digits_f64(v, in + (r / L1) * N1, r % L1, lane, T);
         fft512_fwd(v, xp_s[w], T, lane);
         const double2 *gc = g + (size_t)r * 1024;
@@ -129,9 +147,11 @@ __global__ void __launch_bounds__(128) extprod1_split_kernel(ExtProdArgs a)
     const uint32_t *in = a.trlwe + (size_t)p * 2 * N1;
     const float4 *g = reinterpret_cast<const float4 *>(a.trgsw) + (a.shared ? 0 : (size_t)p * 6 * 1024);
     CP f0[16], f1[16];
+    prefetch_rows(g, 0, 2, a, lane);
 #pragma unroll 1
     for (int r = 0; r < 2 * L1; ++r) {
         float2 v[16];
+        prefetch_rows(g, r + 2, 1, a, lane);
         digits_f32(v, in + (r / L1) * N1, r % L1, lane, T);
         ffft512_fwd(v, reinterpret_cast<float2 *>(xp_s[w]), T, lane);
         const float4 *gc = g + (size_t)r * 1024;

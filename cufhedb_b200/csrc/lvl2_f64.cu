@@ -282,11 +282,21 @@ __global__ void __launch_bounds__(T2) extprod2_kernel(ExtProd2Args a)
     const Fft1024Tables &T = *a.tables;
     const uint64_t *in = a.trlwe + p * 2 * N2;
     const double2 *g = a.trgsw + (a.shared ? 0 : p * 2 * L2 * 2 * 1024);
+    // the TRGSW rows two ahead of the one in use are fetched into L2 (32 KB
+    // per row: both outputs), so the loads after each transform find them there
+    constexpr uint32_t ROW_BYTES = 2 * 1024 * sizeof(double2);
+    auto prefetch = [&](int r0, int n) {
+        if (a.shared || t != 0) return;
+        for (int k = r0; k < r0 + n && k < 2 * L2; ++k)
+            bulk_prefetch_l2(reinterpret_cast<const unsigned char *>(g) + (size_t)k * ROW_BYTES, ROW_BYTES);
+    };
+    prefetch(0, 2);
     double2 f0[8], f1[8];
 #pragma unroll 1
     for (int r = 0; r < 2 * L2; ++r) {
         double2 v[8];
         uint64_t xw[16];
+        prefetch(r + 2, 1);
         digit_words2<false>(xw, in + (r / L2) * N2, 0, t);
         digits2(v, xw, r % L2);
         fft8x_fwd<double2, T2>(v, xp_s, T, t, 1);
