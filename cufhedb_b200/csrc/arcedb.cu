@@ -148,6 +148,7 @@ struct Arc {
         a.B = B;
         a.shared = 0;
         a.tables = prec == CUFHEDB_FP64 ? (const void *)c->tab512 : (const void *)c->tab512f;
+        a.err = c->err;
         cudaError_t e = launch_extprod1(a, prec == CUFHEDB_FP64 ? 0 : 1, st);
         return e == cudaSuccess ? CUFHEDB_OK : cuda_error(e, "ArcEDB external product");
     }

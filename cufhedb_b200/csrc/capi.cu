@@ -356,6 +356,7 @@ int cufhedb_ctx_create(cufhedb_ctx **out, int device)
     if (e == cudaSuccess) e = init_pbs01_f64();
     if (e == cudaSuccess) e = init_pbs01_split();
     if (e == cudaSuccess) e = init_pbs02_f64();
+    if (e == cudaSuccess) e = init_extprod1();
     if (e == cudaSuccess) e = noalloc_scratch_address(&ctx->noalloc_scratch);
     if (e == cudaSuccess) {
         // The entry points take their scratch from the device's stream-ordered
@@ -1187,6 +1188,7 @@ int cufhedb_extprod_lvl1(cufhedb_ctx *ctx, const uint32_t *trlwe, const void *tr
     a.B = B;
     a.shared = shared ? 1 : 0;
     a.tables = precision == CUFHEDB_FP64 ? (const void *)ctx->tab512 : (const void *)ctx->tab512f;
+    a.err = ctx->err;
     CK(launch_extprod1(a, precision == CUFHEDB_FP64 ? 0 : 1, (cudaStream_t)stream));
     return CUFHEDB_OK;
 }
@@ -1355,6 +1357,7 @@ int cufhedb_extprod_lvl1_host(cufhedb_ctx *ctx, const uint32_t *trlwe, const dou
         a.B = B;
         a.shared = shared ? 1 : 0;
         a.tables = ctx->tab512;
+        a.err = ctx->err;
         e = launch_extprod1(a, 0, st);
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, tb, cudaMemcpyDeviceToHost, st);

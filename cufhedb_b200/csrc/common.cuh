@@ -41,6 +41,7 @@ enum : int {
     DEV_TIMEOUT_EMPTY = 2,   // producer gave up waiting for a free ring slot
     DEV_TIMEOUT_DRAIN = 3,   // producer gave up waiting for its last copies
     DEV_TIMEOUT_MMA = 4,     // a warp gave up waiting for its tensor-core product
+    DEV_TIMEOUT_ROW = 5,     // a warp gave up waiting for a TRGSW row it copies in
 };
 
 // bounded waits: polls of mbarrier.try_wait (each poll may suspend in hardware
@@ -125,8 +126,6 @@ __device__ __forceinline__ void bulk_g2s(void *smem_dst, const void *gsrc, uint3
         : "memory");
 }
 
-// signed Bg-bit field d (0 = most significant) of x: two plain shifts, the
-// field moved to the top and sign-extended back down
 // asks L2 to fetch [gsrc, gsrc + bytes) ahead of its use (no data returned;
 // gsrc 16-byte aligned, bytes a multiple of 16)
 __device__ __forceinline__ void bulk_prefetch_l2(const void *gsrc, uint32_t bytes)
@@ -134,6 +133,8 @@ __device__ __forceinline__ void bulk_prefetch_l2(const void *gsrc, uint32_t byte
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(gsrc), "r"(bytes) : "memory");
 }
 
+// signed Bg-bit field d (0 = most significant) of x: two plain shifts, the
+// field moved to the top and sign-extended back down
 __device__ __forceinline__ int digit_field1(uint32_t x, int d)
 {
     return (int)(x << (BGBIT1 * d)) >> (32 - BGBIT1);

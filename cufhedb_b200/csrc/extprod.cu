@@ -5,12 +5,17 @@
 // Restates trgswfftExternalProduct<lvl1param> (thirdparty/TFHEpp/src/
 // trgsw.cpp:77-103): res_o = sum_{k,d} IFFT(dec_d(trlwe_k)) * trgsw[k l + d][o],
 // transformed back per output polynomial.  One warp per product; the TRGSW
-// rows (one per TRGSW or one shared by the batch) are read straight from HBM
-// in the per-lane chunk layout the PBS kernels use, so every load is a
-// coalesced 16-byte access and each TRGSW byte is read once.  A warp's loads
-// of TRGSW row r come after the transform of digit polynomial r, so lane 0
-// asks L2 for the rows two ahead (a bulk prefetch) and the loads find them
-// there instead of waiting on HBM.
+// rows (one per TRGSW or one shared by the batch) are stored in the per-lane
+// chunk layout the PBS kernels use, and each TRGSW byte is read once.  The
+// FP64 kernel reads them straight from global memory.  In the split kernel
+// every warp copies its product's TRGSW row by row into its own 16 KB of
+// shared memory (a bulk copy completing on the warp's mbarrier), the copy of
+// row r + 1 issued as soon as the products of row r are read out, so it runs
+// under the transform of digit polynomial r + 1; lane 0 also asks L2 for the
+// rows two ahead (a bulk prefetch), so each copy finds its row there.  Waits
+// are bounded: a warp that gives up records DEV_TIMEOUT_ROW, issues no
+// further copy and, before it exits, waits (bounded again) for the one it
+// gave up on.
 
 #include "extprod.cuh"
 #include "fft_f32.cuh"
@@ -21,6 +26,59 @@ namespace {
 
 // 16 KB per TRGSW row (1,024 complex FP64, or 1,024 (hi, lo) FP32 pairs)
 constexpr uint32_t TRGSW_ROW_BYTES = 16384;
+constexpr int EP_WARPS = 4;   // products (warps) per CTA
+
+// dynamic shared memory of a CTA: per warp a staged TRGSW row and its
+// transpose scratch (XPB bytes), then one mbarrier per warp
+template <int XPB>
+constexpr int ep_smem_bytes()
+{
+    return EP_WARPS * (int)TRGSW_ROW_BYTES + EP_WARPS * XPB + EP_WARPS * 8;
+}
+
+// one warp's TRGSW row staged in shared memory (see the file comment)
+struct RowStage {
+    unsigned char *buf;   // TRGSW_ROW_BYTES, 128-byte aligned
+    uint64_t *bar;
+    uint32_t phase;
+    bool ok;              // warp-uniform: no wait has given up
+
+    __device__ __forceinline__ void init(int lane)
+    {
+        if (lane == 0) {
+            mbar_init(bar, 1);
+            fence_barrier_init();
+        }
+        __syncwarp();
+    }
+    // after every lane's last read of the buffer (callers __syncwarp first)
+    __device__ __forceinline__ void issue(const unsigned char *row, int lane)
+    {
+        if (lane == 0 && ok) {
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(bar, TRGSW_ROW_BYTES);
+            bulk_g2s(buf, row, TRGSW_ROW_BYTES, bar);
+        }
+    }
+    __device__ __forceinline__ void wait(int *err, int lane)
+    {
+        if (!ok) return;
+        const bool done = __all_sync(0xffffffffu, mbar_wait(bar, phase));
+        if (done) {
+            phase ^= 1;
+        } else {
+            ok = false;
+            if (lane == 0) report_error(err, DEV_TIMEOUT_ROW);
+        }
+    }
+    // a copy given up on may still be in flight: wait for it (bounded)
+    __device__ __forceinline__ void drain(int *err, int lane)
+    {
+        if (ok) return;
+        const bool done = __all_sync(0xffffffffu, mbar_wait(bar, phase));
+        if (!done && lane == 0) report_error(err, DEV_TIMEOUT_DRAIN);
+    }
+};
 
 // rows r and r + 1 of this warp's own TRGSW into L2 (nothing to do when the
 // batch shares one TRGSW: it stays in L2 anyway)
@@ -56,23 +114,25 @@ __device__ __forceinline__ void digits_f32(float2 v[16], const uint32_t *poly, i
     }
 }
 
-__global__ void __launch_bounds__(128) extprod1_f64_kernel(ExtProdArgs a)
+// The FP64 kernel reads its TRGSW rows straight from global memory: staged
+// through shared memory like the split kernel it measured slower (4,096
+// products 0.145 -> 0.190 ms).
+__global__ void __launch_bounds__(EP_WARPS * 32) extprod1_f64_kernel(ExtProdArgs a)
 {
-    __shared__ double2 xp_s[4][FFT512_XP];
+    __shared__ double2 xp_s[EP_WARPS][FFT512_XP];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int p = blockIdx.x * 4 + w;
+    const int p = blockIdx.x * EP_WARPS + w;
     if (p >= a.B) return;
+    double2 *xp = xp_s[w];
     const Fft512Tables &T = *reinterpret_cast<const Fft512Tables *>(a.tables);
     const uint32_t *in = a.trlwe + (size_t)p * 2 * N1;
     const double2 *g = reinterpret_cast<const double2 *>(a.trgsw) + (a.shared ? 0 : (size_t)p * 6 * 1024);
     double2 f0[16], f1[16];
-    prefetch_rows(g, 0, 2, a, lane);
 #pragma unroll 1
     for (int r = 0; r < 2 * L1; ++r) {
         double2 v[16];
-        prefetch_rows(g, r + 2, 1, a, lane);
         digits_f64(v, in + (r / L1) * N1, r % L1, lane, T);
-        fft512_fwd(v, xp_s[w], T, lane);
+        fft512_fwd(v, xp, T, lane);
         const double2 *gc = g + (size_t)r * 1024;
         if (r == 0) {
 #pragma unroll
@@ -89,7 +149,7 @@ __global__ void __launch_bounds__(128) extprod1_f64_kernel(ExtProdArgs a)
         }
     }
     uint32_t *o = a.out + (size_t)p * 2 * N1;
-    fft512_inv(f0, xp_s[w], T, lane);
+    fft512_inv(f0, xp, T, lane);
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int m = lane + 32 * m2;
@@ -97,7 +157,7 @@ __global__ void __launch_bounds__(128) extprod1_f64_kernel(ExtProdArgs a)
         o[m] = f64_to_torus32(y.x * (1.0 / 512.0));
         o[m + 512] = f64_to_torus32(y.y * (1.0 / 512.0));
     }
-    fft512_inv(f1, xp_s[w], T, lane);
+    fft512_inv(f1, xp, T, lane);
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int m = lane + 32 * m2;
@@ -137,33 +197,46 @@ __device__ __forceinline__ void pmac_limbs(CP &f, float2 v, float4 k, bool first
     }
 }
 
-__global__ void __launch_bounds__(128) extprod1_split_kernel(ExtProdArgs a)
+constexpr int XPB_SPLIT = FFT512_XP * (int)sizeof(unsigned long long);
+
+__global__ void __launch_bounds__(EP_WARPS * 32) extprod1_split_kernel(ExtProdArgs a)
 {
-    __shared__ unsigned long long xp_s[4][FFT512_XP];
+    extern __shared__ __align__(128) unsigned char smem[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int p = blockIdx.x * 4 + w;
+    const int p = blockIdx.x * EP_WARPS + w;
     if (p >= a.B) return;
+    unsigned long long *xp =
+        reinterpret_cast<unsigned long long *>(smem + EP_WARPS * TRGSW_ROW_BYTES + w * XPB_SPLIT);
+    RowStage rs{smem + w * TRGSW_ROW_BYTES,
+                reinterpret_cast<uint64_t *>(smem + EP_WARPS * (TRGSW_ROW_BYTES + XPB_SPLIT)) + w, 0u, true};
+    rs.init(lane);
     const Fft512TablesPlain &T = reinterpret_cast<const Fft512TablesF *>(a.tables)->plain;
     const uint32_t *in = a.trlwe + (size_t)p * 2 * N1;
-    const float4 *g = reinterpret_cast<const float4 *>(a.trgsw) + (a.shared ? 0 : (size_t)p * 6 * 1024);
+    const unsigned char *g = reinterpret_cast<const unsigned char *>(a.trgsw) +
+                             (a.shared ? 0 : (size_t)p * 2 * L1 * TRGSW_ROW_BYTES);
+    prefetch_rows(g, 1, 2, a, lane);
+    rs.issue(g, lane);
     CP f0[16], f1[16];
-    prefetch_rows(g, 0, 2, a, lane);
 #pragma unroll 1
     for (int r = 0; r < 2 * L1; ++r) {
         float2 v[16];
-        prefetch_rows(g, r + 2, 1, a, lane);
+        prefetch_rows(g, r + 3, 1, a, lane);
         digits_f32(v, in + (r / L1) * N1, r % L1, lane, T);
-        ffft512_fwd(v, reinterpret_cast<float2 *>(xp_s[w]), T, lane);
-        const float4 *gc = g + (size_t)r * 1024;
+        ffft512_fwd(v, reinterpret_cast<float2 *>(xp), T, lane);
+        rs.wait(a.err, lane);
+        const float4 *gc = reinterpret_cast<const float4 *>(rs.buf);
 #pragma unroll
         for (int s = 0; s < 16; ++s) {
             pmac_limbs(f0[s], v[s], gc[(2 * s) * 32 + lane], r == 0);
             pmac_limbs(f1[s], v[s], gc[(2 * s + 1) * 32 + lane], r == 0);
         }
+        __syncwarp();
+        if (r + 1 < 2 * L1) rs.issue(g + (size_t)(r + 1) * TRGSW_ROW_BYTES, lane);
     }
+    rs.drain(a.err, lane);
     uint32_t *o = a.out + (size_t)p * 2 * N1;
-    store_split(o, f0, xp_s[w], lane, T);
-    store_split(o + N1, f1, xp_s[w], lane, T);
+    store_split(o, f0, xp, lane, T);
+    store_split(o + N1, f1, xp, lane, T);
 }
 
 }  // namespace
@@ -171,9 +244,18 @@ __global__ void __launch_bounds__(128) extprod1_split_kernel(ExtProdArgs a)
 cudaError_t launch_extprod1(const ExtProdArgs &a, int precision, cudaStream_t st)
 {
     if (a.B <= 0) return cudaSuccess;
-    if (precision == 0) extprod1_f64_kernel<<<(a.B + 3) / 4, 128, 0, st>>>(a);
-    else extprod1_split_kernel<<<(a.B + 3) / 4, 128, 0, st>>>(a);
+    const unsigned grid = (unsigned)((a.B + EP_WARPS - 1) / EP_WARPS);
+    if (precision == 0)
+        extprod1_f64_kernel<<<grid, EP_WARPS * 32, 0, st>>>(a);
+    else
+        extprod1_split_kernel<<<grid, EP_WARPS * 32, ep_smem_bytes<XPB_SPLIT>(), st>>>(a);
     return cudaGetLastError();
+}
+
+cudaError_t init_extprod1()
+{
+    return cudaFuncSetAttribute(extprod1_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                ep_smem_bytes<XPB_SPLIT>());
 }
 
 }  // namespace cfdb

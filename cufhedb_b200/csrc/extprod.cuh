@@ -11,9 +11,12 @@ struct ExtProdArgs {
     int B;
     int shared;              // 1: one TRGSW for the whole batch
     const void *tables;      // Fft512Tables (FP64 path) or Fft512TablesF (split path)
+    int *err;                // device error word (bounded waits that gave up)
 };
 
 // precision 0: FP64, 1: split-precision FP32
 cudaError_t launch_extprod1(const ExtProdArgs &a, int precision, cudaStream_t st);
+// once per process and device, before the first launch (dynamic shared memory)
+cudaError_t init_extprod1();
 
 }  // namespace cfdb
