@@ -132,6 +132,12 @@ __device__ __forceinline__ void bulk_prefetch_l2(const void *gsrc, uint32_t byte
 {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(gsrc), "r"(bytes) : "memory");
 }
+// the same for a buffer whose alignment the caller does not control (a hint:
+// nothing is done unless gsrc is 16-byte aligned)
+__device__ __forceinline__ void bulk_prefetch_l2_if_aligned(const void *gsrc, uint32_t bytes)
+{
+    if ((reinterpret_cast<uintptr_t>(gsrc) & 15u) == 0 && (bytes & 15u) == 0) bulk_prefetch_l2(gsrc, bytes);
+}
 
 // signed Bg-bit field d (0 = most significant) of x: two plain shifts, the
 // field moved to the top and sign-extended back down

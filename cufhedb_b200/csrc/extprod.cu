@@ -126,6 +126,7 @@ __global__ void __launch_bounds__(EP_WARPS * 32) extprod1_f64_kernel(ExtProdArgs
     double2 *xp = xp_s[w];
     const Fft512Tables &T = *reinterpret_cast<const Fft512Tables *>(a.tables);
     const uint32_t *in = a.trlwe + (size_t)p * 2 * N1;
+    if (lane == 0) bulk_prefetch_l2_if_aligned(in, 2 * N1 * sizeof(uint32_t));   // the TRLWE, read per digit
     const double2 *g = reinterpret_cast<const double2 *>(a.trgsw) + (a.shared ? 0 : (size_t)p * 6 * 1024);
     double2 f0[16], f1[16];
 #pragma unroll 1
@@ -212,6 +213,7 @@ __global__ void __launch_bounds__(EP_WARPS * 32) extprod1_split_kernel(ExtProdAr
     rs.init(lane);
     const Fft512TablesPlain &T = reinterpret_cast<const Fft512TablesF *>(a.tables)->plain;
     const uint32_t *in = a.trlwe + (size_t)p * 2 * N1;
+    if (lane == 0) bulk_prefetch_l2_if_aligned(in, 2 * N1 * sizeof(uint32_t));   // the TRLWE, read per digit
     const unsigned char *g = reinterpret_cast<const unsigned char *>(a.trgsw) +
                              (a.shared ? 0 : (size_t)p * 2 * L1 * TRGSW_ROW_BYTES);
     prefetch_rows(g, 1, 2, a, lane);

@@ -291,6 +291,7 @@ __global__ void __launch_bounds__(T2) extprod2_kernel(ExtProd2Args a)
             bulk_prefetch_l2(reinterpret_cast<const unsigned char *>(g) + (size_t)k * ROW_BYTES, ROW_BYTES);
     };
     prefetch(0, 2);
+    if (t == 0) bulk_prefetch_l2_if_aligned(in, 2 * N2 * sizeof(uint64_t));   // the TRLWE, read per digit polynomial
     double2 f0[8], f1[8];
 #pragma unroll 1
     for (int r = 0; r < 2 * L2; ++r) {
