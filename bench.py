@@ -519,6 +519,7 @@ def run_ours(args):
     tune = {f"pbs01_{name}": {"pass_ms_by_shape": tuned[f"pbs01_{name}"],
                               "ciphertexts_per_cta": eng.launch_shape(1, PREC[name], B)}
             for name in ("split32", "fp64", "split32tc")}
+    tune["pbs01_split32"]["stage1_layout"] = eng.launch_layout(B)   # chosen over both split tables
     if single and args.filter_rows:
         tune["pbs02"] = {"pass_ms_by_shape": tuned["pbs02"],
                          "ciphertexts_per_cta_filter": eng.launch_shape(2, FP64, args.filter_rows)}

@@ -71,6 +71,7 @@ SIGNATURES = {
     "cufhedb_autotune_pbs02": [_vp, _vp],
     "cufhedb_autotune_table": [_vp, _i32, _i32, _vp, _vp],
     "cufhedb_launch_shape": [_vp, _i32, _i32, _i32, _vp],
+    "cufhedb_launch_layout": [_vp, _i32, _vp],
     "cufhedb_autotune_save": [_vp, C.c_char_p],
     "cufhedb_autotune_load": [_vp, C.c_char_p],
     "cufhedb_load_keyfile": [_vp, C.c_char_p, _vp],

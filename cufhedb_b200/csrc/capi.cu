@@ -164,7 +164,15 @@ bool valid_precision(int p) { return p == CUFHEDB_FP64 || p == CUFHEDB_SPLIT32 |
 // table picks for the batch (key, tables and kernel set in `a` here)
 int launch_pbs01_any(cufhedb_ctx *ctx, Pbs01Args &a, int precision, cudaStream_t st)
 {
-    const int w = pbs01_choose_w(a.B, ctx->num_sms, ctx->pbs01_pass_ms[precision]);
+    // CUFHEDB_SPLIT32 lets the measured tables pick the stage-1 layout too;
+    // CUFHEDB_SPLIT32_TC forces the tensor-core one
+    int w = pbs01_choose_w(a.B, ctx->num_sms, ctx->pbs01_pass_ms[precision]);
+    if (precision == CUFHEDB_SPLIT32) {
+        const SplitLaunch c = pbs01_split_choose(a.B, ctx->num_sms, ctx->pbs01_pass_ms[CUFHEDB_SPLIT32],
+                                                 ctx->pbs01_pass_ms[CUFHEDB_SPLIT32_TC]);
+        w = c.w;
+        if (c.tc) precision = CUFHEDB_SPLIT32_TC;
+    }
     if (precision == CUFHEDB_FP64) {
         a.bk = ctx->bk01;
         a.tables = ctx->tab512;
@@ -989,7 +997,21 @@ int cufhedb_launch_shape(cufhedb_ctx *ctx, int level, int precision, int B, int 
     NEED(ctx != nullptr && shape != nullptr, "null argument");
     const float *t = shape_table(ctx, level, precision);
     NEED(t != nullptr && B > 0, "bad level, precision or batch");
-    *shape = level == 1 ? pbs01_choose_w(B, ctx->num_sms, t) : pbs02_choose_p(B, ctx->num_sms, t);
+    if (level == 1 && precision == CUFHEDB_SPLIT32)
+        *shape = pbs01_split_choose(B, ctx->num_sms, t, ctx->pbs01_pass_ms[CUFHEDB_SPLIT32_TC]).w;
+    else
+        *shape = level == 1 ? pbs01_choose_w(B, ctx->num_sms, t) : pbs02_choose_p(B, ctx->num_sms, t);
+    return CUFHEDB_OK;
+}
+
+int cufhedb_launch_layout(cufhedb_ctx *ctx, int B, int *tensor_core_stage1)
+{
+    NEED(ctx != nullptr && tensor_core_stage1 != nullptr && B > 0, "bad argument");
+    *tensor_core_stage1 = pbs01_split_choose(B, ctx->num_sms, ctx->pbs01_pass_ms[CUFHEDB_SPLIT32],
+                                             ctx->pbs01_pass_ms[CUFHEDB_SPLIT32_TC])
+                              .tc
+                              ? 1
+                              : 0;
     return CUFHEDB_OK;
 }
 

@@ -107,6 +107,36 @@ inline int pbs01_choose_w(int B, int num_sms, const float pass_ms[NSHAPES])
 {
     return choose_shape(B, num_sms, PBS01_SHAPES, pass_ms);
 }
+// a pass-time table still at the context's untuned default (every entry
+// exactly 1.0; no measured pass takes exactly 1 ms)
+inline bool shape_table_measured(const float pass_ms[NSHAPES])
+{
+    for (int i = 0; i < NSHAPES; ++i)
+        if (pass_ms[i] != 1.0f) return true;
+    return false;
+}
+// The split path's launch: the shape and the stage-1 layout (CUDA cores, or
+// tensor cores when both tables are measured) with the least passes x pass
+// time; ties go to the CUDA-core layout, then to the earlier shape.
+struct SplitLaunch {
+    int w;
+    bool tc;
+};
+inline SplitLaunch pbs01_split_choose(int B, int num_sms, const float cc_ms[NSHAPES], const float tc_ms[NSHAPES])
+{
+    auto cost = [&](int i, const float *t) {
+        const int groups = (B + PBS01_SHAPES[i] - 1) / PBS01_SHAPES[i];
+        return (float)((groups + num_sms - 1) / num_sms) * t[i];
+    };
+    SplitLaunch best{PBS01_SHAPES[0], false};
+    float best_cost = cost(0, cc_ms);
+    for (int i = 1; i < NSHAPES; ++i)
+        if (cost(i, cc_ms) < best_cost) best = {PBS01_SHAPES[i], false}, best_cost = cost(i, cc_ms);
+    if (shape_table_measured(cc_ms) && shape_table_measured(tc_ms))
+        for (int i = 0; i < NSHAPES; ++i)
+            if (cost(i, tc_ms) < best_cost) best = {PBS01_SHAPES[i], true}, best_cost = cost(i, tc_ms);
+    return best;
+}
 inline int pbs02_choose_p(int B, int num_sms, const float pass_ms[NSHAPES])
 {
     return choose_shape(B, num_sms, PBS02_SHAPES, pass_ms);

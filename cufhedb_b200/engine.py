@@ -180,6 +180,13 @@ class Engine:
         check(self.lib.cufhedb_launch_shape(self.ctx, level, precision, B, C.byref(w)))
         return w.value
 
+    def launch_layout(self, B: int) -> str:
+        """stage-1 layout a split32 launch of B bootstraps would use now:
+        "cuda-core" or "tensor-core" """
+        tc = C.c_int(0)
+        check(self.lib.cufhedb_launch_layout(self.ctx, B, C.byref(tc)))
+        return "tensor-core" if tc.value else "cuda-core"
+
     def autotune_save(self, path: str):
         check(self.lib.cufhedb_autotune_save(self.ctx, path.encode()))
 

@@ -391,8 +391,12 @@ CUFHEDB_API int cufhedb_selftest_wait_timeout(cufhedb_ctx *ctx, uint32_t polls);
  * takes ceil(ceil(B / shape) / SMs) passes; every launch (PBS, gates,
  * operator chains) picks the shape with the least passes x measured pass
  * time, ties to the earlier shape; without measurements all pass times count
- * as equal.  No counterpart in the reference, which runs one ciphertext per
- * launch.  The tuning calls are synchronous; call them outside stream capture. */
+ * as equal.  CUFHEDB_SPLIT32 launches also pick the layout of the first
+ * transform step, on the CUDA cores or on the tensor cores (the
+ * CUFHEDB_SPLIT32_TC kernel), by the same rule over both tables once both
+ * are measured, ties to the CUDA cores.  No counterpart in the reference,
+ * which runs one ciphertext per launch.  The tuning calls are synchronous;
+ * call them outside stream capture. */
 /* times one full pass of each lvl01 shape for `precision` (uniform random lvl0
  * inputs, the loaded key) and keeps them in the context; ms_w7 / ms_w8 (may be
  * NULL) receive the 7- and 8-per-CTA pass times */
@@ -404,6 +408,9 @@ CUFHEDB_API int cufhedb_autotune_pbs02(cufhedb_ctx *ctx, float *ms);
 CUFHEDB_API int cufhedb_autotune_table(cufhedb_ctx *ctx, int level, int precision, int *shapes, float *pass_ms);
 /* the shape (ciphertexts per CTA) a launch of B ciphertexts would use now */
 CUFHEDB_API int cufhedb_launch_shape(cufhedb_ctx *ctx, int level, int precision, int B, int *shape);
+/* the stage-1 layout a CUFHEDB_SPLIT32 launch of B ciphertexts would use now:
+ * *tensor_core_stage1 = 1 (tensor cores) or 0 (CUDA cores) */
+CUFHEDB_API int cufhedb_launch_layout(cufhedb_ctx *ctx, int B, int *tensor_core_stage1);
 /* persist / restore the context's pass times: a text file keyed by the device
  * name, the SM count and a hash of the parameter set and shape lists; load
  * refuses a table made for anything else (CUFHEDB_ERR_ARG), after which the

@@ -403,6 +403,7 @@ class CuFFT_Torus {
         if constexpr (P::n == 1024) {
             cufhedb_dropin::check(cufhedb_autotune_pbs01(ctx, CUFHEDB_FP64, nullptr, nullptr));
             cufhedb_dropin::check(cufhedb_autotune_pbs01(ctx, CUFHEDB_SPLIT32, nullptr, nullptr));
+            cufhedb_dropin::check(cufhedb_autotune_pbs01(ctx, CUFHEDB_SPLIT32_TC, nullptr, nullptr));
         } else {
             cufhedb_dropin::check(cufhedb_autotune_pbs02(ctx, nullptr));
         }

@@ -75,6 +75,42 @@ def test_every_lvl01_shape_bootstraps_correctly(eng2, tmp_path, precision, shape
         assert eng2.autotune_load(real)
 
 
+def test_split_launch_picks_the_stage1_layout_from_the_tables(eng2, tmp_path):
+    """CUFHEDB_SPLIT32 launches take the tensor-core stage 1 only when its
+    measured pass time is the shortest: with this GPU's measured tables the
+    CUDA-core layout (as on B200), with a table in which the tensor-core
+    7-per-CTA pass is the only short one the tensor-core layout, and the
+    gates decrypt either way."""
+    import torch
+    from cufhedb_b200 import SPLIT32, SPLIT32_TC
+    B = 1000
+    eng2.autotune()
+    measured = eng2.autotune_table(1, SPLIT32)
+    measured_tc = eng2.autotune_table(1, SPLIT32_TC)
+    cc_best = min(-(-(-(-B // w)) // eng2.num_sms) * t for w, t in measured.items())
+    tc_best = min(-(-(-(-B // w)) // eng2.num_sms) * t for w, t in measured_tc.items())
+    assert eng2.launch_layout(B) == ("tensor-core" if tc_best < cc_best else "cuda-core")
+    real = _force(eng2, tmp_path, 1, SPLIT32_TC, 7)
+    try:
+        assert eng2.launch_layout(B) == "tensor-core"
+        assert eng2.launch_shape(1, SPLIT32, B) == 7
+        bits = torch.randint(0, 2, (2, B), generator=torch.Generator().manual_seed(77))
+        msg = torch.where(bits == 1, MU1, -MU1).to(torch.int32).cuda()
+        ca = torch.empty(B * (N1 + 1), dtype=torch.int32, device="cuda")
+        cb = torch.empty_like(ca)
+        eng2.encrypt_lvl1(SEED, 0xC7, 0, msg[0].contiguous(), ca)
+        eng2.encrypt_lvl1(SEED, 0xC7, B, msg[1].contiguous(), cb)
+        out = torch.empty_like(ca)
+        eng2.gate_lvl1("NAND", ca, cb, out, SPLIT32)
+        ph = torch.empty(B, dtype=torch.int32, device="cuda")
+        eng2.phase_lvl1(out, ph)
+        eng2.sync()
+        got = (ph > 0).cpu().numpy().astype(int)
+        assert np.array_equal(got, 1 - (bits[0] & bits[1]).numpy().astype(int))
+    finally:
+        assert eng2.autotune_load(real)
+
+
 @pytest.mark.parametrize("shape", [3, 2, 1])
 def test_every_lvl02_shape_bootstraps_correctly(eng2, oracle, keys, tmp_path, shape):
     import torch

@@ -106,3 +106,58 @@ def test_hand_worked_cases(choices):
     assert c(2, "f64", SMS + 1) == 2                        # 2 x 8.0 = 16.0 vs one pass of 2 (13.5)
     assert c(2, "f64", 2 * SMS + 1) == 3                    # 297: one pass of 3 (17.7) vs 2 of 2 (27.0)
     assert c(2, "f64", 16384) == 3                          # 37 x 17.7 = 654.9 vs 56 x 13.5 = 756.0
+
+
+SPLIT_PROG = r"""
+#include "pbs_common.cuh"
+#include <cstdio>
+#include <cstdlib>
+int main(int argc, char **argv)
+{
+    float cc[3], tc[3];
+    for (int i = 0; i < 3; ++i) cc[i] = (float)atof(argv[1 + i]), tc[i] = (float)atof(argv[4 + i]);
+    for (int B = 1; B <= %d; ++B) {
+        const cfdb::SplitLaunch c = cfdb::pbs01_split_choose(B, %d, cc, tc);
+        std::printf("%%d %%d\n", c.w, c.tc ? 1 : 0);
+    }
+    return 0;
+}
+""" % (BMAX, SMS)
+
+
+def _split_rule(B, cc, tc):
+    """the split launch: least passes x pass time over the CUDA-core table,
+    then the tensor-core one (only when both are measured); ties to the
+    CUDA-core layout and the earlier shape"""
+    measured = lambda t: any(x != 1.0 for x in t)
+    cost = lambda i, t: -(-(-(-B // SHAPES[1][i])) // SMS) * t[i]
+    best, best_cost = (SHAPES[1][0], 0), cost(0, cc)
+    for i in range(1, 3):
+        if cost(i, cc) < best_cost:
+            best, best_cost = (SHAPES[1][i], 0), cost(i, cc)
+    if measured(cc) and measured(tc):
+        for i in range(3):
+            if cost(i, tc) < best_cost:
+                best, best_cost = (SHAPES[1][i], 1), cost(i, tc)
+    return best
+
+
+@pytest.mark.parametrize("cc, tc", [
+    ((9.40, 10.30, 7.50), (13.06, 13.12, 9.93)),   # as measured on B200: the CUDA cores everywhere
+    ((9.40, 10.30, 7.50), (1.0, 1.0, 1.0)),        # tensor-core table unmeasured: never chosen
+    ((9.40, 10.30, 7.50), (9.0, 10.30, 7.50)),     # tensor cores faster at 7 per CTA only
+    ((1.0, 1.0, 1.0), (0.5, 0.5, 0.5)),            # CUDA-core table unmeasured: CUDA cores
+])
+def test_split_layout_choice_matches_rule(tmp_path, cc, tc):
+    nvcc = _nvcc()
+    if nvcc is None:
+        pytest.skip("nvcc not available")
+    src, exe = tmp_path / "split.cu", tmp_path / "split"
+    src.write_text(SPLIT_PROG)
+    subprocess.run([nvcc, "-std=c++17", "-I", CSRC, "-o", str(exe), str(src)], check=True, capture_output=True)
+    out = subprocess.run([str(exe), *map(str, cc), *map(str, tc)], check=True, capture_output=True,
+                         text=True).stdout.split("\n")
+    got = [tuple(int(x) for x in line.split()) for line in out if line]
+    assert len(got) == BMAX
+    for B in range(1, BMAX + 1):
+        assert got[B - 1] == _split_rule(B, [float(x) for x in cc], [float(x) for x in tc]), B
