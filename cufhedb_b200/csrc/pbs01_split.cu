@@ -121,87 +121,104 @@ __device__ __forceinline__ CP pmul_first(unsigned long long vr, unsigned long lo
 }
 
 // Tensor-core stage 1 (tc_stage1.cuh), shared by the warps of a group of
-// four (warps 0-3 and 4-7; a producer warp takes no part): each warp writes
-// its 32 A rows into its own sub-partition's lanes of the group's A columns,
-// the group meets at a named barrier, one lane of the group's first warp
-// issues the M = 128 MMAs for all four and commits them to the group's
-// mbarrier for that buffer, and every warp of the group waits on it.  Per
-// group: A double-buffered (16 columns each), D double-buffered (32 columns
-// each).  Every warp takes part in every step, active or not (a warp whose
-// rotation is 0 for this CMux writes no rows and reads no result), so the
-// barriers and the buffer reuse stay in step.  Addresses are recomputed from
-// the block's shared memory and the warp index at each use (the kernel runs
-// at the 255-register limit).
-constexpr uint32_t TC_GROUP_COLS = 96;
+// four (warps 0-3 and 4-7; a producer warp takes no part), one polynomial at
+// a time: when a polynomial's decomposition words are formed, each warp
+// writes the A rows of all three of its digit polynomials into its own
+// sub-partition's lanes of the group's A columns (the words are dead right
+// after), the group meets at a named barrier, and one lane of the group's
+// first warp issues the polynomial's three M = 128 products into three of the
+// group's six D buffers and commits them to the polynomial's mbarrier.
+// Polynomial 0's products are issued at the start of a CMux and taken at
+// digit 0; polynomial 1's are issued at digit 1 (A is free again: every
+// warp waited for polynomial 0's products at digit 0) and run under the
+// transforms of digits 1 and 2.  Per group (256 columns): D 6 x 32 columns
+// first, each on a 32-column boundary, then A 3 x 16.
+// Every warp takes part in every step, active or not (a warp whose rotation
+// is 0 for this CMux writes no rows and reads no result), so the barriers and
+// the buffer reuse stay in step.  Addresses are recomputed from the block's
+// shared memory and the warp index at each use (the kernel runs at the
+// 255-register limit).
+constexpr uint32_t TC_D_COLS = 6 * 32, TC_GROUP_COLS = 256;   // D at [0, 192), A at [192, 240)
 
 template <class L, int W>
 struct TcStage {
     unsigned char *smem;
-    uint32_t phase;     // per buffer (bits 0, 1): parity of its next completion
+    uint32_t phase;     // per polynomial (bits 0, 1): parity of its next completion
 
     __device__ __forceinline__ static int group(int warp) { return warp >> 2; }
     __device__ __forceinline__ uint32_t tbase() const
     {
         return *reinterpret_cast<const volatile uint32_t *>(smem + L::TC_SLOT_OFF);
     }
-    __device__ __forceinline__ uint64_t *bar(int warp, int buf) const
+    __device__ __forceinline__ uint32_t lanes(int warp) const
     {
-        return reinterpret_cast<uint64_t *>(smem + L::TC_BAR_OFF) + 2 * group(warp) + buf;
+        return tbase() + TC_GROUP_COLS * group(warp) + ((32u * (warp & 3)) << 16);
     }
-    // A(buf) <- the digit-d row of this lane (only when active)
-    __device__ __forceinline__ void put(const uint32_t *w, bool active, int d, int buf, int warp)
+    __device__ __forceinline__ uint64_t *bar(int warp, int poly) const
+    {
+        return reinterpret_cast<uint64_t *>(smem + L::TC_BAR_OFF) + 2 * group(warp) + poly;
+    }
+    // A(d) <- the digit-d row of this lane, d < 3 (only when active), then the
+    // group meets and its first warp issues D(3 poly + d) = A(d) (Bhi + Blo)
+    __device__ __forceinline__ void put_issue(const uint32_t *w, bool active, int poly, int warp, int lane)
     {
         if (active) {
-            uint32_t a[16];
-            tc_a_row(a, w, d);
-            tmem_st16(tbase() + TC_GROUP_COLS * group(warp) + ((32u * (warp & 3)) << 16) + 16 * buf, a);
+#pragma unroll 1
+            for (int d = 0; d < L1; ++d) {
+                uint32_t a[16];
+                tc_a_row(a, w, d);
+                tmem_st16(lanes(warp) + TC_D_COLS + 16 * d, a);
+            }
             tmem_wait_st();
         }
-    }
-    // the group meets, then its first warp issues D(buf) = A(buf) (Bhi + Blo)
-    __device__ __forceinline__ void issue(int buf, int warp, int lane)
-    {
         tc_fence_before();
         if (group(warp) == 0) asm volatile("bar.sync 2, %0;" ::"n"(32 * (W < 4 ? W : 4)) : "memory");
         else asm volatile("bar.sync 3, %0;" ::"n"(32 * (W > 4 ? W - 4 : 1)) : "memory");
         if ((warp & 3) == 0 && lane == 0) {
             tc_fence_after();
             const uint32_t gcol = tbase() + TC_GROUP_COLS * group(warp);
-            const uint32_t a = gcol + 16 * buf, dcol = gcol + 32 + 32 * buf;
             const uint32_t b = smem_u32(smem + L::TC_OFF), limb = TC_B_HALVES * 2, kstep = 2 * TC_B_LBO;
-            umma_ts(dcol, a, tc_smem_desc(b, TC_B_LBO, TC_B_SBO), 0);
-            umma_ts(dcol, a + 8, tc_smem_desc(b + kstep, TC_B_LBO, TC_B_SBO), 1);
-            umma_ts(dcol, a, tc_smem_desc(b + limb, TC_B_LBO, TC_B_SBO), 1);
-            umma_ts(dcol, a + 8, tc_smem_desc(b + limb + kstep, TC_B_LBO, TC_B_SBO), 1);
-            umma_commit(bar(warp, buf));
+#pragma unroll
+            for (int d = 0; d < L1; ++d) {
+                const uint32_t a = gcol + TC_D_COLS + 16 * d, dcol = gcol + 32 * (L1 * poly + d);
+                umma_ts(dcol, a, tc_smem_desc(b, TC_B_LBO, TC_B_SBO), 0);
+                umma_ts(dcol, a + 8, tc_smem_desc(b + kstep, TC_B_LBO, TC_B_SBO), 1);
+                umma_ts(dcol, a, tc_smem_desc(b + limb, TC_B_LBO, TC_B_SBO), 1);
+                umma_ts(dcol, a + 8, tc_smem_desc(b + limb + kstep, TC_B_LBO, TC_B_SBO), 1);
+            }
+            umma_commit(bar(warp, poly));
         }
         __syncwarp();
     }
-    // waits for the group's product in buffer buf and (when active) reads
-    // this lane's row: v[q] = X[q]
-    __device__ __forceinline__ void take(float2 v[16], bool active, int buf, int warp, int *err)
+    // waits for a polynomial's three products
+    __device__ __forceinline__ void wait(int poly, int warp, int *err)
     {
-        if (!mbar_wait(bar(warp, buf), (phase >> buf) & 1)) report_error(err, DEV_TIMEOUT_MMA);
-        phase ^= 1u << buf;
+        if (!mbar_wait(bar(warp, poly), (phase >> poly) & 1)) report_error(err, DEV_TIMEOUT_MMA);
+        phase ^= 1u << poly;
+        tc_fence_after();
+    }
+    // this lane's row of digit polynomial r's product (only when active):
+    // v[q] = X[q]
+    __device__ __forceinline__ void take(float2 v[16], bool active, int r, int warp)
+    {
         if (active) {
-            tc_fence_after();
-            uint32_t r[32];
-            tmem_ld32(tbase() + TC_GROUP_COLS * group(warp) + ((32u * (warp & 3)) << 16) + 32 + 32 * buf, r);
+            uint32_t x[32];
+            tmem_ld32(lanes(warp) + 32 * r, x);
 #pragma unroll
-            for (int q = 0; q < 16; ++q) v[q] = make_float2(__uint_as_float(r[q]), __uint_as_float(r[16 + q]));
+            for (int q = 0; q < 16; ++q) v[q] = make_float2(__uint_as_float(x[q]), __uint_as_float(x[16 + q]));
         }
         tc_fence_before();
         __syncwarp();
     }
 };
 
-// tensor-memory columns of a block: TC_GROUP_COLS per group of four consumer
-// warps, rounded up to a power of two (the allocation unit)
 template <int W>
 constexpr uint32_t tc_cols()
 {
-    return ((W + 3) / 4) * TC_GROUP_COLS <= 128 ? 128u : 256u;
+    return ((W + 3) / 4) * TC_GROUP_COLS <= 256 ? 256u : 512u;
 }
+static_assert(2 * TC_GROUP_COLS <= 512 && TC_D_COLS + 3 * 16 <= TC_GROUP_COLS,
+              "two groups' columns within one SM's tensor memory");
 
 // W consumer warps, plus a producer warp when PRODUCER (ring.cuh has both
 // feeds; the launch picks per shape, see launch_pbs01_split).  TC: the first
@@ -287,28 +304,19 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
             const bool active = ab != 0;
             CP f0[16], f1[16];
             uint32_t w[32];
-            if constexpr (TC) {
-                // the product of digit polynomial 0 is in flight before the loop
-                if (active) digit_words1(w, acc, ab, lane);
-                tc.put(w, active, 0, 0, warp);
-                tc.issue(0, warp, lane);
-            }
 #pragma unroll 1
             for (int r = 0; r < 2 * L1; ++r, ++c) {
                 float2 v[16];
                 if constexpr (TC) {
-                    // stage the next digit polynomial, take this one's product,
-                    // then start the next one's, which runs while this one is
-                    // transformed
-                    if (r + 1 < 2 * L1 && active) {
-                        // the words are recomputed for each digit polynomial
-                        // (not carried across the transform: register room)
-                        uint32_t wn[32];
-                        digit_words1(wn, acc + ((r + 1) / L1) * N1, ab, lane);
-                        tc.put(wn, true, (r + 1) % L1, (r + 1) & 1, warp);
+                    if (r < 2) {
+                        // polynomial r's three products (one call site for both:
+                        // code size); polynomial 1's run under the transforms of
+                        // digits 1 and 2
+                        if (active) digit_words1(w, acc + r * N1, ab, lane);
+                        tc.put_issue(w, active, r, warp, lane);
                     }
-                    tc.take(v, active, r & 1, warp, a.err);
-                    if (r + 1 < 2 * L1) tc.issue((r + 1) & 1, warp, lane);
+                    if (r % L1 == 0) tc.wait(r / L1, warp, a.err);
+                    tc.take(v, active, r, warp);
                 } else {
                     if (active && r % L1 == 0) digit_words1(w, acc + (r / L1) * N1, ab, lane);
                 }

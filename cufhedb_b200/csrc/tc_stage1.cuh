@@ -20,13 +20,15 @@
 // carries FP32 accumulation rounding only, as the CUDA-core stage does.
 //
 // The consumer warps work in groups of four (one per sub-partition).  A group
-// has its own tensor-memory columns: A (16 columns: 32 FP16 per row, two per
-// 32-bit column) and D (32 FP32 columns), both double-buffered.  Each warp
-// writes its 32 rows into the 32 lanes of its sub-partition (tcgen05.st), the
-// group meets at a named barrier, one lane of its first warp issues the
-// M = 128 MMAs (A from tensor memory, B from shared memory) for all four
-// warps and commits them to the group's mbarrier, and each warp reads its own
-// 32 rows of D back (tcgen05.ld).
+// has its own 256 tensor-memory columns: D for the six digit polynomials of a
+// CMux (6 x 32 FP32 columns, each on a 32-column boundary) and A for the
+// three digits of one polynomial (3 x 16 columns: 32 FP16 per row, two per
+// 32-bit column).  Each warp writes its 32 rows into the 32 lanes of its
+// sub-partition (tcgen05.st), the group meets at a named barrier, one lane of
+// its first warp issues a polynomial's M = 128 MMAs (A from tensor memory, B
+// from shared memory) for all four warps and commits them to that
+// polynomial's mbarrier, and each warp reads its own 32 rows of D back
+// (tcgen05.ld).
 #pragma once
 #include <cuda_fp16.h>
 
