@@ -274,7 +274,9 @@ int main()
             want[P1::n] += c;
             worst_lift = std::max<int64_t>(worst_lift, std::llabs((int64_t)phase(lift, sk) - phase(want, sk)));
         }
-        report("cuARCEDB HomAND / HomOR / lift_and_and, 8 inputs", bad == 0 && worst_lift < (1 << 24),
+        // two independent bootstraps' outputs differ by ~sqrt(2) x the output
+        // noise (std ~2^22.3), so the bound is 2^25 as in the other phase checks
+        report("cuARCEDB HomAND / HomOR / lift_and_and, 8 inputs", bad == 0 && worst_lift < (1 << 25),
                "wrong " + std::to_string(bad) + ", lift phase |diff| vs TFHEpp " + std::to_string(worst_lift));
     }
 
