@@ -170,11 +170,144 @@ __global__ void __launch_bounds__(NT) iks_kernel(IksArgs a)
     }
 }
 
+// ---- key-stationary lvl2 -> lvl1 switch (large batches) ------------------------
+// The gather above reads each selected 4,100-byte key row once per ciphertext:
+// 75 GB per 1,024 ciphertexts, served from L2 (the 0.59 GB key stays there).
+// Turned around, each CTA owns 16 output words of 256 ciphertexts and walks
+// the whole key once, staging those 16 words of every key row in shared
+// memory (2.4 GB of L2 reads per 1,024 ciphertexts), and each thread, one
+// ciphertext, subtracts the staged words of the rows its digits select.  The
+// subtractions are the gather's, in the same order per word (ascending i,
+// j), so the results are identical.
+constexpr int KS_TILE = 256;                          // ciphertexts per CTA, one per thread
+constexpr int KS_WB = 16;                             // output words per CTA
+constexpr int KS_NB = (N1 + 1 + KS_WB - 1) / KS_WB;   // word blocks: 65
+constexpr int KS_IC = 2;                              // input coefficients per staged chunk
+constexpr int KS_DIG = 1 << KS21_BASEBIT;             // digit values 0..7 (row 0: zeros)
+constexpr int KS_ROWS = KS_IC * KS21_T * KS_DIG;      // staged rows per chunk: 160
+constexpr int KS_RW4 = 5;                             // uint4 per staged row: 16 words + 4 pad
+constexpr int KS_P4 = ksk_pitch(N1 + 1) / 4;          // uint4 per key row in HBM: 257
+constexpr int KS_LOADS = KS_IC * KS21_T * (KS_DIG - 1) * (KS_WB / 4);   // uint4 per chunk: 560
+constexpr int KS_PER = (KS_LOADS + KS_TILE - 1) / KS_TILE;              // per thread: 3
+constexpr uint64_t KS_PREC = 1ull << (64 - (1 + KS21_BASEBIT * KS21_T));
+constexpr int KS_SHIFT = 64 - KS21_BASEBIT * KS21_T;                    // the digits' 30 bits
+
+// X[i][b] = the top 30 bits of a_i + prec_offset (ciphertext b's ten digits
+// of coefficient i), 0 for the padding b >= B
+__global__ void ks21_prep_kernel(const uint64_t *__restrict__ in, uint32_t *X, int B, int Bp)
+{
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (size_t)N2 * Bp) return;
+    const int i = (int)(idx / Bp), b = (int)(idx % Bp);
+    X[idx] = b < B ? (uint32_t)((in[(size_t)b * (N2 + 1) + i] + KS_PREC) >> KS_SHIFT) : 0u;
+}
+
+__global__ void __launch_bounds__(KS_TILE) ks21_kernel(const uint32_t *__restrict__ X, int Bp,
+                                                       const uint4 *__restrict__ ksk, const uint64_t *in,
+                                                       uint32_t *out, int B, uint64_t offset64)
+{
+    __shared__ uint4 stage[2][KS_ROWS * KS_RW4];
+    const int t = threadIdx.x, s = blockIdx.x, ct = blockIdx.y * KS_TILE + t;
+    // digit-0 rows are zero in both buffers (never written again)
+    for (int e = t; e < 2 * KS_IC * KS21_T * KS_RW4; e += KS_TILE) {
+        const int buf = e / (KS_IC * KS21_T * KS_RW4), rem = e % (KS_IC * KS21_T * KS_RW4);
+        stage[buf][(rem / KS_RW4) * KS_DIG * KS_RW4 + rem % KS_RW4] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    // this thread's share of chunk c: key row (i, j, d) words 16 s + 4 q .. + 3,
+    // where they exist (the last word block holds only the padded row's word
+    // 1024 and its pad: q = 0)
+    uint4 r[KS_PER];
+    auto load = [&](int c) {
+#pragma unroll
+        for (int k = 0; k < KS_PER; ++k) {
+            const int e = t + k * KS_TILE;
+            r[k] = make_uint4(0u, 0u, 0u, 0u);
+            if (e < KS_LOADS) {
+                const int q = e % 4, row = e / 4;   // row = (ii T + j) (2^b - 1) + d - 1
+                const int w4 = (KS_WB / 4) * s + q;
+                if (w4 < KS_P4) {
+                    const size_t g = (size_t)c * KS_IC * KS21_T * (KS_DIG - 1) + row;
+                    r[k] = __ldg(ksk + g * KS_P4 + w4);
+                }
+            }
+        }
+    };
+    auto store = [&](int buf) {
+#pragma unroll
+        for (int k = 0; k < KS_PER; ++k) {
+            const int e = t + k * KS_TILE;
+            if (e < KS_LOADS) {
+                const int q = e % 4, row = e / 4, ij = row / (KS_DIG - 1), d = row % (KS_DIG - 1) + 1;
+                stage[buf][(ij * KS_DIG + d) * KS_RW4 + q] = r[k];
+            }
+        }
+    };
+    uint32_t acc[KS_WB];
+#pragma unroll
+    for (int k = 0; k < KS_WB; ++k) acc[k] = 0u;
+    constexpr int NCHUNK = N2 / KS_IC;
+    load(0);
+    store(0);
+    __syncthreads();
+#pragma unroll 1
+    for (int c = 0; c < NCHUNK; ++c) {
+        if (c + 1 < NCHUNK) load(c + 1);
+        const uint4 *buf = stage[c & 1];
+#pragma unroll
+        for (int ii = 0; ii < KS_IC; ++ii) {
+            const uint32_t x = X[(size_t)(c * KS_IC + ii) * Bp + (size_t)blockIdx.y * KS_TILE + t];
+#pragma unroll
+            for (int j = 0; j < KS21_T; ++j) {
+                const uint32_t d = (x >> (KS21_BASEBIT * (KS21_T - 1 - j))) & (KS_DIG - 1);
+                const uint4 *row = buf + ((ii * KS21_T + j) * KS_DIG + d) * KS_RW4;
+#pragma unroll
+                for (int q = 0; q < KS_WB / 4; ++q) {
+                    const uint4 v = row[q];
+                    acc[4 * q] -= v.x;
+                    acc[4 * q + 1] -= v.y;
+                    acc[4 * q + 2] -= v.z;
+                    acc[4 * q + 3] -= v.w;
+                }
+            }
+        }
+        if (c + 1 < NCHUNK) store((c + 1) & 1);
+        __syncthreads();
+    }
+    if (ct >= B) return;
+    const uint32_t bnew = (uint32_t)((in[(size_t)ct * (N2 + 1) + N2] + offset64 + (1ull << 31)) >> 32);
+    uint32_t *o = out + (size_t)ct * (N1 + 1);
+#pragma unroll
+    for (int k = 0; k < KS_WB; ++k) {
+        const int w = KS_WB * s + k;
+        if (w < N1) o[w] = acc[k];
+        else if (w == N1) o[w] = acc[k] + bnew;
+    }
+}
+
+// batches from this size on take the key-stationary lvl2 -> lvl1 switch
+constexpr int KS21_MIN_BATCH = 512;
+
 }  // namespace
 
 cudaError_t launch_iks(const IksArgs &a, int kind, cudaStream_t st)
 {
     if (a.B <= 0) return cudaSuccess;
+    if (kind == 21 && a.B >= KS21_MIN_BATCH) {
+        const int tiles = (a.B + KS_TILE - 1) / KS_TILE, Bp = tiles * KS_TILE;
+        uint32_t *X = nullptr;
+        cudaError_t e = cudaMallocAsync((void **)&X, (size_t)N2 * Bp * sizeof(uint32_t), st);
+        if (e != cudaSuccess) return e;
+        const size_t n = (size_t)N2 * Bp;
+        ks21_prep_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.in64, X, a.B, Bp);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) {
+            ks21_kernel<<<dim3(KS_NB, tiles), KS_TILE, 0, st>>>(X, Bp, reinterpret_cast<const uint4 *>(a.ksk),
+                                                                 a.in64, a.out, a.B, a.offset64);
+            e = cudaGetLastError();
+        }
+        const cudaError_t ef = cudaFreeAsync(X, st);
+        return e != cudaSuccess ? e : ef;
+    }
     // one 16-byte word of a padded row per thread: 169 of 192 (lvl0 rows),
     // 257 of 288 (lvl1 rows)
     if (kind == 10)

@@ -149,6 +149,32 @@ def test_iks_from_lvl2_bit_exact(engine2, oracle, keys, kind):
         assert np.array_equal(oracle.iks(kind, x, SEED, keys), o)
 
 
+def test_iks21_key_stationary_batch_equals_gather(engine2, oracle, keys):
+    """Batches of 512 and more take the key-stationary lvl2 -> lvl1 switch; on
+    600 ciphertexts (a ragged third tile of 256) it gives bit for bit what
+    the per-ciphertext gather gives on the same inputs in batches of 8, and
+    sampled rows equal the oracle's key switch."""
+    import torch
+    _, _, s2 = keys
+    B, width = 600, N1 + 1
+    rng = np.random.default_rng(71)
+    xs = rng.integers(0, 2 ** 64, (B, N2 + 1), dtype=np.uint64)
+    xs[0, :] = 0
+    xs[1, :N2] = 0
+    x_d = _dev(xs).reshape(-1)
+    big = torch.empty(B * width, dtype=torch.int32, device="cuda")
+    engine2.iks(21, x_d, big)
+    small = torch.empty_like(big)
+    per = N2 + 1
+    for b0 in range(0, B, 8):
+        engine2.iks(21, x_d[b0 * per:(b0 + 8) * per], small[b0 * width:(b0 + 8) * width])
+    engine2.sync()
+    assert torch.equal(big, small)
+    got = big.cpu().numpy().view(np.uint32).reshape(B, width)
+    for i in (0, 1, 2, 255, 256, 511, 512, B - 1):
+        assert np.array_equal(oracle.iks(21, xs[i], SEED, keys), got[i]), i
+
+
 def test_host_ksk21_loads_into_the_padded_device_layout(engine2, oracle, keys):
     """A whole lvl21 key-switching key handed over as a host array in TFHEpp's
     packed row layout (cufhedb_load_ksk) lands in the device layout (rows
