@@ -173,22 +173,25 @@ __global__ void __launch_bounds__(NT) iks_kernel(IksArgs a)
 // ---- key-stationary lvl2 -> lvl1 switch (large batches) ------------------------
 // The gather above reads each selected 4,100-byte key row once per ciphertext:
 // 75 GB per 1,024 ciphertexts, served from L2 (the 0.59 GB key stays there).
-// Turned around, each CTA owns 16 output words of 256 ciphertexts and walks
-// the whole key once, staging those 16 words of every key row in shared
+// Turned around, each CTA owns 8 output words of 256 ciphertexts and walks
+// the whole key once, staging those 8 words of every key row in shared
 // memory (2.4 GB of L2 reads per 1,024 ciphertexts), and each thread, one
 // ciphertext, subtracts the staged words of the rows its digits select.  The
 // subtractions are the gather's, in the same order per word (ascending i,
-// j), so the results are identical.
+// j), so the results are identical.  Eight words per CTA (129 word blocks)
+// give 28 warps per SM at 1,024 ciphertexts; the staged rows are padded to
+// 48 bytes, so the eight digit values of a quarter-warp's 16-byte reads fall
+// in eight distinct bank groups.
 constexpr int KS_TILE = 256;                          // ciphertexts per CTA, one per thread
-constexpr int KS_WB = 16;                             // output words per CTA
-constexpr int KS_NB = (N1 + 1 + KS_WB - 1) / KS_WB;   // word blocks: 65
+constexpr int KS_WB = 8;                              // output words per CTA
+constexpr int KS_NB = (N1 + 1 + KS_WB - 1) / KS_WB;   // word blocks: 129
 constexpr int KS_IC = 2;                              // input coefficients per staged chunk
 constexpr int KS_DIG = 1 << KS21_BASEBIT;             // digit values 0..7 (row 0: zeros)
 constexpr int KS_ROWS = KS_IC * KS21_T * KS_DIG;      // staged rows per chunk: 160
-constexpr int KS_RW4 = 5;                             // uint4 per staged row: 16 words + 4 pad
+constexpr int KS_RW4 = 3;                             // uint4 per staged row: 8 words + 4 pad
 constexpr int KS_P4 = ksk_pitch(N1 + 1) / 4;          // uint4 per key row in HBM: 257
-constexpr int KS_LOADS = KS_IC * KS21_T * (KS_DIG - 1) * (KS_WB / 4);   // uint4 per chunk: 560
-constexpr int KS_PER = (KS_LOADS + KS_TILE - 1) / KS_TILE;              // per thread: 3
+constexpr int KS_LOADS = KS_IC * KS21_T * (KS_DIG - 1) * (KS_WB / 4);   // uint4 per chunk: 280
+constexpr int KS_PER = (KS_LOADS + KS_TILE - 1) / KS_TILE;              // per thread: 2
 constexpr uint64_t KS_PREC = 1ull << (64 - (1 + KS21_BASEBIT * KS21_T));
 constexpr int KS_SHIFT = 64 - KS21_BASEBIT * KS21_T;                    // the digits' 30 bits
 
@@ -202,7 +205,7 @@ __global__ void ks21_prep_kernel(const uint64_t *__restrict__ in, uint32_t *X, i
     X[idx] = b < B ? (uint32_t)((in[(size_t)b * (N2 + 1) + i] + KS_PREC) >> KS_SHIFT) : 0u;
 }
 
-__global__ void __launch_bounds__(KS_TILE) ks21_kernel(const uint32_t *__restrict__ X, int Bp,
+__global__ void __launch_bounds__(KS_TILE, 4) ks21_kernel(const uint32_t *__restrict__ X, int Bp,
                                                        const uint4 *__restrict__ ksk, const uint64_t *in,
                                                        uint32_t *out, int B, uint64_t offset64)
 {
@@ -223,7 +226,7 @@ __global__ void __launch_bounds__(KS_TILE) ks21_kernel(const uint32_t *__restric
             const int e = t + k * KS_TILE;
             r[k] = make_uint4(0u, 0u, 0u, 0u);
             if (e < KS_LOADS) {
-                const int q = e % 4, row = e / 4;   // row = (ii T + j) (2^b - 1) + d - 1
+                const int q = e % (KS_WB / 4), row = e / (KS_WB / 4);   // row = (ii T + j) (2^b - 1) + d - 1
                 const int w4 = (KS_WB / 4) * s + q;
                 if (w4 < KS_P4) {
                     const size_t g = (size_t)c * KS_IC * KS21_T * (KS_DIG - 1) + row;
@@ -237,7 +240,8 @@ __global__ void __launch_bounds__(KS_TILE) ks21_kernel(const uint32_t *__restric
         for (int k = 0; k < KS_PER; ++k) {
             const int e = t + k * KS_TILE;
             if (e < KS_LOADS) {
-                const int q = e % 4, row = e / 4, ij = row / (KS_DIG - 1), d = row % (KS_DIG - 1) + 1;
+                const int q = e % (KS_WB / 4), row = e / (KS_WB / 4), ij = row / (KS_DIG - 1),
+                          d = row % (KS_DIG - 1) + 1;
                 stage[buf][(ij * KS_DIG + d) * KS_RW4 + q] = r[k];
             }
         }
