@@ -8,6 +8,8 @@ first transform step on the tensor cores):
   TFHEpp's, and output phases agree within 2^25 (the bootstrapping noise is
   about 2^18.5; 2^25 is 1/16 of mu);
 * HomNAND (TFHEpp src/gate.cpp:50-65: IKS10 + PBS01);
+* GateBootstrappingTLWE2TLWEFFT<lvl02param> on a two-pass batch (phases
+  within 2^56 of the 64-bit torus, mu = 2^61);
 * the HEDB comparison chains greater_than / greater_than_equal / less_than /
   less_than_equal / equal (src/HEDB/comparison/HomCompare.h:14-75, MSB
   extraction src/HEDB/comparison/extract_msb.cpp) at lvl1 widths 4, 8, 9
@@ -30,7 +32,7 @@ import pytest
 
 from conftest import SEED, signed_diff
 
-from oracle.oracle import N0, N1, NS_LVL0, NS_LVL1, NS_LVL2
+from oracle.oracle import N0, N1, N2, NS_LVL0, NS_LVL1, NS_LVL2
 
 pytestmark = pytest.mark.gpu
 MU = 1 << 29
@@ -91,6 +93,31 @@ def test_pbs01_matches_reference_on_both_launch_shapes(engine, oracle, ref_keyed
         assert np.array_equal((pr > 0).astype(int), bits), B
         d = np.abs(pg - pr)
         assert np.max(d) < 2 ** 25, (B, int(np.max(d)))
+
+
+def test_pbs02_matches_reference_on_a_two_pass_batch(eng_all, oracle, ref_all, keys):
+    """GateBootstrappingTLWE2TLWEFFT<lvl02param> on 3 x #SMs + 7 ciphertexts
+    (one full pass of the 3-per-CTA shape and a ragged second): every output
+    decrypts to its bit, and 40 sampled outputs agree with TFHEpp's on the
+    same keys and inputs within 2^56 of the 64-bit torus (mu = 2^61)."""
+    import torch
+    from cufhedb_b200 import testvec_const
+    s0, _, s2 = keys
+    MU2 = 1 << 61
+    B = 3 * eng_all.num_sms + 7
+    bits = np.random.default_rng(0xA5).integers(0, 2, B)
+    x = np.stack([oracle.tlwe32(MU if b else (-MU) & 0xFFFFFFFF, s0, NS_LVL0, SEED, 0xA5, i)
+                  for i, b in enumerate(bits)])
+    out = torch.zeros(B * (N2 + 1), dtype=torch.int64, device="cuda")
+    eng_all.pbs_lvl02(_dev(x), out, testvec_const(MU2))
+    eng_all.sync()
+    got = out.cpu().numpy().view(np.uint64).reshape(B, -1)
+    pg = np.array([int(signed_diff(oracle.phase64(o, s2), 0, 64)) for o in got], dtype=object)
+    assert np.array_equal(np.array([int(p > 0) for p in pg]), bits)
+    tv = np.full(N2, MU2, np.uint64)
+    for i in np.random.default_rng(0xA6).choice(B, 40, replace=False):
+        pr = int(signed_diff(oracle.phase64(ref_all.pbs02(x[i], tv), s2), 0, 64))
+        assert (pr > 0) == bool(bits[i]) and abs(pr - int(pg[i])) < 2 ** 56, int(i)
 
 
 @pytest.mark.parametrize("precision", PRECISIONS)
