@@ -298,6 +298,14 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
             acc[N1 + j] = testvec_rot1(a.tv, j, bbar);
         }
         __syncwarp();
+        if constexpr (TC) {
+            // polynomial 0's products of CMux 0; those of every later CMux are
+            // issued between the previous CMux's two inverse transforms
+            const uint32_t ab0 = valid ? abar_s[0] : 0u;
+            uint32_t w0[32];
+            if (ab0) digit_words1(w0, acc, ab0, lane);
+            tc.put_issue(w0, ab0 != 0, 0, warp, lane);
+        }
 
         for (int i = 0; i < N0; ++i) {
             const uint32_t ab = valid ? abar_s[i] : 0u;
@@ -308,12 +316,11 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
             for (int r = 0; r < 2 * L1; ++r, ++c) {
                 float2 v[16];
                 if constexpr (TC) {
-                    if (r < 2) {
-                        // polynomial r's three products (one call site for both:
-                        // code size); polynomial 1's run under the transforms of
+                    if (r == 1) {
+                        // polynomial 1's products, under the transforms of
                         // digits 1 and 2
-                        if (active) digit_words1(w, acc + r * N1, ab, lane);
-                        tc.put_issue(w, active, r, warp, lane);
+                        if (active) digit_words1(w, acc + N1, ab, lane);
+                        tc.put_issue(w, active, 1, warp, lane);
                     }
                     if (r % L1 == 0) tc.wait(r / L1, warp, a.err);
                     tc.take(v, active, r, warp);
@@ -349,7 +356,23 @@ __global__ void __launch_bounds__((W + (PRODUCER ? 1 : 0)) * 32, 1) pbs01_split_
                 }
                 ring.release(c, lane);
             }
-            if (active) {
+            if constexpr (TC) {
+                if (active) {
+                    add_inverse_split(acc, f0, xp, lane, *T);
+                    __syncwarp();
+                }
+                if (i + 1 < N0) {
+                    // the next CMux's polynomial 0 is final here: its products
+                    // run under this CMux's second inverse transform
+                    const uint32_t abn = valid ? abar_s[i + 1] : 0u;
+                    if (abn) digit_words1(w, acc, abn, lane);
+                    tc.put_issue(w, abn != 0, 0, warp, lane);
+                }
+                if (active) {
+                    add_inverse_split(acc + N1, f1, xp, lane, *T);
+                    __syncwarp();
+                }
+            } else if (active) {
                 add_inverse_split(acc, f0, xp, lane, *T);
                 add_inverse_split(acc + N1, f1, xp, lane, *T);
                 __syncwarp();
